@@ -1,0 +1,584 @@
+// driver.cu -- host drivers of the matrix-exponential path and the C ABI.
+//
+// The drivers follow calaman_G's control flow step for step (file:line
+// citations per function) but every kernel they enqueue is this library's own:
+// the norm, Pade combinations and split from elementwise.cu, the tensor-core
+// GEMMs from gemm.cu and the cluster LU from lu.cu.
+#include <cstdio>
+#include <cstring>
+#include <utility>
+
+#include "kernels.cuh"
+
+namespace clm {
+
+namespace {
+
+constexpr int kMaxDim = 46340;  // flat int indexing bound, src/expm/detail.cppm:25-28
+
+// ---- Pade tables (src/expm/expm_bridge.h:58-91; Higham 2005 eq. 2.2) -------
+constexpr double kB3[4] = {1.0, 1.0 / 2.0, 1.0 / 10.0, 1.0 / 120.0};
+constexpr double kB5[6] = {1.0, 1.0 / 2.0, 1.0 / 9.0, 1.0 / 72.0, 1.0 / 1008.0, 1.0 / 30240.0};
+constexpr double kB7[8] = {1.0,          1.0 / 2.0,     3.0 / 26.0,     5.0 / 312.0,
+                           5.0 / 3432.0, 1.0 / 11440.0, 1.0 / 308880.0, 1.0 / 17297280.0};
+constexpr double kB9[10] = {1.0,            1.0 / 2.0,        2.0 / 17.0,       7.0 / 408.0,
+                            7.0 / 4080.0,   1.0 / 8160.0,     1.0 / 159120.0,   1.0 / 4455360.0,
+                            1.0 / 196035840.0, 1.0 / 17643225600.0};
+constexpr double kB13[14] = {1.0,
+                             1.0 / 2.0,
+                             3.0 / 25.0,
+                             11.0 / 600.0,
+                             11.0 / 5520.0,
+                             3.0 / 18400.0,
+                             1.0 / 96600.0,
+                             1.0 / 1932000.0,
+                             1.0 / 48944000.0,
+                             1.0 / 1585785600.0,
+                             1.0 / 67395888000.0,
+                             1.0 / 3953892096000.0,
+                             1.0 / 355850288640000.0,
+                             1.0 / 64764752532480000.0};
+
+const double *pade_coeffs(int m) {
+  switch (m) {
+  case 3: return kB3;
+  case 5: return kB5;
+  case 7: return kB7;
+  case 9: return kB9;
+  case 13: return kB13;
+  default: return nullptr;
+  }
+}
+int pade_num_powers(int m) { return (m == 13) ? 3 : (m - 1) / 2; }
+int pade_num_gemms(int m) { return pade_num_powers(m) + 1 + ((m == 13) ? 2 : 0); }
+
+// theta_m, src/expm/plan.cppm:51-85: u = 2^-53 and u = 2^-24 columns.
+double theta_double(int m) {
+  switch (m) {
+  case 3: return 1.495585217958292e-2;
+  case 5: return 2.539398330063232e-1;
+  case 7: return 9.504178996162932e-1;
+  case 9: return 2.097847961257067;
+  case 13: return 5.371920351148152;
+  default: return 0.0;
+  }
+}
+float theta_single(int m) {
+  switch (m) {
+  case 3: return 4.258730034897931e-1f;
+  case 5: return 1.880152698533769f;
+  case 7: return 3.925724846433284f;
+  case 9: return 6.249156334514102f;
+  case 13: return 1.124873763647540e1f;
+  default: return 0.0f;
+  }
+}
+
+// expm_plan<T>, src/expm/plan.cppm:112-130 (the single column is compared and
+// log2'd in float, as the reference's float instantiation does).
+template <typename R>
+calamanExpmPlan_t plan_for(R norm1) {
+  static const int degrees[5] = {3, 5, 7, 9, 13};
+  for (int m : degrees) {
+    const R th = sizeof(R) == 4 ? (R)theta_single(m) : (R)theta_double(m);
+    if (norm1 <= th) return calamanExpmPlan_t{m, 0, pade_num_gemms(m)};
+  }
+  const R theta = sizeof(R) == 4 ? (R)theta_single(13) : (R)theta_double(13);
+  int s = (int)std::ceil(std::log2(norm1 / theta));
+  if (s < 0) s = 0;
+  return calamanExpmPlan_t{13, s, pade_num_gemms(13) + s};
+}
+
+// ---- workspaces --------------------------------------------------------
+// pade(): [P0 .. P_{np-1} | X (m = 13) | V | W | LU scratch], all 256-aligned.
+// P0 doubles as U = A W and then as the numerator p = V + U; V becomes the
+// denominator q = V - U and is factored in place (src/expm/detail.cppm:47-98).
+template <typename T>
+struct PadeWs {
+  T *P[4] = {nullptr, nullptr, nullptr, nullptr};
+  T *X = nullptr, *V = nullptr, *W = nullptr;
+  void *lu = nullptr;
+  std::size_t carve(void *base, int n, int m) {
+    Layout L(base);
+    const std::size_t nn = (std::size_t)n * n;
+    const int np = pade_num_powers(m);
+    for (int k = 0; k < np; ++k) P[k] = L.take<T>(nn);
+    if (m == 13) X = L.take<T>(nn);
+    V = L.take<T>(nn);
+    W = L.take<T>(nn);
+    lu = L.take<char>(lu_scratch_bytes(n));
+    return L.used;
+  }
+};
+
+// expm(): [As (also the squaring scratch) | colsum | norm | pade region]
+template <typename T>
+struct ExpmWs {
+  T *As = nullptr;
+  double *colsum = nullptr;
+  double *norm = nullptr;
+  void *pade = nullptr;
+  std::size_t carve(void *base, int n) {
+    Layout L(base);
+    As = L.take<T>((std::size_t)n * n);
+    colsum = L.take<double>(n);
+    norm = L.take<double>(1);
+    pade = L.cursor();
+    return L.used;
+  }
+};
+
+template <typename T>
+std::size_t pade_bytes(int n, int m) {
+  PadeWs<T> w;
+  return w.carve(nullptr, n, m);
+}
+
+template <typename T>
+std::size_t expm_bytes(int n) {
+  ExpmWs<T> e;
+  std::size_t worst = 0;
+  for (int m : {3, 5, 7, 9, 13}) worst = std::max(worst, pade_bytes<T>(n, m));
+  return e.carve(nullptr, n) + worst;
+}
+
+struct PointerModeScope {  // save / force host / restore, src/expm/expm.cppm:107-115
+  calamanHandle_t h;
+  int saved;
+  explicit PointerModeScope(calamanHandle_t handle) : h(handle), saved(CALAMAN_POINTER_MODE_HOST) {
+    if (h) {
+      saved = h->pointer_mode;
+      h->pointer_mode = CALAMAN_POINTER_MODE_HOST;
+    }
+  }
+  ~PointerModeScope() {
+    if (h) h->pointer_mode = saved;
+  }
+};
+
+// ---- pade<T>, src/expm/pade.cppm:77-191 -------------------------------------
+template <typename T>
+calamanStatus_t pade_run(cudaStream_t st, int m, int n, const T *A, int lda, T *R, int ldr,
+                         void *work, int *d_info) {
+  const double *b = pade_coeffs(m);
+  PadeWs<T> ws;
+  ws.carve(work, n, m);
+  const int np = pade_num_powers(m);
+  auto mm = [&](const T *X, int ldx, const T *Y, int ldy, double beta, T *Z) {
+    return gemm_nn<T>(st, n, n, n, 1.0, X, ldx, Y, ldy, beta, Z, n);
+  };
+  CLM_CUDA(mm(A, lda, A, lda, 0.0, ws.P[0]));                      // A2
+  if (np >= 2) CLM_CUDA(mm(ws.P[0], n, ws.P[0], n, 0.0, ws.P[1]));  // A4
+  if (np >= 3) CLM_CUDA(mm(ws.P[1], n, ws.P[0], n, 0.0, ws.P[2]));  // A6
+  if (np >= 4) CLM_CUDA(mm(ws.P[1], n, ws.P[1], n, 0.0, ws.P[3]));  // A8
+
+  double cv[5] = {0, 0, 0, 0, 0}, cw[5] = {0, 0, 0, 0, 0};
+  if (m != 13) {
+    for (int i = 0; i <= np; ++i) {
+      cv[i] = b[2 * i];
+      cw[i] = b[2 * i + 1];
+    }
+    CLM_CUDA(launch_pade_even_odd<T>(st, n, np, ws.P[0], ws.P[1], ws.P[2], ws.P[3], cv, cw, ws.V, ws.W));
+  } else {
+    // odd parity: X = b9 A2 + b11 A4 + b13 A6, W = b1 I + b3 A2 + b5 A4 + b7 A6; W += A6 X
+    const double cvo[5] = {0.0, b[9], b[11], b[13], 0.0};
+    const double cwo[5] = {b[1], b[3], b[5], b[7], 0.0};
+    CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, ws.P[0], ws.P[1], ws.P[2], nullptr, cvo, cwo, ws.X, ws.W));
+    CLM_CUDA(mm(ws.P[2], n, ws.X, n, 1.0, ws.W));
+    // even parity: X = b8 A2 + b10 A4 + b12 A6, V = b0 I + b2 A2 + b4 A4 + b6 A6; V += A6 X
+    const double cve[5] = {0.0, b[8], b[10], b[12], 0.0};
+    const double cwe[5] = {b[0], b[2], b[4], b[6], 0.0};
+    CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, ws.P[0], ws.P[1], ws.P[2], nullptr, cve, cwe, ws.X, ws.V));
+    CLM_CUDA(mm(ws.P[2], n, ws.X, n, 1.0, ws.V));
+  }
+  T *U = ws.P[0];
+  CLM_CUDA(mm(A, lda, ws.W, n, 0.0, U));  // U = A W
+  // p = V + U over U (the same thread reads then writes each element), q = V - U over V
+  CLM_CUDA(launch_pade_split<T>(st, n, U, ws.V, U, n, ws.V));
+  CLM_CUDA(getrf<T>(st, n, ws.V, n, ws.lu, d_info));
+  CLM_CUDA(getrs<T>(st, n, n, ws.V, n, ws.lu, U, n, R, ldr, d_info + 1));
+  return ok_status();
+}
+
+template <typename T>
+calamanStatus_t pade_api(calamanHandle_t blas, calamanStream_t stream, int m, int n, const T *A,
+                         int lda, T *R, int ldr, void *work, std::size_t lwork, int *d_info) {
+  if (pade_coeffs(m) == nullptr || n < 1 || n > kMaxDim || lda < n || ldr < n || work == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (lwork < pade_bytes<T>(n, m)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  if (A == nullptr || R == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  PointerModeScope pm(blas);
+  return pade_run<T>(static_cast<cudaStream_t>(stream), m, n, A, lda, R, ldr, work, d_info);
+}
+
+// ---- expm<T>, src/expm/expm.cppm:87-174 -------------------------------------
+template <typename T>
+calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, const T *A, int lda,
+                         T *E, int lde, void *work, std::size_t lwork, int *d_info,
+                         calamanExpmPlan_t *plan_out) {
+  using R = typename elem<T>::real;
+  if (n < 1 || n > kMaxDim || lda < n || lde < n || work == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (lwork < expm_bytes<T>(n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  if (A == nullptr || E == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  PointerModeScope pm(blas);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  ExpmWs<T> ws;
+  ws.carve(work, n);
+
+  // the norm the whole plan hangs off: FP64 sums on the device, one readback
+  CLM_CUDA(launch_norm1<T>(st, n, A, lda, nullptr, ws.norm));
+  double norm = 0.0;
+  double *host = (blas && blas->h_pinned) ? blas->h_pinned : &norm;
+  CLM_CUDA(cudaMemcpyAsync(host, ws.norm, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CLM_CUDA(cudaStreamSynchronize(st));
+  norm = *host;
+  if (!std::isfinite(norm)) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+
+  const calamanExpmPlan_t chosen = plan_for<R>((R)norm);
+  if (plan_out) *plan_out = chosen;
+
+  const T *src = A;
+  int ld_src = lda;
+  if (chosen.s > 0) {
+    CLM_CUDA(launch_scale_copy<T>(st, n, std::ldexp(1.0, -chosen.s), A, lda, ws.As, n));
+    src = ws.As;
+    ld_src = n;
+  }
+  CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info));
+
+  // square s times, ping-ponging between the output and the scratch
+  T *cur = E, *other = ws.As;
+  int ld_cur = lde, ld_other = n;
+  for (int k = 0; k < chosen.s; ++k) {
+    CLM_CUDA(gemm_nn<T>(st, n, n, n, 1.0, cur, ld_cur, cur, ld_cur, 0.0, other, ld_other));
+    std::swap(cur, other);
+    std::swap(ld_cur, ld_other);
+  }
+  if (cur != E) CLM_CUDA(launch_scale_copy<T>(st, n, 1.0, cur, ld_cur, E, lde));
+  return ok_status();
+}
+
+template <typename T, typename R>
+R norm1_api(calamanStream_t stream, int n, const T *A, int lda, R *d_colsum) {
+  if (n < 1 || lda < n || A == nullptr || d_colsum == nullptr) return (R)NAN;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (launch_colsums_then_max<T, R>(st, n, A, lda, d_colsum) != cudaSuccess) return (R)NAN;
+  R host = (R)NAN;
+  if (cudaMemcpyAsync(&host, d_colsum, sizeof(R), cudaMemcpyDeviceToHost, st) != cudaSuccess) return (R)NAN;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return (R)NAN;
+  return host;
+}
+
+// ---- horner<T>, src/horner/interface.cppm:104-194 ---------------------------
+template <typename T>
+std::size_t horner_bytes(int n) {
+  const std::size_t order = (std::size_t)(n < 1 ? 1 : n);
+  return align_up(order * order * sizeof(T), 256);
+}
+
+template <typename T>
+calamanStatus_t horner_api(calamanHandle_t h, int n, const T *c, int degree, const T *A, int lda,
+                           T *P, int ldp, void *work, std::size_t wbytes) {
+  const calamanStatus_t bad = blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (!(n >= 1 && degree >= 0 && lda >= n && ldp >= n)) return bad;
+  if (c == nullptr || A == nullptr || P == nullptr) return bad;
+  if (!(degree == 0 || (work != nullptr && wbytes >= horner_bytes<T>(n)))) return bad;
+  if (h == nullptr) return bad;
+  cudaStream_t st = h->stream;
+  T *buf[2] = {P, static_cast<T *>(work)};
+  const int ld[2] = {ldp, n};
+  int cur = (degree % 2 == 0) ? 0 : 1;
+  CLM_CUDA(launch_set_scaled_identity<T>(st, buf[cur], n, ld[cur], c + degree));
+  for (int k = degree - 1; k >= 0; --k) {
+    const int next = 1 - cur;
+    CLM_CUDA(gemm_nn<T>(st, n, n, n, 1.0, buf[cur], ld[cur], A, lda, 0.0, buf[next], ld[next]));
+    cur = next;
+    CLM_CUDA(launch_add_scaled_identity<T>(st, buf[cur], n, ld[cur], c + k));
+  }
+  return ok_status();
+}
+
+// ---- paterson_stockmeyer<T>, src/paterson_stockmeyer/interface.cppm:117-422 --
+int ps_cost(int degree, int s) {
+  if (s < 1 || degree < 1) return 0;
+  const int r = degree / s;
+  const int max_power = (r >= 1) ? s : degree;
+  const int num_powers = (max_power >= 2) ? (max_power - 1) : 0;
+  return num_powers + r;
+}
+int ps_block_size(int degree) {
+  if (degree < 1) return 1;
+  int best_s = 1, best = ps_cost(degree, 1);
+  for (int s = 2; s <= degree + 1; ++s) {
+    const int cst = ps_cost(degree, s);
+    if (cst < best) {
+      best = cst;
+      best_s = s;
+    }
+  }
+  return best_s;
+}
+calamanPatersonStockmeyerPlan_t ps_plan(int degree, int s_requested) {
+  calamanPatersonStockmeyerPlan_t p{1, 0, 0, 0, 0};
+  if (degree < 0) return p;
+  int s = (s_requested > 0) ? s_requested : ps_block_size(degree);
+  if (s > degree + 1) s = degree + 1;
+  if (s < 1) s = 1;
+  p.s = s;
+  p.r = degree / s;
+  const int max_power = (p.r >= 1) ? s : degree;
+  p.num_powers = (max_power >= 2) ? (max_power - 1) : 0;
+  p.num_blocks = p.num_powers + ((p.r >= 1) ? 1 : 0);
+  p.num_gemms = p.num_powers + p.r;
+  return p;
+}
+template <typename T>
+std::size_t ps_stride(int n) {
+  const std::size_t order = (std::size_t)(n < 1 ? 1 : n);
+  return align_up(order * order * sizeof(T), 256) / sizeof(T);
+}
+template <typename T>
+std::size_t ps_bytes(int n, int degree, int s_requested) {
+  const int order = n < 1 ? 1 : n;
+  const calamanPatersonStockmeyerPlan_t plan = ps_plan(degree, s_requested);
+  Layout L(nullptr);
+  if (plan.num_powers > 0) L.take<T>((std::size_t)plan.num_powers * ps_stride<T>(order));
+  if (plan.r >= 1) L.take<T>((std::size_t)order * order);
+  return L.used;
+}
+
+template <typename T>
+calamanStatus_t ps_api(calamanHandle_t h, int n, const T *c, int degree, const T *A, int lda, T *P,
+                       int ldp, void *work, std::size_t wbytes, int s_requested) {
+  const calamanStatus_t bad = blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (n < 1 || degree < 0 || lda < n || ldp < n || s_requested < 0) return bad;
+  if (c == nullptr || A == nullptr || P == nullptr) return bad;
+  const calamanPatersonStockmeyerPlan_t plan = ps_plan(degree, s_requested);
+  if (plan.num_blocks > 0 && (work == nullptr || wbytes < ps_bytes<T>(n, degree, s_requested)))
+    return bad;
+  if (h == nullptr) return bad;
+  cudaStream_t st = h->stream;
+  const std::size_t stride = ps_stride<T>(n);
+  Layout L(work);
+  T *powers = plan.num_powers > 0 ? L.take<T>((std::size_t)plan.num_powers * stride) : nullptr;
+  T *scratch = plan.r >= 1 ? L.take<T>((std::size_t)n * n) : nullptr;
+  // power bank: A^k = A^(k-1) A
+  for (int k = 2; k <= plan.num_powers + 1; ++k) {
+    const T *left = (k == 2) ? A : powers + (std::size_t)(k - 3) * stride;
+    const int ldl = (k == 2) ? lda : n;
+    CLM_CUDA(gemm_nn<T>(st, n, n, n, 1.0, left, ldl, A, lda, 0.0, powers + (std::size_t)(k - 2) * stride, n));
+  }
+  const bool have_x = plan.r >= 1;
+  const T *X = !have_x ? nullptr : (plan.s >= 2 ? powers + (std::size_t)(plan.s - 2) * stride : A);
+  const int ldx = (plan.s >= 2) ? n : lda;
+  T *buf[2] = {P, scratch};
+  const int ld[2] = {ldp, n};
+  int cur = (plan.r % 2 == 0) ? 0 : 1;
+  auto terms = [&](int j) {
+    const int remaining = degree - j * plan.s + 1;
+    return remaining < plan.s ? remaining : plan.s;
+  };
+  CLM_CUDA(launch_ps_build_block<T>(st, buf[cur], ld[cur], n, A, lda, powers, stride,
+                                    c + (std::size_t)plan.r * plan.s, terms(plan.r)));
+  for (int j = plan.r - 1; j >= 0; --j) {
+    const int next = 1 - cur;
+    CLM_CUDA(launch_ps_build_block<T>(st, buf[next], ld[next], n, A, lda, powers, stride,
+                                      c + (std::size_t)j * plan.s, terms(j)));
+    CLM_CUDA(gemm_nn<T>(st, n, n, n, 1.0, buf[cur], ld[cur], X, ldx, 1.0, buf[next], ld[next]));
+    cur = next;
+  }
+  return ok_status();
+}
+
+}  // namespace
+
+int sm_count() {
+  int dev = 0, cnt = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  if (cudaDeviceGetAttribute(&cnt, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+  return cnt;
+}
+
+}  // namespace clm
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using namespace clm;
+
+extern "C" {
+
+calamanStatus_t calamanCreate(calamanHandle_t *handle) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  *handle = nullptr;
+  int dev = 0;
+  CLM_CUDA(cudaGetDevice(&dev));
+  calamanContext *c = new calamanContext();
+  c->device = dev;
+  cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  const cudaError_t e = cudaMallocHost(&c->h_pinned, 4 * sizeof(double));
+  if (e != cudaSuccess) {
+    delete c;
+    return runtime_status(e);
+  }
+  *handle = c;
+  return ok_status();
+}
+
+calamanStatus_t calamanDestroy(calamanHandle_t handle) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (handle->h_pinned) cudaFreeHost(handle->h_pinned);
+  delete handle;
+  return ok_status();
+}
+
+calamanStatus_t calamanSetStream(calamanHandle_t handle, calamanStream_t stream) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  handle->stream = static_cast<cudaStream_t>(stream);
+  return ok_status();
+}
+
+calamanStatus_t calamanGetStream(calamanHandle_t handle, calamanStream_t *stream) {
+  if (handle == nullptr || stream == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  *stream = handle->stream;
+  return ok_status();
+}
+
+calamanStatus_t calamanSetPointerMode(calamanHandle_t handle, int mode) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (mode != CALAMAN_POINTER_MODE_HOST && mode != CALAMAN_POINTER_MODE_DEVICE)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  handle->pointer_mode = mode;
+  return ok_status();
+}
+
+calamanStatus_t calamanGetPointerMode(calamanHandle_t handle, int *mode) {
+  if (handle == nullptr || mode == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  *mode = handle->pointer_mode;
+  return ok_status();
+}
+
+const char *calamanGetVersion(void) { return "calaman_b200 0.1.0 (sm_100a)"; }
+
+float calaman_pade_theta_s(int m) { return theta_single(m); }
+double calaman_pade_theta_d(int m) { return theta_double(m); }
+calamanExpmPlan_t calaman_expm_plan_s(float norm1) { return plan_for<float>(norm1); }
+calamanExpmPlan_t calaman_expm_plan_d(double norm1) { return plan_for<double>(norm1); }
+int calaman_pade_num_powers(int m) { return pade_coeffs(m) ? pade_num_powers(m) : 0; }
+int calaman_pade_num_gemms(int m) { return pade_coeffs(m) ? pade_num_gemms(m) : 0; }
+
+#define CLM_BUFSZ(SUF, T)                                                                     \
+  calamanStatus_t calaman_expm_bufferSize_##SUF(calamanSolverHandle_t, int n, size_t *bytes) { \
+    if (n < 1 || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);          \
+    *bytes = expm_bytes<T>(n);                                                                \
+    return ok_status();                                                                       \
+  }                                                                                           \
+  calamanStatus_t calaman_pade_bufferSize_##SUF(calamanSolverHandle_t, int m, int n,          \
+                                                size_t *bytes) {                              \
+    if (pade_coeffs(m) == nullptr || n < 1 || bytes == nullptr)                               \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                       \
+    *bytes = pade_bytes<T>(n, m);                                                             \
+    return ok_status();                                                                       \
+  }
+CLM_BUFSZ(s, float)
+CLM_BUFSZ(d, double)
+CLM_BUFSZ(c, float2)
+CLM_BUFSZ(z, double2)
+#undef CLM_BUFSZ
+
+calamanStatus_t calaman_expm_s(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int n, const float *A, int lda, float *E, int lde, void *w,
+                               size_t lw, int *info, calamanExpmPlan_t *plan) {
+  return expm_api<float>(blas, stream, n, A, lda, E, lde, w, lw, info, plan);
+}
+calamanStatus_t calaman_expm_d(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int n, const double *A, int lda, double *E, int lde, void *w,
+                               size_t lw, int *info, calamanExpmPlan_t *plan) {
+  return expm_api<double>(blas, stream, n, A, lda, E, lde, w, lw, info, plan);
+}
+calamanStatus_t calaman_expm_c(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int n, const void *A, int lda, void *E, int lde, void *w, size_t lw,
+                               int *info, calamanExpmPlan_t *plan) {
+  return expm_api<float2>(blas, stream, n, static_cast<const float2 *>(A), lda,
+                          static_cast<float2 *>(E), lde, w, lw, info, plan);
+}
+calamanStatus_t calaman_expm_z(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int n, const void *A, int lda, void *E, int lde, void *w, size_t lw,
+                               int *info, calamanExpmPlan_t *plan) {
+  return expm_api<double2>(blas, stream, n, static_cast<const double2 *>(A), lda,
+                           static_cast<double2 *>(E), lde, w, lw, info, plan);
+}
+
+calamanStatus_t calaman_pade_s(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int m, int n, const float *A, int lda, float *R, int ldr, void *w,
+                               size_t lw, int *info) {
+  return pade_api<float>(blas, stream, m, n, A, lda, R, ldr, w, lw, info);
+}
+calamanStatus_t calaman_pade_d(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int m, int n, const double *A, int lda, double *R, int ldr, void *w,
+                               size_t lw, int *info) {
+  return pade_api<double>(blas, stream, m, n, A, lda, R, ldr, w, lw, info);
+}
+calamanStatus_t calaman_pade_c(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int m, int n, const void *A, int lda, void *R, int ldr, void *w,
+                               size_t lw, int *info) {
+  return pade_api<float2>(blas, stream, m, n, static_cast<const float2 *>(A), lda,
+                          static_cast<float2 *>(R), ldr, w, lw, info);
+}
+calamanStatus_t calaman_pade_z(calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream,
+                               int m, int n, const void *A, int lda, void *R, int ldr, void *w,
+                               size_t lw, int *info) {
+  return pade_api<double2>(blas, stream, m, n, static_cast<const double2 *>(A), lda,
+                           static_cast<double2 *>(R), ldr, w, lw, info);
+}
+
+float calaman_matrix_norm1_s(calamanStream_t s, int n, const float *A, int lda, float *cs) {
+  return norm1_api<float, float>(s, n, A, lda, cs);
+}
+double calaman_matrix_norm1_d(calamanStream_t s, int n, const double *A, int lda, double *cs) {
+  return norm1_api<double, double>(s, n, A, lda, cs);
+}
+float calaman_matrix_norm1_c(calamanStream_t s, int n, const void *A, int lda, float *cs) {
+  return norm1_api<float2, float>(s, n, static_cast<const float2 *>(A), lda, cs);
+}
+double calaman_matrix_norm1_z(calamanStream_t s, int n, const void *A, int lda, double *cs) {
+  return norm1_api<double2, double>(s, n, static_cast<const double2 *>(A), lda, cs);
+}
+
+size_t calaman_horner_bufferSize_s(int n) { return horner_bytes<float>(n); }
+size_t calaman_horner_bufferSize_d(int n) { return horner_bytes<double>(n); }
+calamanStatus_t calaman_horner_s(calamanBlasHandle_t h, int n, const float *c, int degree,
+                                 const float *A, int lda, float *P, int ldp, void *w, size_t wb) {
+  return horner_api<float>(h, n, c, degree, A, lda, P, ldp, w, wb);
+}
+calamanStatus_t calaman_horner_d(calamanBlasHandle_t h, int n, const double *c, int degree,
+                                 const double *A, int lda, double *P, int ldp, void *w, size_t wb) {
+  return horner_api<double>(h, n, c, degree, A, lda, P, ldp, w, wb);
+}
+
+int calaman_paterson_stockmeyer_cost(int degree, int s) { return ps_cost(degree, s); }
+int calaman_paterson_stockmeyer_block_size(int degree) { return ps_block_size(degree); }
+calamanPatersonStockmeyerPlan_t calaman_paterson_stockmeyer_plan(int degree, int s_requested) {
+  return ps_plan(degree, s_requested);
+}
+size_t calaman_paterson_stockmeyer_power_stride_s(int n) { return ps_stride<float>(n); }
+size_t calaman_paterson_stockmeyer_power_stride_d(int n) { return ps_stride<double>(n); }
+size_t calaman_paterson_stockmeyer_bufferSize_s(int n, int degree, int s_req) {
+  return ps_bytes<float>(n, degree, s_req);
+}
+size_t calaman_paterson_stockmeyer_bufferSize_d(int n, int degree, int s_req) {
+  return ps_bytes<double>(n, degree, s_req);
+}
+calamanStatus_t calaman_paterson_stockmeyer_s(calamanBlasHandle_t h, int n, const float *c, int degree,
+                                              const float *A, int lda, float *P, int ldp, void *w,
+                                              size_t wb, int s_req) {
+  return ps_api<float>(h, n, c, degree, A, lda, P, ldp, w, wb, s_req);
+}
+calamanStatus_t calaman_paterson_stockmeyer_d(calamanBlasHandle_t h, int n, const double *c,
+                                              int degree, const double *A, int lda, double *P,
+                                              int ldp, void *w, size_t wb, int s_req) {
+  return ps_api<double>(h, n, c, degree, A, lda, P, ldp, w, wb, s_req);
+}
+
+}  // extern "C"

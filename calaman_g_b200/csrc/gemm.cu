@@ -1,0 +1,471 @@
+// gemm.cu -- C = alpha A B + beta C (NN, column-major) for the four element
+// types of the path.
+//
+//   double   : FP64 tensor-core tiles (mma.sync m16n8k8 .f64, "DMMA"); tcgen05
+//              has no f64 kind, so this is the FP64 tensor path on sm_100a.
+//   double2  : complex128 as four real DMMA products per tile
+//              (Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br), operands read once
+//              as interleaved 16-byte pairs.
+//   float / float2 : register-tiled FP32 SIMT kernel (the plain single tier).
+//
+// Operands are staged global -> shared by cp.async in a multi-stage ring; all
+// edges (M, N, K not multiples of the tile) are zero-filled by the copy's
+// src-size operand, so any shape and any leading dimension is legal.
+#include "kernels.cuh"
+
+namespace clm {
+
+namespace {
+
+// ---- cp.async helpers -------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+// 16-byte copy with zero fill past src_bytes (0, 8 or 16)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// D = A B + D on a 16x8x8 FP64 tile. Fragment ownership (g = lane>>2,
+// t = lane&3): A a0=(g,t) a1=(g+8,t) a2=(g,t+4) a3=(g+8,t+4); B b0=(t,g)
+// b1=(t+4,g); C c0=(g,2t) c1=(g,2t+1) c2=(g+8,2t) c3=(g+8,2t+1).
+__device__ __forceinline__ void dmma16x8x8(double (&d)[4], const double (&a)[4],
+                                           const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// ---------------------------------------------------------------------------
+// Real FP64: CTA tile BM x BN x 16, warp tile WM x WN built from 16x8 DMMAs.
+// Shared layout: sA[k][m] (row stride BM+4 doubles), sB[n][k] (stride 20);
+// both strides are 4 mod 16 doubles, which makes every 8-byte fragment load
+// of a half-warp hit 16 distinct bank pairs.
+// ---------------------------------------------------------------------------
+template <int BM, int BN, int WM, int WN, int STAGES, bool V16>
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
+    dgemm_nn_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, int lda,
+                    const double *__restrict__ B, int ldb, double beta, double *__restrict__ C,
+                    int ldc) {
+  constexpr int BK = 16;
+  constexpr int NT = (BM / WM) * (BN / WN) * 32;
+  constexpr int SA = BM + 4;
+  constexpr int SB = BK + 4;
+  constexpr int MI = WM / 16;
+  constexpr int NI = WN / 8;
+  extern __shared__ __align__(16) double smem_d[];
+  double *sA = smem_d;                       // [STAGES][BK][SA]
+  double *sB = smem_d + STAGES * BK * SA;    // [STAGES][BN][SB]
+
+  const int m0 = blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp % (BM / WM)) * WM;
+  const int wn0 = (warp / (BM / WM)) * WN;
+
+  auto load_tile = [&](int stage, int kt) {
+    const int k0 = kt * BK;
+    double *a = sA + stage * BK * SA;
+    double *b = sB + stage * BN * SB;
+    if (V16) {
+      constexpr int CA = BK * BM / 2;
+#pragma unroll
+      for (int c = tid; c < CA; c += NT) {
+        const int kk = c / (BM / 2), mm = (c % (BM / 2)) * 2;
+        const int gm = m0 + mm, gk = k0 + kk;
+        int bytes = (gk < K) ? (M - gm) * 8 : 0;
+        bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+        const double *src = bytes ? A + (std::size_t)gk * lda + gm : A;
+        cp_async16(a + kk * SA + mm, src, bytes);
+      }
+      constexpr int CB = BN * BK / 2;
+#pragma unroll
+      for (int c = tid; c < CB; c += NT) {
+        const int nn = c / (BK / 2), kk = (c % (BK / 2)) * 2;
+        const int gn = n0 + nn, gk = k0 + kk;
+        int bytes = (gn < N) ? (K - gk) * 8 : 0;
+        bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+        const double *src = bytes ? B + (std::size_t)gn * ldb + gk : B;
+        cp_async16(b + nn * SB + kk, src, bytes);
+      }
+    } else {
+      constexpr int CA = BK * BM;
+#pragma unroll 4
+      for (int c = tid; c < CA; c += NT) {
+        const int kk = c / BM, mm = c % BM;
+        const int gm = m0 + mm, gk = k0 + kk;
+        const int bytes = (gk < K && gm < M) ? 8 : 0;
+        cp_async8(a + kk * SA + mm, bytes ? A + (std::size_t)gk * lda + gm : A, bytes);
+      }
+      constexpr int CB = BN * BK;
+#pragma unroll 4
+      for (int c = tid; c < CB; c += NT) {
+        const int nn = c / BK, kk = c % BK;
+        const int gn = n0 + nn, gk = k0 + kk;
+        const int bytes = (gn < N && gk < K) ? 8 : 0;
+        cp_async8(b + nn * SB + kk, bytes ? B + (std::size_t)gn * ldb + gk : B, bytes);
+      }
+    }
+  };
+
+  double acc[MI][NI][4];
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+
+  const int KT = (K + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_commit();
+  }
+
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + STAGES - 1;
+      if (nk < KT) load_tile(nk % STAGES, nk);
+      cp_commit();
+    }
+    const double *a = sA + (kt % STAGES) * BK * SA;
+    const double *b = sB + (kt % STAGES) * BN * SB;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double af[MI][4], bf[NI][2];
+#pragma unroll
+      for (int i = 0; i < MI; ++i) {
+        const int m = wm0 + i * 16 + g;
+        af[i][0] = a[(kk + t) * SA + m];
+        af[i][1] = a[(kk + t) * SA + m + 8];
+        af[i][2] = a[(kk + t + 4) * SA + m];
+        af[i][3] = a[(kk + t + 4) * SA + m + 8];
+      }
+#pragma unroll
+      for (int j = 0; j < NI; ++j) {
+        const int nn = wn0 + j * 8 + g;
+        bf[j][0] = b[nn * SB + kk + t];
+        bf[j][1] = b[nn * SB + kk + t + 4];
+      }
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NI; ++j) dmma16x8x8(acc[i][j], af[i], bf[j]);
+    }
+  }
+  cp_wait<0>();
+
+  // epilogue: C = alpha acc + beta C (beta == 0 never reads C)
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
+        const int n = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        if (m < M && n < N) {
+          double *c = C + (std::size_t)n * ldc + m;
+          const double v = alpha * acc[i][j][r];
+          *c = (beta == 0.0) ? v : fma(beta, *c, v);
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Complex128: CTA tile BM x BN x 16 complex, interleaved (re, im) in shared
+// memory; each fragment element is one 16-byte load. Row strides BM+2 and 20
+// (complex units) are 2 and 4 mod 8, so a quarter-warp's 16-byte loads hit
+// 8 distinct bank quads.
+// ---------------------------------------------------------------------------
+template <int BM, int BN, int WM, int WN, int STAGES>
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
+    zgemm_nn_kernel(int M, int N, int K, double alpha, const double2 *__restrict__ A, int lda,
+                    const double2 *__restrict__ B, int ldb, double beta, double2 *__restrict__ C,
+                    int ldc) {
+  constexpr int BK = 16;
+  constexpr int NT = (BM / WM) * (BN / WN) * 32;
+  constexpr int SA = BM + 2;
+  constexpr int SB = BK + 4;
+  constexpr int MI = WM / 16;
+  constexpr int NI = WN / 8;
+  extern __shared__ __align__(16) double2 smem_z[];
+  double2 *sA = smem_z;
+  double2 *sB = smem_z + STAGES * BK * SA;
+
+  const int m0 = blockIdx.x * BM;
+  const int n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp % (BM / WM)) * WM;
+  const int wn0 = (warp / (BM / WM)) * WN;
+
+  auto load_tile = [&](int stage, int kt) {
+    const int k0 = kt * BK;
+    double2 *a = sA + stage * BK * SA;
+    double2 *b = sB + stage * BN * SB;
+    constexpr int CA = BK * BM;
+#pragma unroll
+    for (int c = tid; c < CA; c += NT) {
+      const int kk = c / BM, mm = c % BM;
+      const int gm = m0 + mm, gk = k0 + kk;
+      const int bytes = (gk < K && gm < M) ? 16 : 0;
+      cp_async16(a + kk * SA + mm, bytes ? A + (std::size_t)gk * lda + gm : A, bytes);
+    }
+    constexpr int CB = BN * BK;
+#pragma unroll
+    for (int c = tid; c < CB; c += NT) {
+      const int nn = c / BK, kk = c % BK;
+      const int gn = n0 + nn, gk = k0 + kk;
+      const int bytes = (gn < N && gk < K) ? 16 : 0;
+      cp_async16(b + nn * SB + kk, bytes ? B + (std::size_t)gn * ldb + gk : B, bytes);
+    }
+  };
+
+  double re[MI][NI][4], im[MI][NI][4];
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) re[i][j][r] = im[i][j][r] = 0.0;
+
+  const int KT = (K + BK - 1) / BK;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) load_tile(s, s);
+    cp_commit();
+  }
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int nk = kt + STAGES - 1;
+      if (nk < KT) load_tile(nk % STAGES, nk);
+      cp_commit();
+    }
+    const double2 *a = sA + (kt % STAGES) * BK * SA;
+    const double2 *b = sB + (kt % STAGES) * BN * SB;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double ar[MI][4], ai[MI][4], an[MI][4], br[NI][2], bi[NI][2];
+#pragma unroll
+      for (int i = 0; i < MI; ++i) {
+        const int m = wm0 + i * 16 + g;
+        const double2 x0 = a[(kk + t) * SA + m];
+        const double2 x1 = a[(kk + t) * SA + m + 8];
+        const double2 x2 = a[(kk + t + 4) * SA + m];
+        const double2 x3 = a[(kk + t + 4) * SA + m + 8];
+        ar[i][0] = x0.x; ai[i][0] = x0.y;
+        ar[i][1] = x1.x; ai[i][1] = x1.y;
+        ar[i][2] = x2.x; ai[i][2] = x2.y;
+        ar[i][3] = x3.x; ai[i][3] = x3.y;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) an[i][r] = -ai[i][r];
+      }
+#pragma unroll
+      for (int j = 0; j < NI; ++j) {
+        const int nn = wn0 + j * 8 + g;
+        const double2 y0 = b[nn * SB + kk + t];
+        const double2 y1 = b[nn * SB + kk + t + 4];
+        br[j][0] = y0.x; bi[j][0] = y0.y;
+        br[j][1] = y1.x; bi[j][1] = y1.y;
+      }
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NI; ++j) {
+          dmma16x8x8(re[i][j], ar[i], br[j]);
+          dmma16x8x8(re[i][j], an[i], bi[j]);
+          dmma16x8x8(im[i][j], ar[i], bi[j]);
+          dmma16x8x8(im[i][j], ai[i], br[j]);
+        }
+    }
+  }
+  cp_wait<0>();
+
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
+        const int n = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        if (m < M && n < N) {
+          double2 *c = C + (std::size_t)n * ldc + m;
+          double2 v = make_double2(alpha * re[i][j][r], alpha * im[i][j][r]);
+          if (beta != 0.0) {
+            const double2 o = *c;
+            v.x = fma(beta, o.x, v.x);
+            v.y = fma(beta, o.y, v.y);
+          }
+          *c = v;
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 SIMT (float, complex64): 64 x 64 CTA tile, 16-deep k slices, 256
+// threads each owning a 4 x 4 micro-tile (rows ty + 16 i, cols tx + 16 j).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256)
+    simt_gemm_nn_kernel(int M, int N, int K, double alpha, const T *__restrict__ A, int lda,
+                        const T *__restrict__ B, int ldb, double beta, T *__restrict__ C, int ldc) {
+  using R = typename elem<T>::real;
+  constexpr int BM = 64, BN = 64, BK = 16;
+  __shared__ T sA[2][BK][BM];
+  __shared__ T sB[2][BK][BN + 1];
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = elem<T>::zero();
+
+  auto load = [&](int buf, int k0) {
+#pragma unroll
+    for (int c = tid; c < BK * BM; c += 256) {
+      const int kk = c / BM, mm = c % BM;
+      const int gm = m0 + mm, gk = k0 + kk;
+      sA[buf][kk][mm] = (gm < M && gk < K) ? A[(std::size_t)gk * lda + gm] : elem<T>::zero();
+    }
+#pragma unroll
+    for (int c = tid; c < BK * BN; c += 256) {
+      const int nn = c / BK, kk = c % BK;
+      const int gn = n0 + nn, gk = k0 + kk;
+      sB[buf][kk][nn] = (gn < N && gk < K) ? B[(std::size_t)gn * ldb + gk] : elem<T>::zero();
+    }
+  };
+  const int KT = (K + BK - 1) / BK;
+  load(0, 0);
+  __syncthreads();
+  for (int kt = 0; kt < KT; ++kt) {
+    const int cur = kt & 1;
+    if (kt + 1 < KT) load(cur ^ 1, (kt + 1) * BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = sA[cur][kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = sB[cur][kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmac(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
+      if (m < M && n < N) {
+        T *c = C + (std::size_t)n * ldc + m;
+        T v = scale(acc[i][j], (R)alpha);
+        if (beta != 0.0) v = add(v, scale(*c, (R)beta));
+        *c = v;
+      }
+    }
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES, bool V16>
+cudaError_t run_dgemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, int lda,
+                      const double *B, int ldb, double beta, double *C, int ldc) {
+  constexpr int NT = (BM / WM) * (BN / WN) * 32;
+  constexpr int smem = STAGES * (16 * (BM + 4) + BN * 20) * (int)sizeof(double);
+  auto kern = dgemm_nn_kernel<BM, BN, WM, WN, STAGES, V16>;
+  static bool configured = false;  // attribute is per-function, process-wide
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+  kern<<<grid, NT, smem, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  return cudaGetLastError();
+}
+
+template <int BM, int BN, int WM, int WN, int STAGES>
+cudaError_t run_zgemm(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A, int lda,
+                      const double2 *B, int ldb, double beta, double2 *C, int ldc) {
+  constexpr int NT = (BM / WM) * (BN / WN) * 32;
+  constexpr int smem = STAGES * (16 * (BM + 2) + BN * 20) * (int)sizeof(double2);
+  auto kern = zgemm_nn_kernel<BM, BN, WM, WN, STAGES>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
+  kern<<<grid, NT, smem, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  return cudaGetLastError();
+}
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<std::uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+template <>
+cudaError_t gemm_nn<double>(cudaStream_t s, int M, int N, int K, double alpha, const double *A,
+                            int lda, const double *B, int ldb, double beta, double *C, int ldc) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  const bool v16 = aligned16(A) && aligned16(B) && (lda % 2 == 0) && (ldb % 2 == 0);
+  const long long big_tiles = (long long)((M + 127) / 128) * ((N + 127) / 128);
+  if (big_tiles >= 132) {
+    return v16 ? run_dgemm<128, 128, 64, 32, 3, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+               : run_dgemm<128, 128, 64, 32, 3, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  }
+  return v16 ? run_dgemm<64, 64, 32, 32, 4, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+             : run_dgemm<64, 64, 32, 32, 4, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+template <>
+cudaError_t gemm_nn<double2>(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A,
+                             int lda, const double2 *B, int ldb, double beta, double2 *C, int ldc) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  return run_zgemm<64, 64, 32, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+template <>
+cudaError_t gemm_nn<float>(cudaStream_t s, int M, int N, int K, double alpha, const float *A,
+                           int lda, const float *B, int ldb, double beta, float *C, int ldc) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  dim3 grid((M + 63) / 64, (N + 63) / 64);
+  simt_gemm_nn_kernel<float><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t gemm_nn<float2>(cudaStream_t s, int M, int N, int K, double alpha, const float2 *A,
+                            int lda, const float2 *B, int ldb, double beta, float2 *C, int ldc) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  dim3 grid((M + 63) / 64, (N + 63) / 64);
+  simt_gemm_nn_kernel<float2><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  return cudaGetLastError();
+}
+
+}  // namespace clm

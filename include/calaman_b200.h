@@ -1,0 +1,210 @@
+/*
+ * calaman_b200.h -- C ABI of the B200-native matrix-exponential library.
+ *
+ * A drop-in for calaman_G's `calaman.expm`, `calaman.paterson_stockmeyer` and
+ * `calaman.horner` C++23 modules. Every entry point below names the reference
+ * interface it replaces (paths relative to the calaman_G project). The
+ * reference's template functions are split into one symbol per element type:
+ *   _s float   _d double   _c complex float (interleaved)   _z complex double
+ * horner / paterson_stockmeyer exist for _s and _d only, as in the reference
+ * (src/horner/instantiations.cpp, src/paterson_stockmeyer/instantiations.cpp).
+ *
+ * Conventions kept from the reference:
+ *   - Column-major matrices; every leading dimension >= n.
+ *   - The caller owns every buffer, including the workspace, which must be
+ *     256-byte aligned and sized by the matching *_bufferSize query. The
+ *     library allocates no device memory on these paths.
+ *   - Only the n x n block of an output is written; padding rows between n
+ *     and the leading dimension are left untouched.
+ *   - Everything is stream ordered. expm synchronises its stream once (to
+ *     read the 1-norm); pade, horner and paterson_stockmeyer never do.
+ *   - Errors come back as calamanStatus_t {domain, code}: argument errors are
+ *     rejected before any device work. expm/pade return INVALID_VALUE for bad
+ *     arguments or a non-finite norm and ALLOC_FAILED for a short workspace;
+ *     horner/paterson_stockmeyer return NOT_INITIALIZED for every argument
+ *     error (src/expm/expm.cppm:94-102,122-124,
+ *     src/paterson_stockmeyer/interface.cppm:333-345,
+ *     src/horner/interface.cppm:160-164).
+ *
+ * The handle plays both roles of the reference's wwrblasHandle_t and
+ * wwrsolverDnHandle_t: it carries the stream and the pointer mode.
+ * Complex arguments are passed as pointers to interleaved (re, im) pairs.
+ */
+#ifndef CALAMAN_B200_H
+#define CALAMAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status (src/error_handling/error_handling.cppm:88-187) ------------ */
+typedef enum {
+  CALAMAN_DOMAIN_BLAS = 0,
+  CALAMAN_DOMAIN_SOLVER = 1,
+  CALAMAN_DOMAIN_RUNTIME = 2
+} calamanErrorDomain_t;
+
+/* BLAS-domain codes, numerically those of the CUDA backend's blas status. */
+enum {
+  CALAMAN_STATUS_SUCCESS = 0,
+  CALAMAN_STATUS_NOT_INITIALIZED = 1,
+  CALAMAN_STATUS_ALLOC_FAILED = 3,
+  CALAMAN_STATUS_INVALID_VALUE = 7,
+  CALAMAN_STATUS_ARCH_MISMATCH = 8,
+  CALAMAN_STATUS_EXECUTION_FAILED = 13,
+  CALAMAN_STATUS_INTERNAL_ERROR = 14,
+  CALAMAN_STATUS_NOT_SUPPORTED = 15
+};
+
+typedef struct {
+  int32_t domain; /* calamanErrorDomain_t */
+  int32_t code;   /* 0 = success in every domain */
+} calamanStatus_t;
+
+/* ---- handle (replaces wwrblasHandle_t / wwrsolverDnHandle_t) ----------- */
+typedef struct calamanContext *calamanHandle_t;
+typedef calamanHandle_t calamanBlasHandle_t;
+typedef calamanHandle_t calamanSolverHandle_t;
+typedef void *calamanStream_t; /* a cudaStream_t */
+
+enum { CALAMAN_POINTER_MODE_HOST = 0, CALAMAN_POINTER_MODE_DEVICE = 1 };
+
+/* wwrblasCreate / wwrsolverDnCreate: binds the current device, stream 0. */
+calamanStatus_t calamanCreate(calamanHandle_t *handle);
+calamanStatus_t calamanDestroy(calamanHandle_t handle);
+/* wwrblasSetStream / wwrblasGetStream */
+calamanStatus_t calamanSetStream(calamanHandle_t handle, calamanStream_t stream);
+calamanStatus_t calamanGetStream(calamanHandle_t handle, calamanStream_t *stream);
+/* wwrblasSetPointerMode / GetPointerMode; expm and pade save and restore it
+ * (src/expm/expm.cppm:107-115). */
+calamanStatus_t calamanSetPointerMode(calamanHandle_t handle, int mode);
+calamanStatus_t calamanGetPointerMode(calamanHandle_t handle, int *mode);
+
+/* Library version string and the sm_ target it was compiled for. */
+const char *calamanGetVersion(void);
+
+/* ---- plan (src/expm/plan.cppm:51-130) --------------------------------- */
+typedef struct {
+  int m;         /* Pade degree in {3, 5, 7, 9, 13} */
+  int s;         /* squarings: the matrix is evaluated at A / 2^s */
+  int num_gemms; /* matrix products the evaluation issues */
+} calamanExpmPlan_t;
+
+/* pade_theta<T>(m): backward-error threshold, 0 off the ladder. _s/_c use
+ * the u = 2^-24 column, _d/_z the u = 2^-53 column. */
+float calaman_pade_theta_s(int m);
+double calaman_pade_theta_d(int m);
+/* expm_plan<T>(norm1) */
+calamanExpmPlan_t calaman_expm_plan_s(float norm1);
+calamanExpmPlan_t calaman_expm_plan_d(double norm1);
+/* pade_num_powers / pade_num_gemms (src/expm/expm_bridge.h:122-130) */
+int calaman_pade_num_powers(int m);
+int calaman_pade_num_gemms(int m);
+
+/* ---- workspace queries (src/expm/buffer_size.cppm:47-97) --------------- */
+calamanStatus_t calaman_expm_bufferSize_s(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_bufferSize_d(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_bufferSize_c(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_bufferSize_z(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_pade_bufferSize_s(calamanSolverHandle_t h, int m, int n, size_t *bytes);
+calamanStatus_t calaman_pade_bufferSize_d(calamanSolverHandle_t h, int m, int n, size_t *bytes);
+calamanStatus_t calaman_pade_bufferSize_c(calamanSolverHandle_t h, int m, int n, size_t *bytes);
+calamanStatus_t calaman_pade_bufferSize_z(calamanSolverHandle_t h, int m, int n, size_t *bytes);
+
+/* ---- expm (src/expm/expm.cppm:87-174) ----------------------------------
+ * exp(A) by scaling and squaring with a diagonal Pade approximant (Higham
+ * 2005, Algorithm 2.3). d_info: device array of 2 ints ([0] LU info, [1]
+ * solve info). plan may be NULL. Synchronises `stream` once.
+ * The _s/_c tiers run their dense products as split-BF16 tensor-core GEMMs
+ * with FP32 accumulation; the 1-norm is always accumulated in FP64. */
+calamanStatus_t calaman_expm_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int n, const float *d_A, int lda,
+                               float *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                               int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int n, const double *d_A, int lda,
+                               double *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                               int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_c(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int n, const void *d_A, int lda,
+                               void *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                               int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_z(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int n, const void *d_A, int lda,
+                               void *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                               int *d_info, calamanExpmPlan_t *plan);
+
+/* ---- pade (src/expm/pade.cppm:77-191) ----------------------------------
+ * Unscaled r_m(A) = q_m(A)^-1 p_m(A); never synchronises. */
+calamanStatus_t calaman_pade_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int m, int n, const float *d_A, int lda,
+                               float *d_r, int ldr, void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_pade_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int m, int n, const double *d_A, int lda,
+                               double *d_r, int ldr, void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_pade_c(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int m, int n, const void *d_A, int lda,
+                               void *d_r, int ldr, void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_pade_z(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                               calamanStream_t stream, int m, int n, const void *d_A, int lda,
+                               void *d_r, int ldr, void *d_work, size_t lwork_bytes, int *d_info);
+
+/* ---- matrix_norm1 (src/expm/norm1.cppm:45-56) --------------------------
+ * Maximum absolute column sum (true complex modulus), NaN if any element is
+ * NaN. d_colsum: device scratch of n reals of the element's real type; it
+ * receives the column sums and, in [0], the maximum. Synchronises `stream`.
+ * Returns NaN (and writes nothing) for n < 1 or a null pointer. */
+float calaman_matrix_norm1_s(calamanStream_t stream, int n, const float *d_A, int lda,
+                             float *d_colsum);
+double calaman_matrix_norm1_d(calamanStream_t stream, int n, const double *d_A, int lda,
+                              double *d_colsum);
+float calaman_matrix_norm1_c(calamanStream_t stream, int n, const void *d_A, int lda,
+                             float *d_colsum);
+double calaman_matrix_norm1_z(calamanStream_t stream, int n, const void *d_A, int lda,
+                              double *d_colsum);
+
+/* ---- horner (src/horner/interface.cppm:104-194) ------------------------ */
+size_t calaman_horner_bufferSize_s(int n);
+size_t calaman_horner_bufferSize_d(int n);
+/* P = sum_{k=0}^{degree} c_k A^k by Horner's rule; coefficients on the
+ * DEVICE, ascending. d_work may be NULL when degree == 0. */
+calamanStatus_t calaman_horner_s(calamanBlasHandle_t handle, int n, const float *d_coeffs,
+                                 int degree, const float *d_A, int lda, float *d_P, int ldp,
+                                 void *d_work, size_t work_bytes);
+calamanStatus_t calaman_horner_d(calamanBlasHandle_t handle, int n, const double *d_coeffs,
+                                 int degree, const double *d_A, int lda, double *d_P, int ldp,
+                                 void *d_work, size_t work_bytes);
+
+/* ---- paterson_stockmeyer (src/paterson_stockmeyer/interface.cppm:117-422) */
+typedef struct {
+  int s;          /* block size actually used */
+  int r;          /* Horner steps over X = A^s: floor(degree / s) */
+  int num_powers; /* powers held at once: A^2 .. A^(num_powers+1) */
+  int num_blocks; /* n x n workspace blocks */
+  int num_gemms;  /* matrix products issued */
+} calamanPatersonStockmeyerPlan_t;
+
+int calaman_paterson_stockmeyer_cost(int degree, int s);
+int calaman_paterson_stockmeyer_block_size(int degree);
+calamanPatersonStockmeyerPlan_t calaman_paterson_stockmeyer_plan(int degree, int s_requested);
+size_t calaman_paterson_stockmeyer_power_stride_s(int n);
+size_t calaman_paterson_stockmeyer_power_stride_d(int n);
+size_t calaman_paterson_stockmeyer_bufferSize_s(int n, int degree, int s_requested);
+size_t calaman_paterson_stockmeyer_bufferSize_d(int n, int degree, int s_requested);
+calamanStatus_t calaman_paterson_stockmeyer_s(calamanBlasHandle_t handle, int n,
+                                              const float *d_coeffs, int degree, const float *d_A,
+                                              int lda, float *d_P, int ldp, void *d_work,
+                                              size_t work_bytes, int s_requested);
+calamanStatus_t calaman_paterson_stockmeyer_d(calamanBlasHandle_t handle, int n,
+                                              const double *d_coeffs, int degree,
+                                              const double *d_A, int lda, double *d_P, int ldp,
+                                              void *d_work, size_t work_bytes, int s_requested);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CALAMAN_B200_H */

@@ -1,0 +1,248 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle is a C restatement of calaman_G's expm / pade / matrix_norm1 /
+paterson_stockmeyer / horner path, computed in FP64 (see oracle.h for the
+per-function citations). Only tests/, ``__graft_entry__.smoke()`` and
+``bench.py``'s CPU-baseline leg import this module; the product library never
+does.
+
+Matrices are numpy arrays; they are passed column-major (Fortran order), the
+layout the reference uses.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc only; seconds)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+class _ExpmPlan(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_int), ("s", ctypes.c_int), ("num_gemms", ctypes.c_int)]
+
+
+class _PsPlan(ctypes.Structure):
+    _fields_ = [
+        ("s", ctypes.c_int),
+        ("r", ctypes.c_int),
+        ("num_powers", ctypes.c_int),
+        ("num_blocks", ctypes.c_int),
+        ("num_gemms", ctypes.c_int),
+    ]
+
+
+@dataclass(frozen=True)
+class ExpmPlan:
+    m: int
+    s: int
+    num_gemms: int
+
+
+@dataclass(frozen=True)
+class PsPlan:
+    s: int
+    r: int
+    num_powers: int
+    num_blocks: int
+    num_gemms: int
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        c_int, c_double = ctypes.c_int, ctypes.c_double
+        L.oracle_set_threads.argtypes = [c_int]
+        L.oracle_get_threads.restype = c_int
+        L.oracle_pade_theta.argtypes = [c_int, c_int]
+        L.oracle_pade_theta.restype = c_double
+        L.oracle_expm_plan.argtypes = [c_double, c_int]
+        L.oracle_expm_plan.restype = _ExpmPlan
+        L.oracle_pade_coeffs.argtypes = [c_int]
+        L.oracle_pade_coeffs.restype = dp
+        L.oracle_pade_num_powers.argtypes = [c_int]
+        L.oracle_pade_num_gemms.argtypes = [c_int]
+        L.oracle_ps_cost.argtypes = [c_int, c_int]
+        L.oracle_ps_block_size.argtypes = [c_int]
+        L.oracle_ps_plan.argtypes = [c_int, c_int]
+        L.oracle_ps_plan.restype = _PsPlan
+        for suf in ("d", "z"):
+            getattr(L, f"oracle_norm1_{suf}").argtypes = [c_int, dp, c_int]
+            getattr(L, f"oracle_norm1_{suf}").restype = c_double
+            getattr(L, f"oracle_pade_{suf}").argtypes = [c_int, c_int, dp, c_int, dp, c_int, ip]
+            getattr(L, f"oracle_expm_{suf}").argtypes = [
+                c_int, dp, c_int, dp, c_int, c_int, ctypes.POINTER(_ExpmPlan), ip]
+            getattr(L, f"oracle_getrf_{suf}").argtypes = [c_int, dp, c_int, ip]
+            getattr(L, f"oracle_getrs_{suf}").argtypes = [c_int, c_int, dp, c_int, ip, dp, c_int]
+        L.oracle_gemm_d.argtypes = [c_int, c_int, c_int, c_double, dp, c_int, dp, c_int,
+                                    c_double, dp, c_int]
+        L.oracle_gemm_z.argtypes = [c_int, c_int, c_int, dp, dp, c_int, dp, c_int, dp, dp, c_int]
+        L.oracle_paterson_stockmeyer_d.argtypes = [c_int, dp, c_int, dp, c_int, dp, c_int, c_int]
+        L.oracle_horner_d.argtypes = [c_int, dp, c_int, dp, c_int, dp, c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _suffix(a: np.ndarray) -> str:
+    return "z" if np.iscomplexobj(a) else "d"
+
+
+def _as_f64(a) -> np.ndarray:
+    a = np.asarray(a)
+    dt = np.complex128 if np.iscomplexobj(a) else np.float64
+    return np.asfortranarray(a, dtype=dt)
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(int(n))
+
+
+def pade_theta(m: int, single: bool = False) -> float:
+    return lib().oracle_pade_theta(m, int(single))
+
+
+def expm_plan(norm1: float, single: bool = False) -> ExpmPlan:
+    p = lib().oracle_expm_plan(float(norm1), int(single))
+    return ExpmPlan(p.m, p.s, p.num_gemms)
+
+
+def pade_coeffs(m: int):
+    p = lib().oracle_pade_coeffs(m)
+    if not p:
+        return None
+    return [p[i] for i in range(m + 1)]
+
+
+def pade_num_powers(m: int) -> int:
+    return lib().oracle_pade_num_powers(m)
+
+
+def pade_num_gemms(m: int) -> int:
+    return lib().oracle_pade_num_gemms(m)
+
+
+def ps_cost(degree: int, s: int) -> int:
+    return lib().oracle_ps_cost(degree, s)
+
+
+def ps_block_size(degree: int) -> int:
+    return lib().oracle_ps_block_size(degree)
+
+
+def ps_plan(degree: int, s_requested: int = 0) -> PsPlan:
+    p = lib().oracle_ps_plan(degree, s_requested)
+    return PsPlan(p.s, p.r, p.num_powers, p.num_blocks, p.num_gemms)
+
+
+def norm1(a) -> float:
+    a = _as_f64(a)
+    n = a.shape[0]
+    return getattr(lib(), f"oracle_norm1_{_suffix(a)}")(n, _dp(a), max(n, 1))
+
+
+def gemm(a, b, c=None, alpha=1.0, beta=0.0) -> np.ndarray:
+    a, b = _as_f64(a), _as_f64(b)
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(b) or (c is not None and np.iscomplexobj(c))
+    dt = np.complex128 if cplx else np.float64
+    a, b = np.asfortranarray(a, dtype=dt), np.asfortranarray(b, dtype=dt)
+    m, k = a.shape
+    n = b.shape[1]
+    out = np.zeros((m, n), dtype=dt, order="F") if c is None else np.array(c, dtype=dt, order="F")
+    if cplx:
+        al = np.array([complex(alpha).real, complex(alpha).imag])
+        be = np.array([complex(beta).real, complex(beta).imag])
+        lib().oracle_gemm_z(m, n, k, _dp(al), _dp(a), max(m, 1), _dp(b), max(k, 1), _dp(be),
+                            _dp(out), max(m, 1))
+    else:
+        lib().oracle_gemm_d(m, n, k, float(alpha), _dp(a), max(m, 1), _dp(b), max(k, 1),
+                            float(beta), _dp(out), max(m, 1))
+    return out
+
+
+def getrf(a):
+    """LU with partial pivoting; returns (LU, ipiv 0-based, info)."""
+    a = np.array(_as_f64(a), order="F")
+    n = a.shape[0]
+    ipiv = np.zeros(n, dtype=np.int32)
+    info = getattr(lib(), f"oracle_getrf_{_suffix(a)}")(n, _dp(a), n, _ip(ipiv))
+    return a, ipiv, info
+
+
+def pade(a, m: int):
+    """Unscaled r_m(A). Returns (R, getrf_info)."""
+    a = _as_f64(a)
+    n = a.shape[0]
+    r = np.zeros_like(a, order="F")
+    info = ctypes.c_int(0)
+    rc = getattr(lib(), f"oracle_pade_{_suffix(a)}")(m, n, _dp(a), n, _dp(r), n,
+                                                      ctypes.byref(info))
+    if rc != 0:
+        raise ValueError(f"oracle pade rejected its arguments (rc={rc})")
+    return r, info.value
+
+
+def expm(a, single: bool = False):
+    """exp(A) by the reference's scaling and squaring, in FP64.
+
+    ``single`` selects the single-precision theta ladder, i.e. the (m, s) the
+    float / complex-float path picks. Returns (E, ExpmPlan, getrf_info).
+    """
+    a = _as_f64(a)
+    n = a.shape[0]
+    e = np.zeros_like(a, order="F")
+    plan = _ExpmPlan()
+    info = ctypes.c_int(0)
+    rc = getattr(lib(), f"oracle_expm_{_suffix(a)}")(n, _dp(a), n, _dp(e), n, int(single),
+                                                      ctypes.byref(plan), ctypes.byref(info))
+    if rc == -2:
+        raise FloatingPointError("1-norm is not finite")
+    if rc != 0:
+        raise ValueError(f"oracle expm rejected its arguments (rc={rc})")
+    return e, ExpmPlan(plan.m, plan.s, plan.num_gemms), info.value
+
+
+def paterson_stockmeyer(a, coeffs, s_requested: int = 0) -> np.ndarray:
+    a = np.asfortranarray(a, dtype=np.float64)
+    c = np.ascontiguousarray(coeffs, dtype=np.float64)
+    n = a.shape[0]
+    p = np.zeros((n, n), order="F")
+    rc = lib().oracle_paterson_stockmeyer_d(n, _dp(c), len(c) - 1, _dp(a), n, _dp(p), n,
+                                            int(s_requested))
+    if rc != 0:
+        raise ValueError("oracle paterson_stockmeyer rejected its arguments")
+    return p
+
+
+def horner(a, coeffs) -> np.ndarray:
+    a = np.asfortranarray(a, dtype=np.float64)
+    c = np.ascontiguousarray(coeffs, dtype=np.float64)
+    n = a.shape[0]
+    p = np.zeros((n, n), order="F")
+    rc = lib().oracle_horner_d(n, _dp(c), len(c) - 1, _dp(a), n, _dp(p), n)
+    if rc != 0:
+        raise ValueError("oracle horner rejected its arguments")
+    return p

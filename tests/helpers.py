@@ -1,0 +1,171 @@
+"""Shared test helpers: seeded inputs in the reference's test shapes, the
+reference's tolerance formulas, and thin runners that call the C ABI directly
+(column-major buffers, explicit leading dimensions) through ctypes."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+NP_DTYPE = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}
+REAL = {"s": np.float32, "d": np.float64, "c": np.float32, "z": np.float64}
+
+
+def eps(suf: str) -> float:
+    return float(np.finfo(REAL[suf]).eps)
+
+
+def norm1(a: np.ndarray) -> float:
+    return float(np.abs(a).sum(axis=0).max())
+
+
+def scaled_random(n: int, target: float, seed: int, cplx: bool = False) -> np.ndarray:
+    """U(-1,1) entries rescaled to 1-norm `target` (test/expm/expm_tests.cpp:316-336)."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-1.0, 1.0, (n, n))
+    if cplx:
+        a = a + 1j * rng.uniform(-1.0, 1.0, (n, n))
+    nrm = norm1(a)
+    return a * (target / nrm) if nrm > 0 else a
+
+
+def gaussian_scaled(n: int, target: float, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n))
+    return a * (target / norm1(a))
+
+
+def gue_skew(n: int, target: float, seed: int) -> np.ndarray:
+    """A = -i H, H = (X + X^H)/2, X complex N(0,1); rescaled to 1-norm target."""
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = (x + x.conj().T) / 2
+    a = -1j * h
+    return a * (target / norm1(a))
+
+
+def elem_tol(oracle: np.ndarray, n: int, factor: float, suf: str) -> float:
+    """factor * eps * max(1, ||oracle||_F) * n (test/expm/expm_tests.cpp:206-217)."""
+    return factor * eps(suf) * max(1.0, float(np.linalg.norm(oracle))) * n
+
+
+def rel_frob(got: np.ndarray, ref: np.ndarray) -> float:
+    return float(np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-300))
+
+
+# ---------------------------------------------------------------------------
+# device runners (torch provides the memory and the stream)
+# ---------------------------------------------------------------------------
+def _dev(x: np.ndarray):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def colmajor_buffer(a: np.ndarray, ld: int, suf: str, fill=-123.5) -> np.ndarray:
+    """Flat column-major buffer of an n x n matrix with leading dimension ld;
+    padding rows carry the sentinel `fill`."""
+    n = a.shape[0]
+    buf = np.full((n, ld), fill, dtype=NP_DTYPE[suf])
+    buf[:, :n] = a.T.astype(NP_DTYPE[suf])
+    return buf.reshape(-1)
+
+
+def from_buffer(buf: np.ndarray, n: int, ld: int) -> np.ndarray:
+    return buf.reshape(n, ld)[:, :n].T.copy()
+
+
+def vp(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Runner:
+    """Calls the C ABI with a fresh handle bound to torch's current stream."""
+
+    def __init__(self):
+        import torch
+
+        from calaman_g_b200 import capi
+
+        self.torch = torch
+        self.capi = capi
+        self.lib = capi.load()
+        h = ctypes.c_void_p()
+        st = self.lib.calamanCreate(ctypes.byref(h))
+        assert st.ok, st
+        self.h = h
+        self.stream = torch.cuda.current_stream().cuda_stream
+        assert self.lib.calamanSetStream(h, ctypes.c_void_p(self.stream)).ok
+
+    def close(self):
+        self.lib.calamanDestroy(self.h)
+
+    def workspace(self, nbytes: int):
+        return self.torch.empty(max(nbytes, 256), dtype=self.torch.uint8, device="cuda")
+
+    def expm(self, a: np.ndarray, suf: str, lda: int | None = None, lde: int | None = None,
+             out_fill=-123.5, lwork: int | None = None):
+        n = a.shape[0]
+        lda = lda or n
+        lde = lde or n
+        dA = _dev(colmajor_buffer(a, lda, suf))
+        dE = _dev(np.full(n * lde, out_fill, dtype=NP_DTYPE[suf]))
+        b = ctypes.c_size_t()
+        assert getattr(self.lib, f"calaman_expm_bufferSize_{suf}")(self.h, n, ctypes.byref(b)).ok
+        w = self.workspace(b.value)
+        info = self.torch.full((2,), -99, dtype=self.torch.int32, device="cuda")
+        plan = self.capi.ExpmPlan()
+        st = getattr(self.lib, f"calaman_expm_{suf}")(
+            self.h, self.h, ctypes.c_void_p(self.stream), n, vp(dA), lda, vp(dE), lde, vp(w),
+            b.value if lwork is None else lwork, ctypes.cast(info.data_ptr(), self.capi.c_int_p),
+            ctypes.byref(plan))
+        self.torch.cuda.synchronize()
+        full = dE.cpu().numpy()
+        return st, plan, from_buffer(full, n, lde), full, info.cpu().numpy()
+
+    def pade(self, a: np.ndarray, m: int, suf: str):
+        n = a.shape[0]
+        dA = _dev(colmajor_buffer(a, n, suf))
+        dR = _dev(np.zeros(n * n, dtype=NP_DTYPE[suf]))
+        b = ctypes.c_size_t()
+        assert getattr(self.lib, f"calaman_pade_bufferSize_{suf}")(self.h, m, n, ctypes.byref(b)).ok
+        w = self.workspace(b.value)
+        info = self.torch.full((2,), -99, dtype=self.torch.int32, device="cuda")
+        st = getattr(self.lib, f"calaman_pade_{suf}")(
+            self.h, self.h, ctypes.c_void_p(self.stream), m, n, vp(dA), n, vp(dR), n, vp(w),
+            b.value, ctypes.cast(info.data_ptr(), self.capi.c_int_p))
+        self.torch.cuda.synchronize()
+        return st, from_buffer(dR.cpu().numpy(), n, n), info.cpu().numpy()
+
+    def norm1(self, a: np.ndarray, suf: str) -> float:
+        n = a.shape[0]
+        dA = _dev(colmajor_buffer(a, n, suf))
+        cs = self.torch.empty(n, dtype=self.torch.float32 if suf in "sc" else self.torch.float64,
+                              device="cuda")
+        return getattr(self.lib, f"calaman_matrix_norm1_{suf}")(
+            ctypes.c_void_p(self.stream), n, vp(dA), n, vp(cs))
+
+    def poly(self, kind: str, a: np.ndarray, c: np.ndarray, suf: str, s_requested: int = 0,
+             ldp: int | None = None, out_fill=0.0):
+        n = a.shape[0]
+        ldp = ldp or n
+        degree = len(c) - 1
+        dA = _dev(colmajor_buffer(a, n, suf))
+        dc = _dev(np.asarray(c, dtype=NP_DTYPE[suf]))
+        dP = _dev(np.full(n * ldp, out_fill, dtype=NP_DTYPE[suf]))
+        if kind == "horner":
+            nb = getattr(self.lib, f"calaman_horner_bufferSize_{suf}")(n) if degree > 0 else 0
+            w = self.workspace(nb) if nb else None
+            st = getattr(self.lib, f"calaman_horner_{suf}")(
+                self.h, n, vp(dc), degree, vp(dA), n, vp(dP), ldp,
+                vp(w) if w is not None else None, nb)
+        else:
+            nb = getattr(self.lib, f"calaman_paterson_stockmeyer_bufferSize_{suf}")(
+                n, degree, s_requested)
+            w = self.workspace(nb) if nb else None
+            st = getattr(self.lib, f"calaman_paterson_stockmeyer_{suf}")(
+                self.h, n, vp(dc), degree, vp(dA), n, vp(dP), ldp,
+                vp(w) if w is not None else None, nb, s_requested)
+        self.torch.cuda.synchronize()
+        full = dP.cpu().numpy()
+        return st, from_buffer(full, n, ldp), full
