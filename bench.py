@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 matrix-exponential path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config expm_c128_1024]
+
+One step = one expm of the workload matrix through the C ABI
+(calaman_expm_<t>). The default workload is the complex128 1024 x 1024
+matrix A = -iH, H = (X + X^H)/2 with X complex N(0,1) (GUE), rescaled to
+1-norm 50 (Pade degree 13, 4 squarings): seeded synthetic data of the shape
+the reference's headline configuration names.
+
+Printed (rank 0, one JSON line):
+  value       expm/s over all ranks, inputs resident in HBM, L2 flushed
+              (256 MiB write, untimed) before every timed step;
+  e2e         the same through the C ABI with pinned host buffers: H2D of A,
+              expm, D2H of exp(A), all inside the timed region;
+  roofline    dense-product throughput measured live with CUDA events around
+              every GEMM launch in the timed steps, against the FP64 tensor
+              peak measured in this run (cuBLAS complex128 GEMM, 4096^3);
+  cpu_baseline  the C oracle (FP64 restatement of the reference algorithm)
+              on this host's cores, on the same matrix.
+With torchrun (N > 1) every rank runs its own replica (a single expm does not
+shard) and value = N * K / (max over ranks of the timed seconds).
+`--impl reference` times the reference algorithm's CPU restatement alone.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "expm/s & TFLOP/s at rel err<=1e-6 vs FP64"
+
+CONFIGS = {
+    # name: (n, type suffix, 1-norm, generator)
+    "expm_c128_1024": dict(n=1024, suf="z", norm=50.0, gen="gue",
+                           desc="complex128 1024x1024, A=-iH (GUE), ||A||_1=50"),
+    "expm_f64_256": dict(n=256, suf="d", norm=4.0, gen="gauss",
+                         desc="float64 256x256, N(0,1) rescaled to ||A||_1=4"),
+    "expm_f64_2048": dict(n=2048, suf="d", norm=6.0, gen="gauss",
+                          desc="float64 2048x2048, N(0,1) rescaled to ||A||_1=6"),
+    "expm_f32_4096": dict(n=4096, suf="s", norm=8.0, gen="gauss",
+                          desc="float32 4096x4096, N(0,1)/sqrt(n) rescaled to ||A||_1=8"),
+}
+NP = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}
+ELEM_BYTES = {"s": 4, "d": 8, "c": 8, "z": 16}
+
+
+def make_matrix(cfg, seed=20261203):
+    rng = np.random.default_rng(seed)
+    n = cfg["n"]
+    if cfg["gen"] == "gue":
+        x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        a = -1j * (x + x.conj().T) / 2
+    else:
+        a = rng.standard_normal((n, n)) / np.sqrt(n)
+    a = a * (cfg["norm"] / np.abs(a).sum(axis=0).max())
+    return np.asfortranarray(a.astype(NP[cfg["suf"]]))
+
+
+def expm_flops(n, m, s, cplx):
+    pim = {3: 2, 5: 3, 7: 4, 9: 5, 13: 6}[m]
+    f = (pim + s) * 2.0 * n ** 3 + (2.0 / 3.0) * n ** 3 + 2.0 * n ** 3
+    return f * (4.0 if cplx else 1.0)
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
+    """The oracle (FP64 restatement of the reference algorithm) on all host
+    threads: whole expm calls of the same matrix until min_seconds."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    reps, t0 = 0, time.perf_counter()
+    result = None
+    while True:
+        result, plan, _ = O.expm(a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64),
+                                 single=cfg["suf"] in "sc")
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds or reps >= max_reps:
+            break
+    return {"value": reps / el, "unit": "expm/s", "cores": cores, "kind": "port",
+            "sample": f"{reps} full expm call(s) of the benchmark matrix ({cfg['desc']}), "
+                      f"{el:.1f} s, C oracle with {cores} threads"}, result
+
+
+def run_reference(args, cfg):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    a = make_matrix(cfg)
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    x = a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
+    for _ in range(args.warmup):
+        O.expm(x, single=cfg["suf"] in "sc")
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _, plan, _ = O.expm(x, single=cfg["suf"] in "sc")
+    el = time.perf_counter() - t0
+    value = args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "expm/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[cfg["suf"]],
+        "data": "synthetic (seeded)",
+        "config": {"workload": args.config, "desc": cfg["desc"], "plan": {"m": plan.m, "s": plan.s}},
+        "tflops": expm_flops(cfg["n"], plan.m, plan.s, cfg["suf"] in "cz") * value / 1e12,
+        "cpu_baseline": {"value": value, "unit": "expm/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} timed expm calls after {args.warmup} warm-up, "
+                                   f"C oracle (FP64 restatement of the reference algorithm), "
+                                   f"{cores} threads"},
+        "e2e": {"value": value, "unit": "expm/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def measure_fp64_peak(torch, dev, cplx):
+    """cuBLAS (torch.matmul) FP64 GEMM throughput at 4096^3: the FP64 tensor
+    denominator (the driver's peak file carries no FP64 figure)."""
+    n = 4096
+    dt = torch.complex128 if cplx else torch.float64
+    a = torch.randn(n, n, dtype=dt, device=dev)
+    b = torch.randn(n, n, dtype=dt, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    flops = (8.0 if cplx else 2.0) * n ** 3
+    del a, b
+    return flops / (best * 1e-3) / 1e12
+
+
+def read_traffic(name):
+    """dram bytes per dense-product launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"{name}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, cfg):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    from calaman_g_b200 import capi
+
+    lib = capi.load()
+    suf, n = cfg["suf"], cfg["n"]
+    cplx = suf in "cz"
+    a = make_matrix(cfg)
+
+    baseline, oracle_result = (None, None)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        baseline, oracle_result = cpu_baseline(a, cfg)
+
+    tdt = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}[suf]
+    host_a = torch.from_numpy(np.ascontiguousarray(a.T).reshape(-1)).to(tdt).pin_memory()
+    host_e = torch.empty_like(host_a).pin_memory()
+    dA = host_a.to(dev)
+    dE = torch.empty_like(dA)
+    stream = torch.cuda.Stream(device=dev)
+    h = ctypes.c_void_p()
+    assert lib.calamanCreate(ctypes.byref(h)).ok
+    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
+    nb = ctypes.c_size_t()
+    assert getattr(lib, f"calaman_expm_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    info = torch.zeros(2, dtype=torch.int32, device=dev)
+    infop = ctypes.cast(info.data_ptr(), capi.c_int_p)
+    plan = capi.ExpmPlan()
+    fn = getattr(lib, f"calaman_expm_{suf}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), n, ctypes.c_void_p(dA.data_ptr()), n,
+                ctypes.c_void_p(dE.data_ptr()), n, ctypes.c_void_p(work.data_ptr()), nb.value,
+                infop, ctypes.byref(plan))
+        if not st.ok:
+            raise RuntimeError(f"expm failed: {st!r}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+
+    # ---- timed: inputs resident, L2 flushed before each step ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.calamanGetLaunchCount()
+    assert lib.calamanSetKernelTiming(h, 1).ok
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                starts[i].record(stream)
+                step()
+                ends[i].record(stream)
+        torch.cuda.synchronize()
+        launches = lib.calamanGetLaunchCount() - launches0
+        kt = capi.KernelTiming()
+        assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
+        lib.calamanSetKernelTiming(h, 0)
+        total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+        # ---- e2e: pinned host in, pinned host out, through the C ABI ----
+        e2e_ms = 0.0
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record(stream)
+                dA.copy_(host_a, non_blocking=True)
+                step()
+                host_e.copy_(dE, non_blocking=True)
+                e.record(stream)
+                e.synchronize()
+                e2e_ms += s.elapsed_time(e)
+    torch.cuda.synchronize()
+    if info.cpu().tolist() != [0, 0]:
+        raise RuntimeError(f"LU reported info {info.cpu().tolist()}")
+
+    t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = t.tolist()
+    value = world * args.steps / (total_ms * 1e-3)
+    e2e_value = world * args.steps / (e2e_ms * 1e-3)
+
+    if rank == 0:
+        flops = expm_flops(n, plan.m, plan.s, cplx)
+        peak = measure_fp64_peak(torch, dev, cplx)
+        achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
+        got = host_e.numpy().reshape(n, n).T
+        acc = {}
+        if oracle_result is not None:
+            acc["rel_frob_vs_oracle"] = float(np.linalg.norm(got - oracle_result)
+                                              / np.linalg.norm(oracle_result))
+        if cfg["gen"] == "gue":
+            g = got.astype(np.complex128)
+            acc["unitarity_frob"] = float(np.linalg.norm(g.conj().T @ g - np.eye(n)))
+        line = {
+            "metric": METRIC, "value": value, "unit": "expm/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[suf],
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.config, "desc": cfg["desc"],
+                       "plan": {"m": plan.m, "s": plan.s, "num_gemms": plan.num_gemms},
+                       "l2": "flushed before every timed step (256 MiB write, untimed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "tflops": flops * value / 1e12,
+            "algorithmic_flops_per_expm": flops,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if achieved else None,
+                         "traffic": read_traffic(f"zgemm_{n}" if cplx else f"dgemm_{n}"),
+                         "kernel": "dense products (every GEMM launch in the timed steps)",
+                         "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
+                         "peak_source": "cuBLAS complex128/float64 GEMM 4096^3 measured in this run "
+                                        "(MEASURED_PEAKS.json has no FP64 figure)"},
+            "cpu_baseline": baseline,
+            "e2e": {"value": e2e_value, "unit": "expm/s",
+                    "h2d_bytes_per_step": n * n * ELEM_BYTES[suf],
+                    "d2h_bytes_per_step": n * n * ELEM_BYTES[suf]},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    lib.calamanDestroy(h)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="expm_c128_1024", choices=sorted(CONFIGS))
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = p.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

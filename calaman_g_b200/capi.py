@@ -69,6 +69,11 @@ class PsPlan(ctypes.Structure):
                 ("num_gemms", c_int)]
 
 
+class KernelTiming(ctypes.Structure):
+    _fields_ = [("gemm_launches", ctypes.c_longlong), ("gemm_ms", c_double),
+                ("gemm_flops", c_double)]
+
+
 # symbol -> (restype, argtypes); the list mirrors include/calaman_b200.h
 _H = c_void_p  # calamanHandle_t
 _EXPM = [_H, _H, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_size_t, c_int_p,
@@ -105,13 +110,19 @@ SIGNATURES = {
     "calaman_paterson_stockmeyer_bufferSize_d": (c_size_t, [c_int, c_int, c_int]),
     "calaman_paterson_stockmeyer_s": (Status, _PS),
     "calaman_paterson_stockmeyer_d": (Status, _PS),
+    "calamanGetLaunchCount": (ctypes.c_ulonglong, []),
+    "calamanSetKernelTiming": (Status, [_H, c_int]),
+    "calamanGetKernelTiming": (Status, [_H, ctypes.POINTER(KernelTiming)]),
 }
+_GEMM = [c_void_p, c_int, c_int, c_int, c_double, c_void_p, c_int, c_void_p, c_int, c_double,
+         c_void_p, c_int]
 for _suf, _real in (("s", c_float), ("d", c_double), ("c", c_float), ("z", c_double)):
     SIGNATURES[f"calaman_expm_bufferSize_{_suf}"] = (Status, [_H, c_int, c_size_t_p])
     SIGNATURES[f"calaman_pade_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int, c_size_t_p])
     SIGNATURES[f"calaman_expm_{_suf}"] = (Status, _EXPM)
     SIGNATURES[f"calaman_pade_{_suf}"] = (Status, _PADE)
     SIGNATURES[f"calaman_matrix_norm1_{_suf}"] = (_real, [c_void_p, c_int, c_void_p, c_int, c_void_p])
+    SIGNATURES[f"calaman_gemm_{_suf}"] = (Status, _GEMM)
 
 _lib = None
 

@@ -11,6 +11,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cmath>
+#include <vector>
 
 #include "../../include/calaman_b200.h"
 
@@ -190,6 +191,32 @@ struct Layout {
 // Number of SMs on the current device (cached per device).
 int sm_count();
 
+// Every launcher bumps this process-wide counter (calamanGetLaunchCount).
+void note_launch(unsigned n = 1);
+// After a <<<>>> launch: count it and return the launch error.
+inline cudaError_t launched() {
+  note_launch(1);
+  return cudaGetLastError();
+}
+
+// CUDA-event timing of GEMM launches, active while a handle with timing
+// enabled is inside one of its calls (set per thread by TimerScope).
+struct KernelTimer {
+  bool enabled = false;
+  std::vector<cudaEvent_t> pool;  // reused event objects
+  std::size_t used = 0;           // events handed out since the last read
+  std::vector<cudaEvent_t> starts, stops;  // one pair per recorded launch
+  std::vector<double> flops;               // algorithmic flops of that launch
+  cudaEvent_t take();
+};
+extern thread_local KernelTimer *tl_timer;
+
+struct TimerScope {
+  KernelTimer *saved;
+  explicit TimerScope(KernelTimer *t) : saved(tl_timer) { tl_timer = (t && t->enabled) ? t : nullptr; }
+  ~TimerScope() { tl_timer = saved; }
+};
+
 }  // namespace clm
 
 // The opaque handle behind calamanHandle_t.
@@ -199,4 +226,5 @@ struct calamanContext {
   int device = 0;
   int sm_count = 0;
   double *h_pinned = nullptr;  // pinned host slots for the 1-norm readback
+  clm::KernelTimer timer;
 };

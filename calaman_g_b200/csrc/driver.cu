@@ -4,6 +4,7 @@
 // citations per function) but every kernel they enqueue is this library's own:
 // the norm, Pade combinations and split from elementwise.cu, the tensor-core
 // GEMMs from gemm.cu and the cluster LU from lu.cu.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <utility>
@@ -12,7 +13,11 @@
 
 namespace clm {
 
+unsigned long long g_launch_count();
+
 namespace {
+
+inline KernelTimer *timer_of(calamanHandle_t h) { return h ? &h->timer : nullptr; }
 
 constexpr int kMaxDim = 46340;  // flat int indexing bound, src/expm/detail.cppm:25-28
 
@@ -208,6 +213,7 @@ calamanStatus_t pade_api(calamanHandle_t blas, calamanStream_t stream, int m, in
   if (lwork < pade_bytes<T>(n, m)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
   if (A == nullptr || R == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   PointerModeScope pm(blas);
+  TimerScope ts(timer_of(blas));
   return pade_run<T>(static_cast<cudaStream_t>(stream), m, n, A, lda, R, ldr, work, d_info);
 }
 
@@ -222,6 +228,7 @@ calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, co
   if (lwork < expm_bytes<T>(n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
   if (A == nullptr || E == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   PointerModeScope pm(blas);
+  TimerScope ts(timer_of(blas));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   ExpmWs<T> ws;
   ws.carve(work, n);
@@ -285,6 +292,7 @@ calamanStatus_t horner_api(calamanHandle_t h, int n, const T *c, int degree, con
   if (c == nullptr || A == nullptr || P == nullptr) return bad;
   if (!(degree == 0 || (work != nullptr && wbytes >= horner_bytes<T>(n)))) return bad;
   if (h == nullptr) return bad;
+  TimerScope ts(timer_of(h));
   cudaStream_t st = h->stream;
   T *buf[2] = {P, static_cast<T *>(work)};
   const int ld[2] = {ldp, n};
@@ -358,6 +366,7 @@ calamanStatus_t ps_api(calamanHandle_t h, int n, const T *c, int degree, const T
   if (plan.num_blocks > 0 && (work == nullptr || wbytes < ps_bytes<T>(n, degree, s_requested)))
     return bad;
   if (h == nullptr) return bad;
+  TimerScope ts(timer_of(h));
   cudaStream_t st = h->stream;
   const std::size_t stride = ps_stride<T>(n);
   Layout L(work);
@@ -398,6 +407,23 @@ int sm_count() {
   if (cudaGetDevice(&dev) != cudaSuccess) return 148;
   if (cudaDeviceGetAttribute(&cnt, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
   return cnt;
+}
+
+namespace {
+std::atomic<unsigned long long> g_launches{0};
+}
+void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+unsigned long long g_launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+thread_local KernelTimer *tl_timer = nullptr;
+
+cudaEvent_t KernelTimer::take() {
+  if (used < pool.size()) return pool[used++];
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  pool.push_back(e);
+  ++used;
+  return e;
 }
 
 }  // namespace clm
@@ -579,6 +605,60 @@ calamanStatus_t calaman_paterson_stockmeyer_d(calamanBlasHandle_t h, int n, cons
                                               int degree, const double *A, int lda, double *P,
                                               int ldp, void *w, size_t wb, int s_req) {
   return ps_api<double>(h, n, c, degree, A, lda, P, ldp, w, wb, s_req);
+}
+
+#define CLM_GEMM_API(SUF, T, PT, CPT)                                                          \
+  calamanStatus_t calaman_gemm_##SUF(calamanStream_t stream, int m, int n, int k, double alpha, \
+                                     CPT A, int lda, CPT B, int ldb, double beta, PT C,         \
+                                     int ldc) {                                                 \
+    if (m < 0 || n < 0 || k < 0 || lda < (m > 1 ? m : 1) || ldb < (k > 1 ? k : 1) ||            \
+        ldc < (m > 1 ? m : 1))                                                                  \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                         \
+    if (m == 0 || n == 0) return ok_status();                                                   \
+    if (C == nullptr || (k > 0 && (A == nullptr || B == nullptr)))                              \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                         \
+    CLM_CUDA(gemm_nn<T>(static_cast<cudaStream_t>(stream), m, n, k, alpha,                      \
+                        reinterpret_cast<const T *>(A), lda, reinterpret_cast<const T *>(B),    \
+                        ldb, beta, reinterpret_cast<T *>(C), ldc));                             \
+    return ok_status();                                                                         \
+  }
+CLM_GEMM_API(s, float, float *, const float *)
+CLM_GEMM_API(d, double, double *, const double *)
+CLM_GEMM_API(c, float2, void *, const void *)
+CLM_GEMM_API(z, double2, void *, const void *)
+#undef CLM_GEMM_API
+
+unsigned long long calamanGetLaunchCount(void) { return g_launch_count(); }
+
+calamanStatus_t calamanSetKernelTiming(calamanHandle_t handle, int enable) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  KernelTimer &t = handle->timer;
+  t.enabled = enable != 0;
+  t.used = 0;
+  t.starts.clear();
+  t.stops.clear();
+  t.flops.clear();
+  return ok_status();
+}
+
+calamanStatus_t calamanGetKernelTiming(calamanHandle_t handle, calamanKernelTiming_t *out) {
+  if (handle == nullptr || out == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  KernelTimer &t = handle->timer;
+  out->gemm_launches = (long long)t.flops.size();
+  out->gemm_ms = 0.0;
+  out->gemm_flops = 0.0;
+  if (!t.stops.empty()) CLM_CUDA(cudaEventSynchronize(t.stops.back()));
+  for (std::size_t i = 0; i < t.flops.size(); ++i) {
+    float ms = 0.f;
+    CLM_CUDA(cudaEventElapsedTime(&ms, t.starts[i], t.stops[i]));
+    out->gemm_ms += ms;
+    out->gemm_flops += t.flops[i];
+  }
+  t.used = 0;
+  t.starts.clear();
+  t.stops.clear();
+  t.flops.clear();
+  return ok_status();
 }
 
 }  // extern "C"

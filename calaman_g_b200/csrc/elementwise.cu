@@ -207,7 +207,7 @@ cudaError_t launch_norm1(cudaStream_t s, int n, const T *A, int lda, double *d_c
   if (blocks > cap) blocks = cap;
   norm1_kernel<T><<<blocks, warps * 32, 0, s>>>(n, A, lda, d_colsum,
                                                 reinterpret_cast<unsigned long long *>(d_norm));
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T, typename R>
@@ -217,10 +217,10 @@ cudaError_t launch_colsums_then_max(cudaStream_t s, int n, const T *A, int lda, 
   int blocks = (n + warps - 1) / warps;
   if (blocks > 148 * 16) blocks = 148 * 16;
   colsum_kernel<T, R><<<blocks, warps * 32, 0, s>>>(n, A, lda, d_colsum);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launched();
   if (e != cudaSuccess) return e;
   max_inplace_kernel<R><<<1, 256, 0, s>>>(n, d_colsum);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T>
@@ -244,21 +244,21 @@ cudaError_t launch_pade_even_odd(cudaStream_t s, int n, int np, const T *P1, con
   default:
     return cudaErrorInvalidValue;
   }
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T>
 cudaError_t launch_pade_split(cudaStream_t s, int n, const T *U, const T *V, T *P, int ldp, T *Q) {
   if (n < 1) return cudaSuccess;
   pade_split_kernel<T><<<grid_2d(n, n), kRowThreads, 0, s>>>(n, U, V, P, ldp, Q);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T>
 cudaError_t launch_scale_copy(cudaStream_t s, int n, double f, const T *A, int lda, T *B, int ldb) {
   if (n < 1) return cudaSuccess;
   scale_copy_kernel<T><<<grid_2d(n, n), kRowThreads, 0, s>>>(n, f, A, lda, B, ldb);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T>
@@ -267,21 +267,21 @@ cudaError_t launch_ps_build_block(cudaStream_t s, T *B, int ldb, int n, const T 
   if (n < 1 || terms < 1) return cudaSuccess;
   ps_build_block_kernel<T><<<grid_2d(n, n), kRowThreads, 0, s>>>(B, ldb, n, A, lda, powers, stride,
                                                                   coeffs, terms);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T>
 cudaError_t launch_set_scaled_identity(cudaStream_t s, T *P, int n, int ldp, const T *d_alpha) {
   if (n < 1) return cudaSuccess;
   set_scaled_identity_kernel<T><<<grid_2d(n, n), kRowThreads, 0, s>>>(P, n, ldp, d_alpha);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename T>
 cudaError_t launch_add_scaled_identity(cudaStream_t s, T *P, int n, int ldp, const T *d_alpha) {
   if (n < 1) return cudaSuccess;
   add_scaled_identity_kernel<T><<<(n + 255) / 256, 256, 0, s>>>(P, n, ldp, d_alpha);
-  return cudaGetLastError();
+  return launched();
 }
 
 // ---- explicit instantiations ------------------------------------------------

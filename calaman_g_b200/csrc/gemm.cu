@@ -427,6 +427,25 @@ cudaError_t run_zgemm(cudaStream_t s, int M, int N, int K, double alpha, const d
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<std::uintptr_t>(p) & 15u) == 0; }
 
+// Launch through `run`, bracketed by CUDA events when a timer is active.
+template <typename F>
+cudaError_t timed_launch(cudaStream_t s, double flops, F &&run) {
+  KernelTimer *t = tl_timer;
+  note_launch();
+  if (t == nullptr) return run();
+  cudaEvent_t a = t->take(), b = t->take();
+  if (a == nullptr || b == nullptr) return run();
+  cudaEventRecord(a, s);
+  const cudaError_t e = run();
+  cudaEventRecord(b, s);
+  t->starts.push_back(a);
+  t->stops.push_back(b);
+  t->flops.push_back(flops);
+  return e;
+}
+
+inline double real_flops(int M, int N, int K) { return 2.0 * M * (double)N * K; }
+
 }  // namespace
 
 template <>
@@ -435,37 +454,45 @@ cudaError_t gemm_nn<double>(cudaStream_t s, int M, int N, int K, double alpha, c
   if (M <= 0 || N <= 0) return cudaSuccess;
   const bool v16 = aligned16(A) && aligned16(B) && (lda % 2 == 0) && (ldb % 2 == 0);
   const long long big_tiles = (long long)((M + 127) / 128) * ((N + 127) / 128);
-  if (big_tiles >= 132) {
-    return v16 ? run_dgemm<128, 128, 64, 32, 3, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
-               : run_dgemm<128, 128, 64, 32, 3, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  }
-  return v16 ? run_dgemm<64, 64, 32, 32, 4, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
-             : run_dgemm<64, 64, 32, 32, 4, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  return timed_launch(s, real_flops(M, N, K), [&] {
+    if (big_tiles >= 132) {
+      return v16 ? run_dgemm<128, 128, 64, 32, 3, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+                 : run_dgemm<128, 128, 64, 32, 3, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    }
+    return v16 ? run_dgemm<64, 64, 32, 32, 4, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+               : run_dgemm<64, 64, 32, 32, 4, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  });
 }
 
 template <>
 cudaError_t gemm_nn<double2>(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A,
                              int lda, const double2 *B, int ldb, double beta, double2 *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  return run_zgemm<64, 64, 32, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  return timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
+    return run_zgemm<64, 64, 32, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  });
 }
 
 template <>
 cudaError_t gemm_nn<float>(cudaStream_t s, int M, int N, int K, double alpha, const float *A,
                            int lda, const float *B, int ldb, double beta, float *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  dim3 grid((M + 63) / 64, (N + 63) / 64);
-  simt_gemm_nn_kernel<float><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  return cudaGetLastError();
+  return timed_launch(s, real_flops(M, N, K), [&] {
+    dim3 grid((M + 63) / 64, (N + 63) / 64);
+    simt_gemm_nn_kernel<float><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    return cudaGetLastError();
+  });
 }
 
 template <>
 cudaError_t gemm_nn<float2>(cudaStream_t s, int M, int N, int K, double alpha, const float2 *A,
                             int lda, const float2 *B, int ldb, double beta, float2 *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
-  dim3 grid((M + 63) / 64, (N + 63) / 64);
-  simt_gemm_nn_kernel<float2><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  return cudaGetLastError();
+  return timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
+    dim3 grid((M + 63) / 64, (N + 63) / 64);
+    simt_gemm_nn_kernel<float2><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    return cudaGetLastError();
+  });
 }
 
 }  // namespace clm

@@ -455,6 +455,7 @@ cudaError_t launch_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb, co
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  note_launch();
   return cudaLaunchKernelEx(&cfg, kern, n, A, lda, k, kb, rpc, sc.ipiv, sc.perm, sc.map_pos,
                             sc.map_src, sc.map_count, info);
 }
@@ -478,7 +479,7 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
   cudaError_t e = cudaMemsetAsync(info_dev, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
   iota_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, sc.perm);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = launched()) != cudaSuccess) return e;
   const int kbn = choose_kb<T>(n);
   for (int k = 0; k < n; k += kbn) {
     const int kb = (k + kbn < n) ? kbn : n - k;
@@ -492,7 +493,7 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
         return e;
       kern<<<(others + warps - 1) / warps, warps * 32, smem, s>>>(n, A, lda, k, kb, sc.map_pos,
                                                                  sc.map_src, sc.map_count);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if ((e = launched()) != cudaSuccess) return e;
     }
     const int rest = n - (k + kb);
     if (rest > 0) {
@@ -515,7 +516,7 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   {
     const int gy = nrhs < 65535 ? nrhs : 65535;
     gather_rows_kernel<T><<<dim3((n + 255) / 256, gy), 256, 0, s>>>(n, nrhs, sc.perm, B, ldb, X, ldx);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launched()) != cudaSuccess) return e;
   }
   constexpr int NB = 64;
   const int warps = 8;
@@ -528,7 +529,7 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   for (int k = 0; k < n; k += NB) {
     const int kb = (k + NB < n) ? NB : n - k;
     kl<<<blocks, warps * 32, sizeof(T) * kb * kb, s>>>(nrhs, LU, lda, k, kb, X, ldx);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launched()) != cudaSuccess) return e;
     if (k + kb < n) {
       e = gemm_nn<T>(s, n - (k + kb), nrhs, kb, -1.0, LU + (std::size_t)k * lda + (k + kb), lda,
                      X + k, ldx, 1.0, X + (k + kb), ldx);
@@ -539,7 +540,7 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   for (int k = last; k >= 0; k -= NB) {
     const int kb = (k + NB < n) ? NB : n - k;
     ku<<<blocks, warps * 32, sizeof(T) * kb * kb, s>>>(nrhs, LU, lda, k, kb, X, ldx);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = launched()) != cudaSuccess) return e;
     if (k > 0) {
       e = gemm_nn<T>(s, k, nrhs, kb, -1.0, LU + (std::size_t)k * lda, lda, X + k, ldx, 1.0, X, ldx);
       if (e != cudaSuccess) return e;

@@ -203,6 +203,39 @@ calamanStatus_t calaman_paterson_stockmeyer_d(calamanBlasHandle_t handle, int n,
                                               const double *d_A, int lda, double *d_P, int ldp,
                                               void *d_work, size_t work_bytes, int s_requested);
 
+/* ---- building blocks and instrumentation ------------------------------
+ * No counterpart in the reference's modules: calaman_G takes its matrix
+ * products from WarpWraps' wwr::gemm (cuBLAS). Exposed so callers (and the
+ * benchmark) can run the same tensor-core GEMM the path uses.
+ * C = alpha A B + beta C, no transposes, column-major, real alpha/beta; for
+ * _c/_z the pointers are interleaved complex. beta == 0 never reads C. */
+calamanStatus_t calaman_gemm_s(calamanStream_t stream, int m, int n, int k, double alpha,
+                               const float *A, int lda, const float *B, int ldb, double beta,
+                               float *C, int ldc);
+calamanStatus_t calaman_gemm_d(calamanStream_t stream, int m, int n, int k, double alpha,
+                               const double *A, int lda, const double *B, int ldb, double beta,
+                               double *C, int ldc);
+calamanStatus_t calaman_gemm_c(calamanStream_t stream, int m, int n, int k, double alpha,
+                               const void *A, int lda, const void *B, int ldb, double beta,
+                               void *C, int ldc);
+calamanStatus_t calaman_gemm_z(calamanStream_t stream, int m, int n, int k, double alpha,
+                               const void *A, int lda, const void *B, int ldb, double beta,
+                               void *C, int ldc);
+
+/* Total kernel launches this library has issued in the process. */
+unsigned long long calamanGetLaunchCount(void);
+
+/* Per-handle CUDA-event timing of the dense products (every GEMM launch the
+ * handle's calls issue, including those inside the LU and the solves).
+ * Enabling clears the record; reading synchronises on the last event. */
+typedef struct {
+  long long gemm_launches;
+  double gemm_ms;        /* summed device time of those launches */
+  double gemm_flops;     /* algorithmic flops: 2mnk real, 8mnk complex */
+} calamanKernelTiming_t;
+calamanStatus_t calamanSetKernelTiming(calamanHandle_t handle, int enable);
+calamanStatus_t calamanGetKernelTiming(calamanHandle_t handle, calamanKernelTiming_t *out);
+
 #ifdef __cplusplus
 }
 #endif
