@@ -123,6 +123,12 @@ for _suf, _real in (("s", c_float), ("d", c_double), ("c", c_float), ("z", c_dou
     SIGNATURES[f"calaman_pade_{_suf}"] = (Status, _PADE)
     SIGNATURES[f"calaman_matrix_norm1_{_suf}"] = (_real, [c_void_p, c_int, c_void_p, c_int, c_void_p])
     SIGNATURES[f"calaman_gemm_{_suf}"] = (Status, _GEMM)
+    SIGNATURES[f"calaman_getrf_{_suf}"] = (Status, [c_void_p, c_int, c_void_p, c_int, c_void_p,
+                                                   c_int_p])
+    SIGNATURES[f"calaman_getrs_{_suf}"] = (Status, [c_void_p, c_int, c_int, c_void_p, c_int,
+                                                   c_void_p, c_void_p, c_int, c_void_p, c_int,
+                                                   c_int_p])
+SIGNATURES["calaman_getrf_bufferSize"] = (Status, [c_int, c_size_t_p])
 
 _lib = None
 

@@ -628,6 +628,40 @@ CLM_GEMM_API(c, float2, void *, const void *)
 CLM_GEMM_API(z, double2, void *, const void *)
 #undef CLM_GEMM_API
 
+calamanStatus_t calaman_getrf_bufferSize(int n, size_t *bytes) {
+  if (n < 1 || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  *bytes = lu_scratch_bytes(n);
+  return ok_status();
+}
+
+#define CLM_LU_API(SUF, T, PT, CPT)                                                            \
+  calamanStatus_t calaman_getrf_##SUF(calamanStream_t stream, int n, PT A, int lda,            \
+                                      void *scratch, int *d_info) {                            \
+    if (n < 1 || n > kMaxDim || lda < n || A == nullptr || scratch == nullptr ||               \
+        d_info == nullptr)                                                                     \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                        \
+    CLM_CUDA(getrf<T>(static_cast<cudaStream_t>(stream), n, reinterpret_cast<T *>(A), lda,     \
+                      scratch, d_info));                                                       \
+    return ok_status();                                                                        \
+  }                                                                                            \
+  calamanStatus_t calaman_getrs_##SUF(calamanStream_t stream, int n, int nrhs, CPT LU,         \
+                                      int lda, const void *scratch, CPT B, int ldb, PT X,      \
+                                      int ldx, int *d_info) {                                  \
+    if (n < 1 || n > kMaxDim || nrhs < 0 || lda < n || ldb < n || ldx < n || LU == nullptr ||  \
+        scratch == nullptr || B == nullptr || X == nullptr || d_info == nullptr)               \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                        \
+    CLM_CUDA(getrs<T>(static_cast<cudaStream_t>(stream), n, nrhs,                              \
+                      reinterpret_cast<const T *>(LU), lda, scratch,                           \
+                      reinterpret_cast<const T *>(B), ldb, reinterpret_cast<T *>(X), ldx,      \
+                      d_info));                                                                \
+    return ok_status();                                                                        \
+  }
+CLM_LU_API(s, float, float *, const float *)
+CLM_LU_API(d, double, double *, const double *)
+CLM_LU_API(c, float2, void *, const void *)
+CLM_LU_API(z, double2, void *, const void *)
+#undef CLM_LU_API
+
 unsigned long long calamanGetLaunchCount(void) { return g_launch_count(); }
 
 calamanStatus_t calamanSetKernelTiming(calamanHandle_t handle, int enable) {

@@ -5,21 +5,27 @@
 //
 // Blocked right-looking factorisation, panel width kb <= 64:
 //   1. panel: one thread-block CLUSTER (<= 8 CTAs) holds the h x kb panel in
-//      the CTAs' shared memory, rows split across the CTAs. Each column costs
-//      one cluster barrier: every CTA publishes its local pivot candidate (and
-//      that candidate's whole row) into a double-buffered slot, the barrier
-//      makes the slots visible, and every CTA then reads all candidates over
-//      distributed shared memory, agrees on the global pivot (largest
-//      |Re|+|Im|, first index on ties -- LAPACK IxAMAX), swaps, scales and
-//      applies the rank-1 update to its own rows.
+//      the CTAs' shared memory, rows split across the CTAs. Per pivot column:
+//        - every CTA reduces its local pivot candidate (largest |Re|+|Im|,
+//          first index on ties -- LAPACK IxAMAX) and publishes it, with the
+//          candidate's whole row, into a double-buffered slot;
+//        - ONE cluster barrier;
+//        - every CTA fetches all candidates and their rows (and row j) over
+//          distributed shared memory in a single round trip, and agrees on
+//          the pivot without further communication;
+//        - one fused pass swaps, scales by the pivot's reciprocal (as xGETF2
+//          does above the safe minimum), applies the rank-1 update to its own
+//          rows and already forms the NEXT column's local candidate.
+//      That is two CTA barriers and one cluster barrier per column.
 //   2. swap + TRSM: one warp per column outside the panel applies the panel's
 //      row permutation (a compact gather of <= 2 kb rows) and, right of the
-//      panel, solves with the unit-lower L11 in registers.
+//      panel, solves with the unit-lower L11 held in shared memory.
 //   3. trailing update: A22 -= L21 U12 on the tensor-core GEMM.
 // The solve gathers the right-hand side through the accumulated row
 // permutation and runs blocked forward / backward substitution (diagonal
 // blocks per warp, off-diagonal blocks on the GEMM).
 #include <cooperative_groups.h>
+#include <cfloat>
 #include <climits>
 
 #include "kernels.cuh"
@@ -33,7 +39,7 @@ namespace {
 constexpr int kMaxKb = 64;
 constexpr int kPanelThreads = 512;
 constexpr int kMaxCluster = 8;
-constexpr std::size_t kPanelSmemBudget = 180 * 1024;  // bytes of panel per CTA
+constexpr std::size_t kPanelSmemBudget = 176 * 1024;  // bytes of panel per CTA
 
 // scratch: ipiv[n] | perm[n] | map_pos[2*kMaxKb] | map_src[2*kMaxKb] | map_count
 struct LuScratch {
@@ -54,8 +60,8 @@ __host__ __device__ inline std::size_t align16(std::size_t x) { return (x + 15) 
 
 // Offsets of the panel kernel's shared-memory regions (host and device agree).
 struct PanelSmem {
-  std::size_t S, slot_row, slot_diag, pivrow, oldrow, slot_val, slot_idx, red_val, red_idx, plist,
-      scal, map_pos, map_org, total;
+  std::size_t S, slot_row, slot_diag, cand, oldrow, slot_rcp, cand_rcp, slot_val, slot_idx,
+      cand_val, cand_idx, red_val, red_idx, plist, flags, map_pos, map_org, total;
 };
 template <typename T>
 __host__ __device__ inline PanelSmem panel_smem(int rpc, int kb) {
@@ -64,14 +70,18 @@ __host__ __device__ inline PanelSmem panel_smem(int rpc, int kb) {
   o.S = at; at = align16(at + sizeof(T) * (std::size_t)rpc * kb);
   o.slot_row = at; at = align16(at + sizeof(T) * 2 * kb);
   o.slot_diag = at; at = align16(at + sizeof(T) * 2 * kb);
-  o.pivrow = at; at = align16(at + sizeof(T) * kb);
+  o.cand = at; at = align16(at + sizeof(T) * kMaxCluster * kb);
   o.oldrow = at; at = align16(at + sizeof(T) * kb);
+  o.slot_rcp = at; at = align16(at + sizeof(T) * 2);
+  o.cand_rcp = at; at = align16(at + sizeof(T) * kMaxCluster);
   o.slot_val = at; at = align16(at + sizeof(double) * 2);
   o.slot_idx = at; at = align16(at + sizeof(int) * 2);
+  o.cand_val = at; at = align16(at + sizeof(double) * kMaxCluster);
+  o.cand_idx = at; at = align16(at + sizeof(int) * kMaxCluster);
   o.red_val = at; at = align16(at + sizeof(double) * (kPanelThreads / 32));
   o.red_idx = at; at = align16(at + sizeof(int) * (kPanelThreads / 32));
   o.plist = at; at = align16(at + sizeof(int) * kb);
-  o.scal = at; at = align16(at + sizeof(double) * 4);
+  o.flags = at; at = align16(at + sizeof(int) * 4);
   o.map_pos = at; at = align16(at + sizeof(int) * 2 * kb);
   o.map_org = at; at = align16(at + sizeof(int) * 2 * kb);
   o.total = at;
@@ -96,6 +106,34 @@ __device__ __forceinline__ void argmax_merge(double &v, int &i, double ov, int o
   }
 }
 
+// one element global -> shared, asynchronously (4, 8 or 16 bytes)
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (sizeof(T) == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+  } else if constexpr (sizeof(T) == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+  }
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
+}
+
+template <typename T> __device__ __forceinline__ double safe_min();
+template <> __device__ __forceinline__ double safe_min<float>() { return FLT_MIN; }
+template <> __device__ __forceinline__ double safe_min<double>() { return DBL_MIN; }
+template <> __device__ __forceinline__ double safe_min<float2>() { return FLT_MIN; }
+template <> __device__ __forceinline__ double safe_min<double2>() { return DBL_MIN; }
+
+__device__ __noinline__ void panel_finish(cg::cluster_group &cluster, int rank, int k, int kb,
+                                          const int *plist, const int *flags, int *mpos, int *morg,
+                                          int *__restrict__ ipiv, int *__restrict__ perm,
+                                          int *__restrict__ g_map_pos, int *__restrict__ g_map_src,
+                                          int *__restrict__ g_map_count, int *__restrict__ info);
+
 template <typename T>
 __global__ void __launch_bounds__(kPanelThreads)
     lu_panel_kernel(int n, T *__restrict__ A, int lda, int k, int kb, int rpc, int *__restrict__ ipiv,
@@ -105,6 +143,7 @@ __global__ void __launch_bounds__(kPanelThreads)
   const int rank = (int)cluster.block_rank();
   const int ncta = (int)cluster.num_blocks();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nt = blockDim.x;  // a multiple of 32, at most kPanelThreads
   const int h = n - k;
   const int r0 = rank * rpc;
   int rows_here = h - r0;
@@ -115,33 +154,45 @@ __global__ void __launch_bounds__(kPanelThreads)
   T *S = reinterpret_cast<T *>(smem_raw + o.S);
   T *slot_row = reinterpret_cast<T *>(smem_raw + o.slot_row);
   T *slot_diag = reinterpret_cast<T *>(smem_raw + o.slot_diag);
-  T *pivrow = reinterpret_cast<T *>(smem_raw + o.pivrow);
+  T *cand = reinterpret_cast<T *>(smem_raw + o.cand);
   T *oldrow = reinterpret_cast<T *>(smem_raw + o.oldrow);
   double *slot_val = reinterpret_cast<double *>(smem_raw + o.slot_val);
   int *slot_idx = reinterpret_cast<int *>(smem_raw + o.slot_idx);
+  double *cand_val = reinterpret_cast<double *>(smem_raw + o.cand_val);
+  int *cand_idx = reinterpret_cast<int *>(smem_raw + o.cand_idx);
   double *red_val = reinterpret_cast<double *>(smem_raw + o.red_val);
   int *red_idx = reinterpret_cast<int *>(smem_raw + o.red_idx);
   int *plist = reinterpret_cast<int *>(smem_raw + o.plist);
-  double *scal = reinterpret_cast<double *>(smem_raw + o.scal);
-  int *spiv = reinterpret_cast<int *>(scal + 2);  // [0] = p, [1] = first zero pivot
+  int *flags = reinterpret_cast<int *>(smem_raw + o.flags);  // [0] first zero pivot
 
-  // ---- stage the panel rows this CTA owns ----
-  for (int idx = tid; idx < rows_here * kb; idx += kPanelThreads) {
+  // Work split of the fused pass: ncph adjacent lanes share a row, each taking
+  // every ncph-th column, so a row's readers of column j sit in one warp and a
+  // __syncwarp orders them before column j is overwritten.
+  int ncph = 1;
+  while (ncph * 2 <= 32 && ncph * 2 * rpc <= nt) ncph *= 2;
+  const int RT = nt / ncph;  // rows covered per sweep
+  const int my_c = tid % ncph, my_r = tid / ncph;
+  const int iters = (rpc + RT - 1) / RT;  // uniform across the CTA
+
+  // ---- stage the panel rows this CTA owns (all copies in flight at once) ----
+  for (int idx = tid; idx < rows_here * kb; idx += nt) {
     const int li = idx % rows_here, c = idx / rows_here;
-    S[(std::size_t)c * rpc + li] = A[(std::size_t)(k + c) * lda + (k + r0 + li)];
+    cp_async_elem(&S[(std::size_t)c * rpc + li], &A[(std::size_t)(k + c) * lda + (k + r0 + li)]);
   }
-  if (tid == 0) spiv[1] = -1;
+  cp_async_wait_all();
+  if (tid == 0) flags[0] = -1;
   __syncthreads();
+
+  // local candidate for column 0 (the lane whose phase owns column 0)
+  double bv = -1.0;
+  int bi = INT_MAX;
+  if (my_c == 0)
+    for (int li = my_r; li < rows_here; li += RT) argmax_merge(bv, bi, abs1(S[li]), r0 + li);
 
   for (int j = 0; j < kb; ++j) {
     const int par = j & 1;
-    // ---- local pivot candidate over rows >= j ----
-    double bv = -1.0;
-    int bi = INT_MAX;
-    for (int li = tid; li < rows_here; li += kPanelThreads) {
-      const int gi = r0 + li;
-      if (gi >= j) argmax_merge(bv, bi, abs1(S[(std::size_t)j * rpc + li]), gi);
-    }
+    const int owner_j = j / rpc;
+    // ---- (1) CTA-wide candidate, published with its row ----
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
@@ -154,36 +205,8 @@ __global__ void __launch_bounds__(kPanelThreads)
     }
     __syncthreads();
     if (warp == 0) {
-      bv = lane < kPanelThreads / 32 ? red_val[lane] : -1.0;
-      bi = lane < kPanelThreads / 32 ? red_idx[lane] : INT_MAX;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        argmax_merge(bv, bi, ov, oi);
-      }
-      if (lane == 0) {
-        slot_val[par] = bv;
-        slot_idx[par] = bi;
-      }
-    }
-    __syncthreads();
-    // ---- publish the candidate's row and, if owned here, row j ----
-    if (tid < kb) {
-      const int cand = slot_idx[par];
-      if (cand != INT_MAX) slot_row[par * kb + tid] = S[(std::size_t)tid * rpc + (cand - r0)];
-      if (j >= r0 && j < r0 + rows_here) slot_diag[par * kb + tid] = S[(std::size_t)tid * rpc + (j - r0)];
-    }
-    cluster.sync();
-
-    // ---- agree on the global pivot ----
-    if (warp == 0) {
-      double v = -1.0;
-      int i = INT_MAX;
-      if (lane < ncta) {
-        v = cluster.map_shared_rank(slot_val, lane)[par];
-        i = cluster.map_shared_rank(slot_idx, lane)[par];
-      }
+      double v = lane < nt / 32 ? red_val[lane] : -1.0;
+      int i = lane < nt / 32 ? red_idx[lane] : INT_MAX;
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, v, off);
@@ -191,69 +214,152 @@ __global__ void __launch_bounds__(kPanelThreads)
         argmax_merge(v, i, ov, oi);
       }
       if (lane == 0) {
-        spiv[0] = i;
-        scal[0] = v;
+        slot_val[par] = v;
+        slot_idx[par] = i;
+      }
+      for (int c = lane; c < kb; c += 32) {
+        if (i != INT_MAX) slot_row[par * kb + c] = S[(std::size_t)c * rpc + (i - r0)];
+        if (rank == owner_j) slot_diag[par * kb + c] = S[(std::size_t)c * rpc + (j - r0)];
+      }
+    }
+    cluster.sync();
+
+    // ---- (2) one DSMEM round trip: every candidate, its row, and row j ----
+    for (int t = tid; t < ncta * kb + kb + ncta; t += nt) {
+      if (t < ncta * kb) {
+        const int q = t / kb, c = t % kb;
+        cand[q * kb + c] = cluster.map_shared_rank(slot_row, q)[par * kb + c];
+      } else if (t < ncta * kb + kb) {
+        const int c = t - ncta * kb;
+        oldrow[c] = cluster.map_shared_rank(slot_diag, owner_j)[par * kb + c];
+      } else {
+        const int q = t - ncta * kb - kb;
+        cand_val[q] = cluster.map_shared_rank(slot_val, q)[par];
+        cand_idx[q] = cluster.map_shared_rank(slot_idx, q)[par];
       }
     }
     __syncthreads();
-    const int p = spiv[0];
-    const int owner_p = p / rpc, owner_j = j / rpc;
-    if (tid < kb) {
-      pivrow[tid] = cluster.map_shared_rank(slot_row, owner_p)[par * kb + tid];
-      if (rank == owner_p && p != j)
-        oldrow[tid] = cluster.map_shared_rank(slot_diag, owner_j)[par * kb + tid];
+
+    // ---- (3) the pivot, agreed by every warp from the same data ----
+    double pv = lane < ncta ? cand_val[lane] : -1.0;
+    int p = lane < ncta ? cand_idx[lane] : INT_MAX;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {  // full butterfly: every lane ends with the winner
+      const double ov = __shfl_xor_sync(0xffffffffu, pv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, p, off);
+      argmax_merge(pv, p, ov, oi);
     }
-    __syncthreads();
-    if (tid < kb) {
-      if (rank == owner_j) S[(std::size_t)tid * rpc + (j - r0)] = pivrow[tid];
-      if (rank == owner_p && p != j) S[(std::size_t)tid * rpc + (p - r0)] = oldrow[tid];
+    if (p == INT_MAX || p < j) {  // no comparable candidate (NaN column): keep row j
+      p = j;
+      pv = 0.0;
     }
+    const T *pivrow = (p == j) ? oldrow : cand + (p / rpc) * kb;
+    const T piv = pivrow[j];
+    const bool singular = is_zero(piv);
+    const bool use_recip = abs1(piv) >= safe_min<T>();
+    const T rpiv = (use_recip && !singular) ? divide(elem<T>::one(), piv) : elem<T>::one();
+    auto scale_by_pivot = [&](T x) -> T {
+      return singular ? x : (use_recip ? mul(x, rpiv) : divide(x, piv));
+    };
     if (tid == 0) {
       plist[j] = p;
-      if (scal[0] == 0.0 && spiv[1] < 0) spiv[1] = j;
+      if (pv == 0.0 && flags[0] < 0) flags[0] = j;
     }
-    __syncthreads();
-    // ---- scale the column below the pivot ----
-    const T piv = pivrow[j];
-    if (!is_zero(piv)) {
-      for (int li = tid; li < rows_here; li += kPanelThreads)
-        if (r0 + li > j) S[(std::size_t)j * rpc + li] = divide(S[(std::size_t)j * rpc + li], piv);
-    }
-    __syncthreads();
-    // ---- rank-1 update of the columns right of j, rows below j ----
-    const int w = kb - j - 1;
-    if (w > 0 && rows_here > 0) {
-      const int total = rows_here * w;
-      for (int idx = tid; idx < total; idx += kPanelThreads) {
-        const int li = idx % rows_here;
-        const int c = j + 1 + idx / rows_here;
-        if (r0 + li > j) {
-          T &x = S[(std::size_t)c * rpc + li];
-          x = sub(x, mul(S[(std::size_t)j * rpc + li], pivrow[c]));
-        }
+
+    // ---- (4a) the two rows that move, one element per thread: position j
+    //      receives the pivot row, position p the old row j (updated) ----
+    bv = -1.0;
+    bi = INT_MAX;
+    const int nextc = j + 1;
+    const bool own_j = rank == owner_j;
+    const bool own_p = p != j && rank == p / rpc;
+    for (int t = tid; t < 2 * kb; t += nt) {
+      if (t < kb) {
+        if (own_j) S[(std::size_t)t * rpc + (j - r0)] = pivrow[t];
+      } else if (own_p) {
+        const int c = t - kb;
+        const T lp = scale_by_pivot(oldrow[j]);
+        T v;
+        if (c < j) v = oldrow[c];
+        else if (c == j) v = lp;
+        else v = sub(oldrow[c], mul(lp, pivrow[c]));
+        S[(std::size_t)c * rpc + (p - r0)] = v;
+        if (c == nextc) argmax_merge(bv, bi, abs1(v), p);
       }
     }
-    __syncthreads();
+
+    // ---- (4b) every other row below j: scale, rank-1 update, next candidate ----
+    for (int it = 0; it < iters; ++it) {
+      const int li = my_r + it * RT;
+      const int gi = r0 + li;
+      const bool row_ok = li < rows_here && gi > j && gi != p;
+      T xj = elem<T>::zero();
+      if (row_ok) xj = S[(std::size_t)j * rpc + li];
+      __syncwarp();  // every lane of this row has read column j
+      if (!row_ok) continue;
+      T *row = S + li;
+      const T l = scale_by_pivot(xj);
+      // first column >= j in this lane's phase (ncph is a power of two)
+      int c = j + ((my_c - j) & (ncph - 1));
+      if (c == j) {
+        row[(std::size_t)j * rpc] = l;
+        c += ncph;
+      }
+      // four columns at a time, all loads issued before the stores
+      for (; c < kb; c += 4 * ncph) {
+        T x[4], pr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int cc = c + u * ncph;
+          if (cc < kb) {
+            x[u] = row[(std::size_t)cc * rpc];
+            pr[u] = pivrow[cc];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int cc = c + u * ncph;
+          if (cc < kb) row[(std::size_t)cc * rpc] = sub(x[u], mul(l, pr[u]));
+        }
+      }
+      // this lane's share of the next column's candidate
+      if (nextc < kb && ((nextc - my_c) & (ncph - 1)) == 0)
+        argmax_merge(bv, bi, abs1(row[(std::size_t)nextc * rpc]), gi);
+    }
   }
 
   // ---- write the factored panel back ----
-  for (int idx = tid; idx < rows_here * kb; idx += kPanelThreads) {
+  __syncthreads();
+  for (int idx = tid; idx < rows_here * kb; idx += nt) {
     const int li = idx % rows_here, c = idx / rows_here;
     A[(std::size_t)(k + c) * lda + (k + r0 + li)] = S[(std::size_t)c * rpc + li];
   }
 
+  panel_finish(cluster, rank, k, kb, plist, flags, reinterpret_cast<int *>(smem_raw + o.map_pos),
+               reinterpret_cast<int *>(smem_raw + o.map_org), ipiv, perm, g_map_pos, g_map_src,
+               g_map_count, info);
+}
+
+// Epilogue shared by both panel kernels: the pivot vector, LAPACK's info, the
+// compact row map the swap kernel replays, and the accumulated permutation.
+// Ends with the cluster barrier that keeps every CTA's shared memory alive
+// until the last remote read of it has completed.
+__device__ __noinline__ void panel_finish(cg::cluster_group &cluster, int rank, int k, int kb,
+                                          const int *plist, const int *flags, int *mpos, int *morg,
+                                          int *__restrict__ ipiv, int *__restrict__ perm,
+                                          int *__restrict__ g_map_pos, int *__restrict__ g_map_src,
+                                          int *__restrict__ g_map_count, int *__restrict__ info) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (rank != 0) {
-    cluster.sync();  // keep every CTA's shared memory alive until rank 0 is done reading
+    cluster.sync();
     return;
   }
   if (tid < kb) ipiv[k + tid] = k + plist[tid];
-  if (tid == 0 && spiv[1] >= 0 && info[0] == 0) info[0] = k + spiv[1] + 1;
+  if (tid == 0 && flags[0] >= 0 && info[0] == 0) info[0] = k + flags[0] + 1;
 
   // ---- compact row map of the panel's swaps (warp 0 of rank 0) ----
   // entries 0..kb-1 are rows k..k+kb-1 in order; extra rows the swaps reached
   // are appended. After replaying the swaps, row pos[e] holds old row org[e].
-  int *mpos = reinterpret_cast<int *>(smem_raw + o.map_pos);
-  int *morg = reinterpret_cast<int *>(smem_raw + o.map_org);
   if (warp == 0) {
     for (int e = lane; e < kb; e += 32) {
       mpos[e] = k + e;
@@ -314,6 +420,224 @@ __global__ void __launch_bounds__(kPanelThreads)
   cluster.sync();
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident panel: the algorithm of lu_panel_kernel with each row of
+// the panel held in the registers of NCPH adjacent lanes (lane phase q keeps
+// columns q, q + NCPH, ...), so the rank-1 update costs no shared-memory
+// traffic; only the pivot row is broadcast from shared memory. The CTA whose
+// candidate wins already publishes the pivot's reciprocal with the row, so
+// the division is done once, by one thread, while the row is being copied.
+// Used when the rows of a CTA fit its NT / NCPH lanes.
+// ---------------------------------------------------------------------------
+template <typename T, int KB, int NCPH, int NT>
+__global__ void __launch_bounds__(NT)
+    lu_panel_reg_kernel(int n, T *__restrict__ A, int lda, int k, int kb, int rpc,
+                        int *__restrict__ ipiv, int *__restrict__ perm, int *__restrict__ g_map_pos,
+                        int *__restrict__ g_map_src, int *__restrict__ g_map_count,
+                        int *__restrict__ info) {
+  constexpr int CPL = KB / NCPH;  // columns per lane
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int ncta = (int)cluster.num_blocks();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int h = n - k;
+  const int r0 = rank * rpc;
+  int rows_here = h - r0;
+  rows_here = rows_here < 0 ? 0 : (rows_here > rpc ? rpc : rows_here);
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const PanelSmem o = panel_smem<T>(0, KB);
+  T *slot_row = reinterpret_cast<T *>(smem_raw + o.slot_row);    // [2][KB]
+  T *slot_diag = reinterpret_cast<T *>(smem_raw + o.slot_diag);  // [2][KB]
+  T *cand = reinterpret_cast<T *>(smem_raw + o.cand);            // [kMaxCluster][KB]
+  T *oldrow = reinterpret_cast<T *>(smem_raw + o.oldrow);
+  T *slot_rcp = reinterpret_cast<T *>(smem_raw + o.slot_rcp);
+  T *cand_rcp = reinterpret_cast<T *>(smem_raw + o.cand_rcp);
+  double *slot_val = reinterpret_cast<double *>(smem_raw + o.slot_val);
+  int *slot_idx = reinterpret_cast<int *>(smem_raw + o.slot_idx);
+  double *cand_val = reinterpret_cast<double *>(smem_raw + o.cand_val);
+  int *cand_idx = reinterpret_cast<int *>(smem_raw + o.cand_idx);
+  double *red_val = reinterpret_cast<double *>(smem_raw + o.red_val);
+  int *red_idx = reinterpret_cast<int *>(smem_raw + o.red_idx);
+  int *plist = reinterpret_cast<int *>(smem_raw + o.plist);
+  int *flags = reinterpret_cast<int *>(smem_raw + o.flags);
+
+  const int phase = tid % NCPH;
+  const int li = tid / NCPH;  // this lane's row within the CTA
+  const bool has_row = li < rows_here;
+  const int gi = r0 + li;     // panel-relative row
+  const int group0 = lane & ~(NCPH - 1);
+
+  // ---- stage: this lane's columns of its row ----
+  T r[CPL];
+#pragma unroll
+  for (int u = 0; u < CPL; ++u) {
+    const int c = phase + u * NCPH;
+    r[u] = (has_row && c < kb) ? A[(std::size_t)(k + c) * lda + (k + gi)] : elem<T>::zero();
+  }
+  if (tid == 0) flags[0] = -1;
+
+  // candidate for column 0: the phase-0 lane of every row
+  double bv = -1.0;
+  int bi = INT_MAX;
+  if (has_row && phase == 0) argmax_merge(bv, bi, abs1(r[0]), gi);
+
+  for (int j = 0; j < kb; ++j) {
+    const int par = j & 1;
+    const int owner_j = j / rpc;
+    const int jphase = j % NCPH, ju = j / NCPH;
+    // ---- (1) CTA-wide candidate; the lanes holding it publish its row ----
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      argmax_merge(bv, bi, ov, oi);
+    }
+    if (lane == 0) {
+      red_val[warp] = bv;
+      red_idx[warp] = bi;
+    }
+    __syncthreads();
+    double cv = lane < nwarps ? red_val[lane] : -1.0;
+    int ci = lane < nwarps ? red_idx[lane] : INT_MAX;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, cv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, ci, off);
+      argmax_merge(cv, ci, ov, oi);
+    }
+    if (tid == 0) {
+      slot_val[par] = cv;
+      slot_idx[par] = ci;
+    }
+    if (has_row && (gi == ci || gi == j)) {
+#pragma unroll
+      for (int u = 0; u < CPL; ++u) {
+        const int c = phase + u * NCPH;
+        if (c < kb) {
+          if (gi == ci) slot_row[par * KB + c] = r[u];
+          if (gi == j) slot_diag[par * KB + c] = r[u];
+        }
+      }
+      if (gi == ci && phase == jphase) {  // one division per column, off the other lanes' path
+        T x = elem<T>::zero();
+#pragma unroll
+        for (int u = 0; u < CPL; ++u)
+          if (u == ju) x = r[u];
+        slot_rcp[par] = is_zero(x) ? elem<T>::one() : divide(elem<T>::one(), x);
+      }
+    }
+    cluster.sync();
+
+    // ---- (2) one DSMEM round trip: every candidate, its row, and row j ----
+    for (int t = tid; t < (kMaxCluster + 1) * KB + kMaxCluster; t += blockDim.x) {
+      if (t < kMaxCluster * KB) {
+        const int q = t / KB, c = t % KB;  // KB is a power of two
+        if (q < ncta && c < kb) cand[q * KB + c] = cluster.map_shared_rank(slot_row, q)[par * KB + c];
+      } else if (t < (kMaxCluster + 1) * KB) {
+        const int c = t - kMaxCluster * KB;
+        if (c < kb) oldrow[c] = cluster.map_shared_rank(slot_diag, owner_j)[par * KB + c];
+      } else {
+        const int q = t - (kMaxCluster + 1) * KB;
+        if (q < ncta) {
+          cand_val[q] = cluster.map_shared_rank(slot_val, q)[par];
+          cand_idx[q] = cluster.map_shared_rank(slot_idx, q)[par];
+          cand_rcp[q] = cluster.map_shared_rank(slot_rcp, q)[par];
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- (3) the pivot ----
+    double pv = lane < ncta ? cand_val[lane] : -1.0;
+    int p = lane < ncta ? cand_idx[lane] : INT_MAX;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, pv, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, p, off);
+      argmax_merge(pv, p, ov, oi);
+    }
+    bool forced = false;
+    if (p == INT_MAX || p < j) {  // no comparable candidate (NaN column): keep row j
+      p = j;
+      pv = 0.0;
+      forced = true;
+    }
+    const int powner = p / rpc;
+    const T *pivrow = (p == j) ? oldrow : cand + powner * KB;
+    const T piv = pivrow[j];
+    const bool singular = forced || is_zero(piv);
+    const bool use_recip = abs1(piv) >= safe_min<T>();
+    const T rpiv = cand_rcp[powner];
+    if (tid == 0) {
+      plist[j] = p;
+      if (pv == 0.0 && flags[0] < 0) flags[0] = j;
+    }
+
+    // ---- (4) swap, scale, rank-1 update, next candidate: all in registers ----
+    T xj_mine = elem<T>::zero();
+#pragma unroll
+    for (int u = 0; u < CPL; ++u)
+      if (u == ju) xj_mine = r[u];
+    T xj = shfl(xj_mine, group0 + jphase);
+    bv = -1.0;
+    bi = INT_MAX;
+    if (has_row && gi >= j) {
+      if (gi == j) {  // position j receives the pivot row
+#pragma unroll
+        for (int u = 0; u < CPL; ++u) {
+          const int c = phase + u * NCPH;
+          if (c < kb) r[u] = pivrow[c];
+        }
+      } else {
+        if (gi == p) {  // position p receives the old row j
+          xj = oldrow[j];
+#pragma unroll
+          for (int u = 0; u < CPL; ++u) {
+            const int c = phase + u * NCPH;
+            if (c < kb) r[u] = oldrow[c];
+          }
+        }
+        const T l = singular ? xj : (use_recip ? mul(xj, rpiv) : divide(xj, piv));
+#pragma unroll
+        for (int u = 0; u < CPL; ++u) {
+          const int c = phase + u * NCPH;
+          if (c == j) r[u] = l;
+          else if (c > j && c < kb) r[u] = sub(r[u], mul(l, pivrow[c]));
+        }
+        if (j + 1 < kb && phase == (j + 1) % NCPH) {
+          const int nu = (j + 1) / NCPH;
+          T xn = elem<T>::zero();
+#pragma unroll
+          for (int u = 0; u < CPL; ++u)
+            if (u == nu) xn = r[u];
+          argmax_merge(bv, bi, abs1(xn), gi);
+        }
+      }
+    }
+  }
+
+  // ---- write the factored panel back ----
+#pragma unroll
+  for (int u = 0; u < CPL; ++u) {
+    const int c = phase + u * NCPH;
+    if (has_row && c < kb) A[(std::size_t)(k + c) * lda + (k + gi)] = r[u];
+  }
+  __syncthreads();
+  panel_finish(cluster, rank, k, kb, plist, flags, reinterpret_cast<int *>(smem_raw + o.map_pos),
+               reinterpret_cast<int *>(smem_raw + o.map_org), ipiv, perm, g_map_pos, g_map_src,
+               g_map_count, info);
+}
+
+// Load the kb x kb diagonal block A[k:k+kb, k:k+kb] into shared memory.
+template <typename T>
+__device__ __forceinline__ void load_diag_block(T *D, const T *A, int lda, int k, int kb) {
+  for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x)
+    cp_async_elem(&D[idx], &A[(std::size_t)(k + idx / kb) * lda + (k + idx % kb)]);
+  cp_async_wait_all();
+}
+
 // ---- swap + TRSM for the columns outside the panel: one warp per column ----
 template <typename T>
 __global__ void __launch_bounds__(256)
@@ -326,10 +650,7 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x & 31;
   const int ci = blockIdx.x * warps + (threadIdx.x >> 5);
   const bool block_needs_L = (int)(blockIdx.x + 1) * warps > k;  // holds a right-of-panel column
-  if (block_needs_L) {
-    for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x)
-      L[idx] = A[(std::size_t)(k + idx / kb) * lda + (k + idx % kb)];
-  }
+  if (block_needs_L) load_diag_block(L, A, lda, k, kb);
   __syncthreads();
   if (ci >= n - kb) return;
   const int c = ci < k ? ci : ci + kb;
@@ -382,15 +703,21 @@ __global__ void gather_rows_kernel(int n, int nrhs, const int *__restrict__ perm
 }
 
 // Diagonal-block triangular solve on rows [k, k+kb) of X, one warp per RHS
-// column. LOWER: unit lower (forward); else non-unit upper (backward).
+// column. LOWER: unit lower (forward); else non-unit upper (backward), whose
+// diagonal reciprocals are formed once per block, off the dependent chain.
 template <typename T, bool LOWER>
 __global__ void __launch_bounds__(256)
     trsm_diag_kernel(int nrhs, const T *__restrict__ LU, int lda, int k, int kb, T *__restrict__ X,
                      int ldx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *D = reinterpret_cast<T *>(smem_raw);
-  for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x)
-    D[idx] = LU[(std::size_t)(k + idx / kb) * lda + (k + idx % kb)];
+  T *rdiag = D + kb * kb;
+  load_diag_block(D, LU, lda, k, kb);
+  __syncthreads();
+  if (!LOWER && threadIdx.x < kb) {
+    const T d = D[threadIdx.x * kb + threadIdx.x];
+    rdiag[threadIdx.x] = divide(elem<T>::one(), d);
+  }
   __syncthreads();
   const int warps = blockDim.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -407,12 +734,9 @@ __global__ void __launch_bounds__(256)
     }
   } else {
     for (int l = kb - 1; l >= 0; --l) {
-      if (l < 32) {
-        if (lane == l) x0 = divide(x0, D[l * kb + l]);
-      } else {
-        if (lane + 32 == l) x1 = divide(x1, D[l * kb + l]);
-      }
-      const T xl = shfl(l < 32 ? x0 : x1, l & 31);
+      const T xl = mul(shfl(l < 32 ? x0 : x1, l & 31), rdiag[l]);
+      if (lane == l) x0 = xl;
+      if (lane + 32 == l) x1 = xl;
       if (lane < l) x0 = sub(x0, mul(D[l * kb + lane], xl));
       if (lane + 32 < l) x1 = sub(x1, mul(D[l * kb + lane + 32], xl));
     }
@@ -421,20 +745,84 @@ __global__ void __launch_bounds__(256)
   if (lane + 32 < kb) col[lane + 32] = x1;
 }
 
+// Register-panel configurations: KB columns, NCPH lanes per row, NT threads
+// per CTA (so NT / NCPH rows per CTA). Each lane keeps KB / NCPH elements,
+// 64 (RegPanel) or 128 (RegPanelWide, more rows per CTA) 32-bit registers.
+template <typename T> struct RegPanel;
+template <> struct RegPanel<double2> { static constexpr int KB = 32, NCPH = 4, NT = 512, kRows = NT / NCPH; };
+template <> struct RegPanel<double> { static constexpr int KB = 64, NCPH = 4, NT = 512, kRows = NT / NCPH; };
+template <> struct RegPanel<float2> { static constexpr int KB = 64, NCPH = 4, NT = 512, kRows = NT / NCPH; };
+template <> struct RegPanel<float> { static constexpr int KB = 64, NCPH = 2, NT = 512, kRows = NT / NCPH; };
+template <typename T> struct RegPanelWide;
+template <> struct RegPanelWide<double2> { static constexpr int KB = 32, NCPH = 1, NT = 256, kRows = NT / NCPH; };
+template <> struct RegPanelWide<double> { static constexpr int KB = 64, NCPH = 1, NT = 256, kRows = NT / NCPH; };
+template <> struct RegPanelWide<float2> { static constexpr int KB = 64, NCPH = 1, NT = 256, kRows = NT / NCPH; };
+template <> struct RegPanelWide<float> { static constexpr int KB = 64, NCPH = 1, NT = 512, kRows = NT / NCPH; };
+
+// Panel width of the outer blocking: complex128 panels are 32 wide so a row's
+// register share stays at 64 registers.
+template <typename T> constexpr int panel_width() { return RegPanel<T>::KB; }
+
 // Panel width for an n x n factorisation: the widest kb <= 64 whose full-height
 // panel fits in kMaxCluster CTAs' shared memory.
 template <typename T>
 int choose_kb(int n) {
-  int kb = kMaxKb;
+  int kb = panel_width<T>();
   while (kb > 1 && (std::size_t)n * kb * sizeof(T) > kPanelSmemBudget * kMaxCluster) kb /= 2;
   return kb;
+}
+
+
+inline cudaLaunchAttribute cluster_attr(int ncta) {
+  cudaLaunchAttribute a;
+  a.id = cudaLaunchAttributeClusterDimension;
+  a.val.clusterDim.x = ncta;
+  a.val.clusterDim.y = 1;
+  a.val.clusterDim.z = 1;
+  return a;
+}
+
+template <typename T, int KB, int NCPH, int NT>
+cudaError_t launch_reg_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb, const LuScratch &sc,
+                             int *info) {
+  constexpr int kRows = NT / NCPH;
+  const int h = n - k;
+  const int ncta = (h + kRows - 1) / kRows;
+  const int rpc = (h + ncta - 1) / ncta;
+  const PanelSmem o = panel_smem<T>(0, KB);
+  auto kern = lu_panel_reg_kernel<T, KB, NCPH, NT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o.total);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ncta, 1, 1);
+  int nt = ((rpc * NCPH + 31) / 32) * 32;
+  if (nt < 64) nt = 64;
+  cfg.blockDim = dim3(nt, 1, 1);
+  cfg.dynamicSmemBytes = o.total;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1] = {cluster_attr(ncta)};
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, kern, n, A, lda, k, kb, rpc, sc.ipiv, sc.perm, sc.map_pos,
+                            sc.map_src, sc.map_count, info);
 }
 
 template <typename T>
 cudaError_t launch_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb, const LuScratch &sc,
                          int *info) {
   const int h = n - k;
+  if (kb <= RegPanel<T>::KB && h <= kMaxCluster * RegPanel<T>::kRows) {
+    return launch_reg_panel<T, RegPanel<T>::KB, RegPanel<T>::NCPH, RegPanel<T>::NT>(s, n, A, lda, k, kb, sc, info);
+  }
+  if (kb <= RegPanel<T>::KB && h <= kMaxCluster * RegPanelWide<T>::kRows) {
+    return launch_reg_panel<T, RegPanelWide<T>::KB, RegPanelWide<T>::NCPH, RegPanelWide<T>::NT>(s, n, A, lda, k, kb, sc, info);
+  }
+  // enough CTAs for the panel to fit, and for every row to get >= 2 lanes of
+  // the fused pass when the cluster allows it (<= 256 rows per CTA)
   int ncta = (int)(((std::size_t)h * kb * sizeof(T) + kPanelSmemBudget - 1) / kPanelSmemBudget);
+  const int by_rows = (h + 255) / 256;
+  if (ncta < by_rows) ncta = by_rows;
   if (ncta < 1) ncta = 1;
   if (ncta > kMaxCluster) ncta = kMaxCluster;
   if (ncta > h) ncta = h;
@@ -445,7 +833,13 @@ cudaError_t launch_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb, co
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ncta, 1, 1);
-  cfg.blockDim = dim3(kPanelThreads, 1, 1);
+  // threads: enough lanes for every row x column phase, in whole warps
+  int ncph = 1;
+  while (ncph * 2 <= 32 && ncph * 2 * rpc <= kPanelThreads) ncph *= 2;
+  int nt = ((rpc * ncph + 31) / 32) * 32;
+  if (nt > kPanelThreads) nt = kPanelThreads;
+  if (nt < 64) nt = 64;
+  cfg.blockDim = dim3(nt, 1, 1);
   cfg.dynamicSmemBytes = o.total;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
@@ -481,18 +875,19 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
   iota_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, sc.perm);
   if ((e = launched()) != cudaSuccess) return e;
   const int kbn = choose_kb<T>(n);
+  auto swap_kern = lu_swap_trsm_kernel<T>;
+  const std::size_t swap_smem = sizeof(T) * (std::size_t)kbn * kbn;
+  if ((e = cudaFuncSetAttribute(swap_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)swap_smem)) !=
+      cudaSuccess)
+    return e;
   for (int k = 0; k < n; k += kbn) {
     const int kb = (k + kbn < n) ? kbn : n - k;
     if ((e = launch_panel<T>(s, n, A, lda, k, kb, sc, info_dev)) != cudaSuccess) return e;
     const int others = n - kb;
     if (others > 0) {
       const int warps = 8;
-      const std::size_t smem = sizeof(T) * (std::size_t)kb * kb;
-      auto kern = lu_swap_trsm_kernel<T>;
-      if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-        return e;
-      kern<<<(others + warps - 1) / warps, warps * 32, smem, s>>>(n, A, lda, k, kb, sc.map_pos,
-                                                                 sc.map_src, sc.map_count);
+      swap_kern<<<(others + warps - 1) / warps, warps * 32, sizeof(T) * (std::size_t)kb * kb, s>>>(
+          n, A, lda, k, kb, sc.map_pos, sc.map_src, sc.map_count);
       if ((e = launched()) != cudaSuccess) return e;
     }
     const int rest = n - (k + kb);
@@ -520,7 +915,7 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   }
   constexpr int NB = 64;
   const int warps = 8;
-  const std::size_t smem = sizeof(T) * NB * NB;
+  const std::size_t smem = sizeof(T) * (NB * NB + NB);
   auto kl = trsm_diag_kernel<T, true>;
   auto ku = trsm_diag_kernel<T, false>;
   if ((e = cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
@@ -528,7 +923,7 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   const int blocks = (nrhs + warps - 1) / warps;
   for (int k = 0; k < n; k += NB) {
     const int kb = (k + NB < n) ? NB : n - k;
-    kl<<<blocks, warps * 32, sizeof(T) * kb * kb, s>>>(nrhs, LU, lda, k, kb, X, ldx);
+    kl<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, kb, X, ldx);
     if ((e = launched()) != cudaSuccess) return e;
     if (k + kb < n) {
       e = gemm_nn<T>(s, n - (k + kb), nrhs, kb, -1.0, LU + (std::size_t)k * lda + (k + kb), lda,
@@ -539,7 +934,7 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   const int last = ((n - 1) / NB) * NB;
   for (int k = last; k >= 0; k -= NB) {
     const int kb = (k + NB < n) ? NB : n - k;
-    ku<<<blocks, warps * 32, sizeof(T) * kb * kb, s>>>(nrhs, LU, lda, k, kb, X, ldx);
+    ku<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, kb, X, ldx);
     if ((e = launched()) != cudaSuccess) return e;
     if (k > 0) {
       e = gemm_nn<T>(s, k, nrhs, kb, -1.0, LU + (std::size_t)k * lda, lda, X + k, ldx, 1.0, X, ldx);

@@ -222,6 +222,35 @@ calamanStatus_t calaman_gemm_z(calamanStream_t stream, int m, int n, int k, doub
                                const void *A, int lda, const void *B, int ldb, double beta,
                                void *C, int ldc);
 
+/* LU with partial pivoting and the n-right-hand-side solve that pade() runs on
+ * q_m(A) (the reference calls the solver library's getrf/getrs through
+ * WarpWraps, src/expm/pade.cppm:186-188). LAPACK semantics: P A = L U, pivot
+ * = first entry of largest |Re|+|Im|. `scratch` is calaman_getrf_bufferSize
+ * device bytes; it begins with the n pivot rows (0-based, int) and must be
+ * passed unchanged to getrs. getrs reads B and writes X (no aliasing).
+ * d_info: getrf writes the first zero pivot (1-based) or 0; getrs writes 0. */
+calamanStatus_t calaman_getrf_bufferSize(int n, size_t *bytes);
+calamanStatus_t calaman_getrf_s(calamanStream_t stream, int n, float *A, int lda, void *scratch,
+                                int *d_info);
+calamanStatus_t calaman_getrf_d(calamanStream_t stream, int n, double *A, int lda, void *scratch,
+                                int *d_info);
+calamanStatus_t calaman_getrf_c(calamanStream_t stream, int n, void *A, int lda, void *scratch,
+                                int *d_info);
+calamanStatus_t calaman_getrf_z(calamanStream_t stream, int n, void *A, int lda, void *scratch,
+                                int *d_info);
+calamanStatus_t calaman_getrs_s(calamanStream_t stream, int n, int nrhs, const float *LU, int lda,
+                                const void *scratch, const float *B, int ldb, float *X, int ldx,
+                                int *d_info);
+calamanStatus_t calaman_getrs_d(calamanStream_t stream, int n, int nrhs, const double *LU, int lda,
+                                const void *scratch, const double *B, int ldb, double *X, int ldx,
+                                int *d_info);
+calamanStatus_t calaman_getrs_c(calamanStream_t stream, int n, int nrhs, const void *LU, int lda,
+                                const void *scratch, const void *B, int ldb, void *X, int ldx,
+                                int *d_info);
+calamanStatus_t calaman_getrs_z(calamanStream_t stream, int n, int nrhs, const void *LU, int lda,
+                                const void *scratch, const void *B, int ldb, void *X, int ldx,
+                                int *d_info);
+
 /* Total kernel launches this library has issued in the process. */
 unsigned long long calamanGetLaunchCount(void);
 
