@@ -129,6 +129,10 @@ for _suf, _real in (("s", c_float), ("d", c_double), ("c", c_float), ("z", c_dou
                                                    c_void_p, c_void_p, c_int, c_void_p, c_int,
                                                    c_int_p])
 SIGNATURES["calaman_getrf_bufferSize"] = (Status, [c_int, c_size_t_p])
+SIGNATURES["calaman_gemm_bf16x_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_size_t_p])
+SIGNATURES["calaman_gemm_bf16x_s"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
+SIGNATURES["calamanSetFloatSplit"] = (Status, [_H, c_int])
+SIGNATURES["calamanGetFloatSplit"] = (Status, [_H, c_int_p])
 
 _lib = None
 

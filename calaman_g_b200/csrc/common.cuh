@@ -217,6 +217,21 @@ struct TimerScope {
   ~TimerScope() { tl_timer = saved; }
 };
 
+// Device scratch for the split-BF16 tensor-core FP32 GEMM, lent by a driver
+// for the duration of one call (the FP32 products inside the LU and the solves
+// included). Without it, FP32 products take the SIMT kernel.
+struct GemmScratch {
+  void *ptr = nullptr;
+  std::size_t bytes = 0;
+  int terms = 6;  // 3 or 6 bf16 part products
+};
+extern thread_local GemmScratch *tl_gemm_scratch;
+struct GemmScratchScope {
+  GemmScratch *saved;
+  explicit GemmScratchScope(GemmScratch *g) : saved(tl_gemm_scratch) { tl_gemm_scratch = g; }
+  ~GemmScratchScope() { tl_gemm_scratch = saved; }
+};
+
 }  // namespace clm
 
 // The opaque handle behind calamanHandle_t.
@@ -226,5 +241,6 @@ struct calamanContext {
   int device = 0;
   int sm_count = 0;
   double *h_pinned = nullptr;  // pinned host slots for the 1-norm readback
+  int split_terms = 6;         // bf16 part products per FP32 product (3 or 6)
   clm::KernelTimer timer;
 };

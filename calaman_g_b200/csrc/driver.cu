@@ -18,6 +18,7 @@ unsigned long long g_launch_count();
 namespace {
 
 inline KernelTimer *timer_of(calamanHandle_t h) { return h ? &h->timer : nullptr; }
+inline int split_terms_of(calamanHandle_t h) { return h ? h->split_terms : 6; }
 
 constexpr int kMaxDim = 46340;  // flat int indexing bound, src/expm/detail.cppm:25-28
 
@@ -95,14 +96,23 @@ calamanExpmPlan_t plan_for(R norm1) {
 }
 
 // ---- workspaces --------------------------------------------------------
-// pade(): [P0 .. P_{np-1} | X (m = 13) | V | W | LU scratch], all 256-aligned.
-// P0 doubles as U = A W and then as the numerator p = V + U; V becomes the
-// denominator q = V - U and is factored in place (src/expm/detail.cppm:47-98).
+// FP32 products run as split-BF16 tensor-core GEMMs and need operand-part
+// scratch sized for the largest (n x n x n) product of the evaluation.
+template <typename T> std::size_t tc_scratch_bytes(int n) {
+  return std::is_same<T, float>::value ? tc_gemm_workspace_bytes(n, n, n, 6) : 0;
+}
+
+// pade(): [P0 .. P_{np-1} | X (m = 13) | V | W | LU scratch | (FP32: tensor-core
+// operand parts)], all 256-aligned. P0 doubles as U = A W and then as the
+// numerator p = V + U; V becomes the denominator q = V - U and is factored in
+// place (src/expm/detail.cppm:47-98).
 template <typename T>
 struct PadeWs {
   T *P[4] = {nullptr, nullptr, nullptr, nullptr};
   T *X = nullptr, *V = nullptr, *W = nullptr;
   void *lu = nullptr;
+  void *tc = nullptr;
+  std::size_t tc_bytes = 0;
   std::size_t carve(void *base, int n, int m) {
     Layout L(base);
     const std::size_t nn = (std::size_t)n * n;
@@ -112,22 +122,34 @@ struct PadeWs {
     V = L.take<T>(nn);
     W = L.take<T>(nn);
     lu = L.take<char>(lu_scratch_bytes(n));
+    tc_bytes = tc_scratch_bytes<T>(n);
+    if (tc_bytes) tc = L.take<char>(tc_bytes);
     return L.used;
   }
 };
 
-// expm(): [As (also the squaring scratch) | colsum | norm | pade region]
+// The FP64 twin of a single-precision element type: the single tiers run
+// their final squarings in FP64.
+template <typename T> struct Wide { using type = T; };
+template <> struct Wide<float> { using type = double; };
+template <> struct Wide<float2> { using type = double2; };
+
+// expm(): [As (also the squaring scratch) | colsum | norm | (single tiers: two
+// FP64 n x n squaring buffers) | pade region]
 template <typename T>
 struct ExpmWs {
+  using W = typename Wide<T>::type;
   T *As = nullptr;
   double *colsum = nullptr;
   double *norm = nullptr;
+  W *wide = nullptr;
   void *pade = nullptr;
   std::size_t carve(void *base, int n) {
     Layout L(base);
     As = L.take<T>((std::size_t)n * n);
     colsum = L.take<double>(n);
     norm = L.take<double>(1);
+    if (elem<T>::single) wide = L.take<W>(2 * (std::size_t)n * n);
     pade = L.cursor();
     return L.used;
   }
@@ -164,10 +186,15 @@ struct PointerModeScope {  // save / force host / restore, src/expm/expm.cppm:10
 // ---- pade<T>, src/expm/pade.cppm:77-191 -------------------------------------
 template <typename T>
 calamanStatus_t pade_run(cudaStream_t st, int m, int n, const T *A, int lda, T *R, int ldr,
-                         void *work, int *d_info) {
+                         void *work, int *d_info, int split_terms) {
   const double *b = pade_coeffs(m);
   PadeWs<T> ws;
   ws.carve(work, n, m);
+  GemmScratch gs;
+  gs.ptr = ws.tc;
+  gs.bytes = ws.tc_bytes;
+  gs.terms = split_terms;
+  GemmScratchScope gss(ws.tc ? &gs : nullptr);
   const int np = pade_num_powers(m);
   auto mm = [&](const T *X, int ldx, const T *Y, int ldy, double beta, T *Z) {
     return gemm_nn<T>(st, n, n, n, 1.0, X, ldx, Y, ldy, beta, Z, n);
@@ -214,7 +241,8 @@ calamanStatus_t pade_api(calamanHandle_t blas, calamanStream_t stream, int m, in
   if (A == nullptr || R == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   PointerModeScope pm(blas);
   TimerScope ts(timer_of(blas));
-  return pade_run<T>(static_cast<cudaStream_t>(stream), m, n, A, lda, R, ldr, work, d_info);
+  return pade_run<T>(static_cast<cudaStream_t>(stream), m, n, A, lda, R, ldr, work, d_info,
+                     split_terms_of(blas));
 }
 
 // ---- expm<T>, src/expm/expm.cppm:87-174 -------------------------------------
@@ -252,7 +280,20 @@ calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, co
     src = ws.As;
     ld_src = n;
   }
-  CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info));
+  CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info, split_terms_of(blas)));
+
+  if (elem<T>::single && chosen.s > 0) {
+    // single tiers: the squarings, where errors grow, run in FP64 tensor cores
+    using W = typename Wide<T>::type;
+    W *cw = ws.wide, *ow = ws.wide + (std::size_t)n * n;
+    CLM_CUDA((launch_convert<T, W>(st, n, E, lde, cw, n)));
+    for (int k = 0; k < chosen.s; ++k) {
+      CLM_CUDA(gemm_nn<W>(st, n, n, n, 1.0, cw, n, cw, n, 0.0, ow, n));
+      std::swap(cw, ow);
+    }
+    CLM_CUDA((launch_convert<W, T>(st, n, cw, n, E, lde)));
+    return ok_status();
+  }
 
   // square s times, ping-ponging between the output and the scratch
   T *cur = E, *other = ws.As;
@@ -416,6 +457,7 @@ void note_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed
 unsigned long long g_launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 thread_local KernelTimer *tl_timer = nullptr;
+thread_local GemmScratch *tl_gemm_scratch = nullptr;
 
 cudaEvent_t KernelTimer::take() {
   if (used < pool.size()) return pool[used++];
@@ -627,6 +669,42 @@ CLM_GEMM_API(d, double, double *, const double *)
 CLM_GEMM_API(c, float2, void *, const void *)
 CLM_GEMM_API(z, double2, void *, const void *)
 #undef CLM_GEMM_API
+
+calamanStatus_t calamanSetFloatSplit(calamanHandle_t handle, int terms) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (terms != 3 && terms != 6) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  handle->split_terms = terms;
+  return ok_status();
+}
+
+calamanStatus_t calamanGetFloatSplit(calamanHandle_t handle, int *terms) {
+  if (handle == nullptr || terms == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  *terms = handle->split_terms;
+  return ok_status();
+}
+
+calamanStatus_t calaman_gemm_bf16x_bufferSize(int m, int n, int k, int terms, size_t *bytes) {
+  if (m < 1 || n < 1 || k < 1 || (terms != 3 && terms != 6) || bytes == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  *bytes = tc_gemm_workspace_bytes(m, n, k, terms);
+  return ok_status();
+}
+
+calamanStatus_t calaman_gemm_bf16x_s(calamanStream_t stream, int m, int n, int k, double alpha,
+                                     const float *A, int lda, const float *B, int ldb, double beta,
+                                     float *C, int ldc, int terms, void *work, size_t work_bytes) {
+  if (m < 1 || n < 1 || k < 1 || lda < m || ldb < k || ldc < m || (terms != 3 && terms != 6) ||
+      A == nullptr || B == nullptr || C == nullptr || work == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (work_bytes < tc_gemm_workspace_bytes(m, n, k, terms)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  GemmScratch gs;
+  gs.ptr = work;
+  gs.bytes = work_bytes;
+  gs.terms = terms;
+  GemmScratchScope gss(&gs);
+  CLM_CUDA(gemm_nn<float>(static_cast<cudaStream_t>(stream), m, n, k, alpha, A, lda, B, ldb, beta, C, ldc));
+  return ok_status();
+}
 
 calamanStatus_t calaman_getrf_bufferSize(int n, size_t *bytes) {
   if (n < 1 || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);

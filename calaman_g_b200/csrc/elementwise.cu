@@ -156,6 +156,19 @@ __global__ void scale_copy_kernel(int n, double f, const T *__restrict__ A, int 
   }
 }
 
+__device__ __forceinline__ double cvt(float x, double *) { return (double)x; }
+__device__ __forceinline__ float cvt(double x, float *) { return (float)x; }
+__device__ __forceinline__ double2 cvt(float2 x, double2 *) { return make_double2(x.x, x.y); }
+__device__ __forceinline__ float2 cvt(double2 x, float2 *) { return make_float2((float)x.x, (float)x.y); }
+
+template <typename Ti, typename To>
+__global__ void convert_kernel(int n, const Ti *__restrict__ A, int lda, To *__restrict__ B, int ldb) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  for (int col = blockIdx.y; col < n; col += gridDim.y)
+    B[(std::size_t)col * ldb + row] = cvt(A[(std::size_t)col * lda + row], (To *)nullptr);
+}
+
 template <typename T>
 __global__ void ps_build_block_kernel(T *__restrict__ B, int ldb, int n, const T *__restrict__ A,
                                       int lda, const T *__restrict__ powers, std::size_t stride,
@@ -260,6 +273,17 @@ cudaError_t launch_scale_copy(cudaStream_t s, int n, double f, const T *A, int l
   scale_copy_kernel<T><<<grid_2d(n, n), kRowThreads, 0, s>>>(n, f, A, lda, B, ldb);
   return launched();
 }
+
+template <typename Ti, typename To>
+cudaError_t launch_convert(cudaStream_t s, int n, const Ti *A, int lda, To *B, int ldb) {
+  if (n < 1) return cudaSuccess;
+  convert_kernel<Ti, To><<<grid_2d(n, n), kRowThreads, 0, s>>>(n, A, lda, B, ldb);
+  return launched();
+}
+template cudaError_t launch_convert<float, double>(cudaStream_t, int, const float *, int, double *, int);
+template cudaError_t launch_convert<double, float>(cudaStream_t, int, const double *, int, float *, int);
+template cudaError_t launch_convert<float2, double2>(cudaStream_t, int, const float2 *, int, double2 *, int);
+template cudaError_t launch_convert<double2, float2>(cudaStream_t, int, const double2 *, int, float2 *, int);
 
 template <typename T>
 cudaError_t launch_ps_build_block(cudaStream_t s, T *B, int ldb, int n, const T *A, int lda,

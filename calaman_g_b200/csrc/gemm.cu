@@ -429,9 +429,9 @@ inline bool aligned16(const void *p) { return (reinterpret_cast<std::uintptr_t>(
 
 // Launch through `run`, bracketed by CUDA events when a timer is active.
 template <typename F>
-cudaError_t timed_launch(cudaStream_t s, double flops, F &&run) {
+cudaError_t timed_launch(cudaStream_t s, double flops, F &&run, bool count = true) {
   KernelTimer *t = tl_timer;
-  note_launch();
+  if (count) note_launch();
   if (t == nullptr) return run();
   cudaEvent_t a = t->take(), b = t->take();
   if (a == nullptr || b == nullptr) return run();
@@ -477,6 +477,13 @@ template <>
 cudaError_t gemm_nn<float>(cudaStream_t s, int M, int N, int K, double alpha, const float *A,
                            int lda, const float *B, int ldb, double beta, float *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  GemmScratch *g = tl_gemm_scratch;
+  if (g && K > 0 && g->ptr && tc_gemm_workspace_bytes(M, N, K, g->terms) <= g->bytes) {
+    return timed_launch(
+        s, real_flops(M, N, K),
+        [&] { return tc_gemm_f32(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, g->ptr, g->bytes, g->terms); },
+        /*count=*/false);  // its split and GEMM kernels count themselves
+  }
   return timed_launch(s, real_flops(M, N, K), [&] {
     dim3 grid((M + 63) / 64, (N + 63) / 64);
     simt_gemm_nn_kernel<float><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);

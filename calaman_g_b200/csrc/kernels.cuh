@@ -35,6 +35,11 @@ cudaError_t launch_pade_split(cudaStream_t s, int n, const T *U, const T *V, T *
 template <typename T>
 cudaError_t launch_scale_copy(cudaStream_t s, int n, double f, const T *A, int lda, T *B, int ldb);
 
+// B = (To) A: precision conversion of an n x n matrix (float <-> double,
+// complex64 <-> complex128).
+template <typename Ti, typename To>
+cudaError_t launch_convert(cudaStream_t s, int n, const Ti *A, int lda, To *B, int ldb);
+
 // ---- matrix polynomials -----------------------------------------------------
 // B_j = c0 I + c1 A + sum_{k>=2} c_k A^k, coefficients on the device
 // (src/paterson_stockmeyer/paterson_stockmeyer.cu:51-85)
@@ -53,6 +58,13 @@ cudaError_t launch_add_scaled_identity(cudaStream_t s, T *P, int n, int ldp, con
 template <typename T>
 cudaError_t gemm_nn(cudaStream_t s, int M, int N, int K, double alpha, const T *A, int lda,
                     const T *B, int ldb, double beta, T *C, int ldc);
+
+// FP32 GEMM on the tcgen05 tensor cores as split-BF16 part products (terms =
+// 3 or 6), accumulated in FP32 TMEM; needs tc_gemm_workspace_bytes of scratch.
+std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms);
+cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const float *A, int lda,
+                        const float *B, int ldb, double beta, float *C, int ldc, void *ws,
+                        std::size_t ws_bytes, int terms);
 
 // ---- LU with partial pivoting and the n-RHS solve -------------------------
 // Scratch the LU needs beyond the matrix: ipiv (n ints), perm (n ints) and a

@@ -1,0 +1,415 @@
+// tc_gemm.cu -- FP32 GEMM as split-BF16 products on the 5th-generation tensor
+// cores (tcgen05, TMEM accumulators, TMA-fed shared memory), for the single-
+// precision tiers of the matrix-exponential path.
+//
+// C = alpha * A B + beta * C with A (M x K), B (K x N), C column-major FP32.
+// Each operand element x is split into bf16 parts
+//     h = bf16(x), m = bf16(x - h), l = bf16(x - h - m)
+// and the product is the sum of the part products the precision level keeps,
+// smallest first, all accumulated into one FP32 accumulator in TMEM:
+//     x3: (m,h) (h,m) (h,h)                          ~16-bit operands
+//     x6: (l,h) (h,l) (m,m) (m,h) (h,m) (h,h)         ~24-bit operands
+// The parts are written once per operand by split kernels into a K-major
+// layout (rows of Kpad bf16, zero padded to the tile grid), so the GEMM's
+// producer warp reads every operand tile with one TMA copy, 128-byte swizzled.
+//
+// Kernel structure (one CTA per 128 x 256 output tile, 6 warps):
+//   warp 0      TMA producer: a 4-stage ring of (A 128x64, B 256x64) bf16 tiles
+//   warp 1      TMEM allocator and MMA issuer (one elected thread issues
+//               tcgen05.mma 128x256x16, commits each stage back to the ring)
+//   warps 2..5  epilogue: tcgen05.ld 32 lanes x 32 columns at a time,
+//               alpha/beta, coalesced column-major stores
+// Every mbarrier wait is bounded; a wait that runs out records an error code
+// and the CTA unwinds (draining its own TMA copies, freeing its TMEM).
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "kernels.cuh"
+
+namespace clm {
+
+namespace {
+
+constexpr int TM = 128;       // UMMA M (TMEM lanes)
+constexpr int TN = 256;       // UMMA N (TMEM columns)
+constexpr int TK = 64;        // k-block: one 128-byte swizzle atom of bf16
+constexpr int UK = 16;        // UMMA K for 16-bit inputs
+constexpr int STAGES = 4;
+constexpr int kThreads = 192;
+constexpr int kA = TM * TK * 2;  // bytes of one A stage
+constexpr int kB = TN * TK * 2;  // bytes of one B stage
+constexpr long long kSpinLimit = 1ll << 26;
+
+struct TcParams {
+  int M, N, nkb;        // nkb: k-blocks per part product (Kpad / TK)
+  int Mpad, Npad;       // rows of one A part / one B part in the part buffers
+  int nterms;
+  int pa[9], pb[9];     // part index of A and of B for every term
+  float alpha, beta;
+  float *C;
+  int ldc;
+  int *err;
+};
+
+__device__ __forceinline__ uint32_t saddr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on the phase of the given parity; false when it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x,
+                                            int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(saddr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(saddr(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile whose
+// 8-row groups are 1024 bytes apart (sm_100 descriptor version 1).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);  // start address (16-byte units)
+  d |= (uint64_t)1u << 16;                 // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024u >> 4) << 32;       // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1u << 46;                 // descriptor version
+  d |= (uint64_t)2u << 61;                 // swizzle: 128 B
+  return d;
+}
+
+// Instruction descriptor: bf16 x bf16 -> f32, both K-major, M = TM, N = TN.
+constexpr uint32_t kIdesc = (1u << 4)              // D format f32
+                            | (1u << 7)            // A format bf16
+                            | (1u << 10)           // B format bf16
+                            | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   saddr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+        "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+        "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void record_error(int *err, int code) {
+  if (err) atomicCAS(err, 0, code);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_split_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
+                         const __grid_constant__ CUtensorMap map_b, const TcParams prm) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte alignment for the 128-byte swizzle atoms
+  unsigned char *base = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char *sA = base;
+  unsigned char *sB = base + STAGES * kA;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sB + STAGES * kB);
+  uint64_t *empty = full + STAGES;
+  uint64_t *acc_full = empty + STAGES;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_full + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
+  const int total = prm.nterms * prm.nkb;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {  // TMEM: 256 columns x 128 lanes of f32
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     saddr(tmem_slot)),
+                 "r"(TN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- producer ----
+    int issued = 0;
+    for (int it = 0; it < total; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)((it / STAGES) & 1);
+      if (!mbar_wait(&empty[s], ph ^ 1u) || *(volatile int *)abort_flag) {
+        record_error(prm.err, 1);
+        *(volatile int *)abort_flag = 1;
+        break;
+      }
+      const int t = it / prm.nkb, kb = it - t * prm.nkb;
+      mbar_expect_tx(&full[s], kA + kB);
+      tma_load_2d(sA + s * kA, &map_a, &full[s], kb * TK, prm.pa[t] * prm.Mpad + m0);
+      tma_load_2d(sB + s * kB, &map_b, &full[s], kb * TK, prm.pb[t] * prm.Npad + n0);
+      issued = it + 1;
+    }
+    // drain: the copies this thread issued must land before the CTA exits
+    for (int it = issued - STAGES > 0 ? issued - STAGES : 0; it < issued; ++it)
+      mbar_wait(&full[it % STAGES], (uint32_t)((it / STAGES) & 1));
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    bool ok = true;
+    for (int it = 0; it < total; ++it) {
+      const int s = it % STAGES;
+      const uint32_t ph = (uint32_t)((it / STAGES) & 1);
+      if (!mbar_wait(&full[s], ph) || *(volatile int *)abort_flag) {
+        record_error(prm.err, 2);
+        *(volatile int *)abort_flag = 1;
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = saddr(sA + s * kA), b0 = saddr(sB + s * kB);
+#pragma unroll
+      for (int k = 0; k < TK / UK; ++k)  // +32 bytes per 16-element k step inside the atom
+        umma(tmem, smem_desc(a0 + k * 32), smem_desc(b0 + k * 32), (it > 0 || k > 0) ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    if (ok) umma_commit(acc_full);
+    else *(volatile int *)abort_flag = 1;
+  } else if (warp >= 2) {
+    // ---- epilogue ----
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    bool ok = mbar_wait(acc_full, 0);
+    if (!ok) record_error(prm.err, 3);
+    if (ok && !*(volatile int *)abort_flag) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const int m = m0 + q * 32 + lane;
+      for (int c0 = 0; c0 < TN; c0 += 32) {
+        if (n0 + c0 >= prm.N) break;
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+        if (m < prm.M) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int n = n0 + c0 + j;
+            if (n < prm.N) {
+              float *c = prm.C + (std::size_t)n * prm.ldc + m;
+              const float x = prm.alpha * __uint_as_float(v[j]);
+              *c = (prm.beta == 0.f) ? x : fmaf(prm.beta, *c, x);
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+  }
+}
+
+// ---- operand split kernels --------------------------------------------------
+__device__ __forceinline__ void split3(float x, __nv_bfloat16 &h, __nv_bfloat16 &m, __nv_bfloat16 &l) {
+  h = __float2bfloat16_rn(x);
+  const float r = x - __bfloat162float(h);
+  m = __float2bfloat16_rn(r);
+  l = __float2bfloat16_rn(r - __bfloat162float(m));
+}
+
+// A (M x K, column-major, lda) -> parts[p][row][k], rows of Kpad, Mpad rows per
+// part; the transpose goes through a 32 x 33 shared tile.
+__global__ void split_a_kernel(int M, int K, const float *__restrict__ A, int lda, int Mpad,
+                               int Kpad, int nparts, __nv_bfloat16 *__restrict__ parts) {
+  __shared__ float tile[32][33];
+  const int mb = blockIdx.x * 32, kb = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int r = ty; r < 32; r += 8) {  // read: consecutive m along tx
+    const int m = mb + tx, k = kb + r;
+    tile[r][tx] = (m < M && k < K) ? A[(std::size_t)k * lda + m] : 0.f;
+  }
+  __syncthreads();
+  const std::size_t part_stride = (std::size_t)Mpad * Kpad;
+  for (int r = ty; r < 32; r += 8) {  // write: consecutive k along tx
+    const int m = mb + r, k = kb + tx;
+    if (m < Mpad && k < Kpad) {
+      __nv_bfloat16 h, mm, l;
+      split3(tile[tx][r], h, mm, l);
+      const std::size_t at = (std::size_t)m * Kpad + k;
+      parts[at] = h;
+      parts[part_stride + at] = mm;
+      if (nparts > 2) parts[2 * part_stride + at] = l;
+    }
+  }
+}
+
+// B (K x N, column-major, ldb) -> parts[p][col][k]: already K-contiguous.
+__global__ void split_b_kernel(int K, int N, const float *__restrict__ B, int ldb, int Npad,
+                               int Kpad, int nparts, __nv_bfloat16 *__restrict__ parts) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Kpad) return;
+  const std::size_t part_stride = (std::size_t)Npad * Kpad;
+  for (int n = blockIdx.y; n < Npad; n += gridDim.y) {
+    const float x = (k < K && n < N) ? B[(std::size_t)n * ldb + k] : 0.f;
+    __nv_bfloat16 h, m, l;
+    split3(x, h, m, l);
+    const std::size_t at = (std::size_t)n * Kpad + k;
+    parts[at] = h;
+    parts[part_stride + at] = m;
+    if (nparts > 2) parts[2 * part_stride + at] = l;
+  }
+}
+
+// ---- host side ----------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (fn == nullptr) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// A row-major bf16 matrix of `rows` x `cols` (cols contiguous), boxes of box_rows x 64.
+bool make_map(CUtensorMap *map, void *ptr, long long rows, long long cols, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (fn == nullptr) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+struct SplitLayout {
+  int Mpad, Npad, Kpad;
+  std::size_t a_bytes, b_bytes, total;
+};
+SplitLayout split_layout(int M, int N, int K, int nparts) {
+  SplitLayout L;
+  L.Mpad = (M + TM - 1) / TM * TM;
+  L.Npad = (N + TN - 1) / TN * TN;
+  L.Kpad = (K + TK - 1) / TK * TK;
+  L.a_bytes = align_up((std::size_t)nparts * L.Mpad * L.Kpad * 2, 256);
+  L.b_bytes = align_up((std::size_t)nparts * L.Npad * L.Kpad * 2, 256);
+  L.total = 256 + L.a_bytes + L.b_bytes;  // [error word | A parts | B parts]
+  return L;
+}
+
+}  // namespace
+
+std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms) {
+  return split_layout(M, N, K, terms == 3 ? 2 : 3).total;
+}
+
+cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const float *A, int lda,
+                        const float *B, int ldb, double beta, float *C, int ldc, void *ws,
+                        std::size_t ws_bytes, int terms) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  const int nparts = terms == 3 ? 2 : 3;
+  const SplitLayout L = split_layout(M, N, K > 0 ? K : 1, nparts);
+  if (ws == nullptr || ws_bytes < L.total) return cudaErrorInvalidValue;
+  char *w = static_cast<char *>(ws);
+  int *err = reinterpret_cast<int *>(w);
+  auto *pa = reinterpret_cast<__nv_bfloat16 *>(w + 256);
+  auto *pb = reinterpret_cast<__nv_bfloat16 *>(w + 256 + L.a_bytes);
+
+  cudaError_t e;
+  split_a_kernel<<<dim3(L.Mpad / 32, L.Kpad / 32), 256, 0, s>>>(M, K, A, lda, L.Mpad, L.Kpad, nparts, pa);
+  if ((e = launched()) != cudaSuccess) return e;
+  {
+    const int gy = L.Npad < 65535 ? L.Npad : 65535;
+    split_b_kernel<<<dim3((L.Kpad + 255) / 256, gy), 256, 0, s>>>(K, N, B, ldb, L.Npad, L.Kpad, nparts, pb);
+    if ((e = launched()) != cudaSuccess) return e;
+  }
+
+  CUtensorMap ma, mb;
+  if (!make_map(&ma, pa, (long long)nparts * L.Mpad, L.Kpad, TM)) return cudaErrorNotSupported;
+  if (!make_map(&mb, pb, (long long)nparts * L.Npad, L.Kpad, TN)) return cudaErrorNotSupported;
+
+  TcParams p = {};
+  p.M = M;
+  p.N = N;
+  p.nkb = L.Kpad / TK;
+  p.Mpad = L.Mpad;
+  p.Npad = L.Npad;
+  if (terms == 3) {
+    const int A3[3] = {1, 0, 0}, B3[3] = {0, 1, 0};
+    p.nterms = 3;
+    for (int t = 0; t < 3; ++t) p.pa[t] = A3[t], p.pb[t] = B3[t];
+  } else {
+    const int A6[6] = {2, 0, 1, 1, 0, 0}, B6[6] = {0, 2, 1, 0, 1, 0};
+    p.nterms = 6;
+    for (int t = 0; t < 6; ++t) p.pa[t] = A6[t], p.pb[t] = B6[t];
+  }
+  p.alpha = (float)alpha;
+  p.beta = (float)beta;
+  p.C = C;
+  p.ldc = ldc;
+  p.err = err;
+
+  const int smem = STAGES * (kA + kB) + 1024 + 256;
+  static bool configured = false;
+  if (!configured) {
+    if ((e = cudaFuncSetAttribute(tc_split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem)) != cudaSuccess)
+      return e;
+    configured = true;
+  }
+  tc_split_gemm_kernel<<<dim3(L.Mpad / TM, L.Npad / TN), kThreads, smem, s>>>(ma, mb, p);
+  return launched();
+}
+
+}  // namespace clm

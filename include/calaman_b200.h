@@ -222,6 +222,20 @@ calamanStatus_t calaman_gemm_z(calamanStream_t stream, int m, int n, int k, doub
                                const void *A, int lda, const void *B, int ldb, double beta,
                                void *C, int ldc);
 
+/* FP32 GEMM on the tcgen05 tensor cores: every operand element is split into
+ * bf16 parts (x = h + m + l) and the product accumulates, in FP32 TMEM, the
+ * part products the precision level keeps: terms = 3 (h and m parts, ~16-bit
+ * operands) or 6 (h, m and l parts, ~24-bit operands, about FP32 accuracy).
+ * This is how the _s tier of expm/pade runs its dense products; `work` holds
+ * the operand parts (calaman_gemm_bf16x_bufferSize bytes, 256-byte aligned). */
+calamanStatus_t calaman_gemm_bf16x_bufferSize(int m, int n, int k, int terms, size_t *bytes);
+calamanStatus_t calaman_gemm_bf16x_s(calamanStream_t stream, int m, int n, int k, double alpha,
+                                     const float *A, int lda, const float *B, int ldb, double beta,
+                                     float *C, int ldc, int terms, void *work, size_t work_bytes);
+/* The split level the handle's _s expm/pade calls use (default 6). */
+calamanStatus_t calamanSetFloatSplit(calamanHandle_t handle, int terms);
+calamanStatus_t calamanGetFloatSplit(calamanHandle_t handle, int *terms);
+
 /* LU with partial pivoting and the n-right-hand-side solve that pade() runs on
  * q_m(A) (the reference calls the solver library's getrf/getrs through
  * WarpWraps, src/expm/pade.cppm:186-188). LAPACK semantics: P A = L U, pivot
