@@ -1,0 +1,185 @@
+// calaman_b200.hpp -- C++ drop-in for calaman_G's `calaman.expm`,
+// `calaman.paterson_stockmeyer` and `calaman.horner` module interfaces.
+//
+// A reference call site such as
+//
+//     import calaman.expm;
+//     calaman::Status st = calaman::expm<double>(blas, solver, stream, n, d_A, lda,
+//                                                d_E, lde, d_work, bytes, d_info, &plan);
+//
+// compiles unchanged against this header once `blas` / `solver` are
+// calaman::BlasHandle / calaman::SolverHandle (both a calamanHandle_t) and the
+// stream is a cudaStream_t. The templates forward to the C ABI in
+// calaman_b200.h; Status keeps the reference's {domain, code} shape, its ok(),
+// name() and outcome equality (src/error_handling/error_handling.cppm:99-187).
+// Element types: float, double, std::complex<float>, std::complex<double>
+// (interleaved, layout-compatible with the reference's wwrFloatComplex /
+// wwrDoubleComplex); horner and paterson_stockmeyer exist for float and double.
+#pragma once
+
+#include <complex>
+#include <cstddef>
+#include <type_traits>
+
+#include "calaman_b200.h"
+
+// cudaStream_t exactly as the CUDA runtime declares it, so this header also
+// compiles in translation units that include no CUDA header.
+struct CUstream_st;
+typedef struct CUstream_st *cudaStream_t;
+
+namespace calaman {
+
+enum class ErrorDomain { blas = CALAMAN_DOMAIN_BLAS, solver = CALAMAN_DOMAIN_SOLVER, runtime = CALAMAN_DOMAIN_RUNTIME };
+
+struct Status {
+  ErrorDomain domain = ErrorDomain::blas;
+  int code = 0;
+  constexpr Status() = default;
+  constexpr Status(calamanStatus_t s) : domain(static_cast<ErrorDomain>(s.domain)), code(s.code) {}
+  [[nodiscard]] constexpr bool ok() const noexcept { return code == 0; }
+  [[nodiscard]] const char *name() const noexcept {
+    if (domain == ErrorDomain::runtime) return ok() ? "cudaSuccess" : "cudaError";
+    switch (code) {
+    case CALAMAN_STATUS_SUCCESS: return "SUCCESS";
+    case CALAMAN_STATUS_NOT_INITIALIZED: return "NOT_INITIALIZED";
+    case CALAMAN_STATUS_ALLOC_FAILED: return "ALLOC_FAILED";
+    case CALAMAN_STATUS_INVALID_VALUE: return "INVALID_VALUE";
+    case CALAMAN_STATUS_ARCH_MISMATCH: return "ARCH_MISMATCH";
+    case CALAMAN_STATUS_EXECUTION_FAILED: return "EXECUTION_FAILED";
+    case CALAMAN_STATUS_INTERNAL_ERROR: return "INTERNAL_ERROR";
+    case CALAMAN_STATUS_NOT_SUPPORTED: return "NOT_SUPPORTED";
+    default: return "UNKNOWN";
+    }
+  }
+  // every success equals every other success; errors compare by domain and code
+  [[nodiscard]] constexpr bool operator==(const Status &o) const noexcept {
+    if (ok() || o.ok()) return ok() && o.ok();
+    return domain == o.domain && code == o.code;
+  }
+};
+
+using BlasHandle = calamanHandle_t;
+using SolverHandle = calamanHandle_t;
+using ExpmPlan = calamanExpmPlan_t;
+using PatersonStockmeyerPlan = calamanPatersonStockmeyerPlan_t;
+
+template <typename T>
+using real_t = std::conditional_t<std::is_same_v<T, std::complex<float>>, float,
+                                  std::conditional_t<std::is_same_v<T, std::complex<double>>, double, T>>;
+
+namespace detail {
+template <typename T> inline constexpr bool is_single = std::is_same_v<real_t<T>, float>;
+template <typename T> inline constexpr bool is_complex =
+    std::is_same_v<T, std::complex<float>> || std::is_same_v<T, std::complex<double>>;
+template <typename T> struct always_false : std::false_type {};
+}  // namespace detail
+
+// ---- plan (src/expm/plan.cppm:51-130) ---------------------------------------
+template <typename T> real_t<T> pade_theta(int m) {
+  if constexpr (detail::is_single<T>) return calaman_pade_theta_s(m);
+  else return calaman_pade_theta_d(m);
+}
+template <typename T> ExpmPlan expm_plan(real_t<T> norm1) {
+  if constexpr (detail::is_single<T>) return calaman_expm_plan_s(norm1);
+  else return calaman_expm_plan_d(norm1);
+}
+
+// ---- workspace queries (src/expm/buffer_size.cppm) ----------------------------
+template <typename T> Status expm_bufferSize(SolverHandle h, int n, std::size_t *bytes) {
+  if constexpr (std::is_same_v<T, float>) return calaman_expm_bufferSize_s(h, n, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_expm_bufferSize_d(h, n, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_expm_bufferSize_c(h, n, bytes);
+  else return calaman_expm_bufferSize_z(h, n, bytes);
+}
+template <typename T> Status pade_bufferSize(SolverHandle h, int m, int n, std::size_t *bytes) {
+  if constexpr (std::is_same_v<T, float>) return calaman_pade_bufferSize_s(h, m, n, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_pade_bufferSize_d(h, m, n, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_pade_bufferSize_c(h, m, n, bytes);
+  else return calaman_pade_bufferSize_z(h, m, n, bytes);
+}
+
+// ---- expm (src/expm/expm.cppm:87-174) ------------------------------------------
+template <typename T>
+Status expm(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int n, const T *d_A, int lda,
+            T *d_expA, int lde, void *d_work, std::size_t lwork_bytes, int *d_info,
+            ExpmPlan *plan = nullptr) {
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_expm_s(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_expm_d(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_expm_c(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+  else
+    return calaman_expm_z(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+}
+
+// ---- pade (src/expm/pade.cppm:77-191) ------------------------------------------
+template <typename T>
+Status pade(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int m, int n, const T *d_A,
+            int lda, T *d_r, int ldr, void *d_work, std::size_t lwork_bytes, int *d_info) {
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_pade_s(blas, solver, stream, m, n, d_A, lda, d_r, ldr, d_work, lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_pade_d(blas, solver, stream, m, n, d_A, lda, d_r, ldr, d_work, lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_pade_c(blas, solver, stream, m, n, d_A, lda, d_r, ldr, d_work, lwork_bytes, d_info);
+  else
+    return calaman_pade_z(blas, solver, stream, m, n, d_A, lda, d_r, ldr, d_work, lwork_bytes, d_info);
+}
+
+// ---- matrix_norm1 (src/expm/norm1.cppm:45-56) -------------------------------------
+template <typename T>
+real_t<T> matrix_norm1(cudaStream_t stream, int n, const T *d_A, int lda, real_t<T> *d_colsum) {
+  if constexpr (std::is_same_v<T, float>) return calaman_matrix_norm1_s(stream, n, d_A, lda, d_colsum);
+  else if constexpr (std::is_same_v<T, double>) return calaman_matrix_norm1_d(stream, n, d_A, lda, d_colsum);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_matrix_norm1_c(stream, n, d_A, lda, d_colsum);
+  else return calaman_matrix_norm1_z(stream, n, d_A, lda, d_colsum);
+}
+
+// ---- horner (src/horner/interface.cppm:104-194) --------------------------------
+template <typename T> std::size_t horner_bufferSize(int n) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "horner: float or double");
+  if constexpr (std::is_same_v<T, float>) return calaman_horner_bufferSize_s(n);
+  else return calaman_horner_bufferSize_d(n);
+}
+template <typename T>
+Status horner(BlasHandle handle, int n, const T *d_coeffs, int degree, const T *d_A, int lda, T *d_P,
+              int ldp, void *d_work, std::size_t work_bytes) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "horner: float or double");
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_horner_s(handle, n, d_coeffs, degree, d_A, lda, d_P, ldp, d_work, work_bytes);
+  else
+    return calaman_horner_d(handle, n, d_coeffs, degree, d_A, lda, d_P, ldp, d_work, work_bytes);
+}
+
+// ---- paterson_stockmeyer (src/paterson_stockmeyer/interface.cppm:117-422) --------
+inline int paterson_stockmeyer_cost(int degree, int s) { return calaman_paterson_stockmeyer_cost(degree, s); }
+inline int paterson_stockmeyer_block_size(int degree) { return calaman_paterson_stockmeyer_block_size(degree); }
+inline PatersonStockmeyerPlan paterson_stockmeyer_plan(int degree, int s_requested = 0) {
+  return calaman_paterson_stockmeyer_plan(degree, s_requested);
+}
+template <typename T> std::size_t paterson_stockmeyer_power_stride(int n) {
+  if constexpr (std::is_same_v<T, float>) return calaman_paterson_stockmeyer_power_stride_s(n);
+  else return calaman_paterson_stockmeyer_power_stride_d(n);
+}
+template <typename T>
+std::size_t paterson_stockmeyer_bufferSize(int n, int degree, int s_requested = 0) {
+  if constexpr (std::is_same_v<T, float>) return calaman_paterson_stockmeyer_bufferSize_s(n, degree, s_requested);
+  else return calaman_paterson_stockmeyer_bufferSize_d(n, degree, s_requested);
+}
+template <typename T>
+Status paterson_stockmeyer(BlasHandle handle, int n, const T *d_coeffs, int degree, const T *d_A,
+                           int lda, T *d_P, int ldp, void *d_work, std::size_t work_bytes,
+                           int s_requested = 0) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>,
+                "paterson_stockmeyer: float or double");
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_paterson_stockmeyer_s(handle, n, d_coeffs, degree, d_A, lda, d_P, ldp, d_work,
+                                         work_bytes, s_requested);
+  else
+    return calaman_paterson_stockmeyer_d(handle, n, d_coeffs, degree, d_A, lda, d_P, ldp, d_work,
+                                         work_bytes, s_requested);
+}
+
+}  // namespace calaman
