@@ -137,6 +137,23 @@ calamanStatus_t calaman_expm_z(calamanBlasHandle_t blas, calamanSolverHandle_t s
                                void *d_expA, int lde, void *d_work, size_t lwork_bytes,
                                int *d_info, calamanExpmPlan_t *plan);
 
+/* ---- expm without a caller workspace ----------------------------------
+ * No counterpart in the reference: calaman_G's expm always takes a caller
+ * workspace. For callers that cannot call cudaMalloc (code hosted by a
+ * framework that owns every device allocation, loops that must not allocate
+ * once running, FFI or plugin callers without a device allocator), this runs
+ * calaman_expm_d on a 4 MiB workspace held in a static device array of the
+ * library, for n <= 256; larger n returns CALAMAN_STATUS_NOT_SUPPORTED. The
+ * array is resident on every GPU that loads the library until exit. Its
+ * address is looked up on the first call made on each device: make that
+ * first call before any stream capture. All calls share the array, so calls
+ * that overlap on the GPU race on it: serialise them. Nothing in it needs to
+ * start at zero; it keeps the last call's data. Same results, status codes
+ * and single stream synchronisation as calaman_expm_d. */
+calamanStatus_t calaman_expm_noalloc_d(calamanBlasHandle_t blas, calamanStream_t stream, int n,
+                                       const double *d_A, int lda, double *d_expA, int lde,
+                                       int *d_info, calamanExpmPlan_t *plan);
+
 /* ---- pade (src/expm/pade.cppm:77-191) ----------------------------------
  * Unscaled r_m(A) = q_m(A)^-1 p_m(A); never synchronises. */
 calamanStatus_t calaman_pade_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
