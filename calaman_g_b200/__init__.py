@@ -21,7 +21,8 @@ from .capi import ExpmPlan, PsPlan, Status
 
 __all__ = [
     "Handle", "Status", "ExpmPlan", "PsPlan", "CalamanError", "expm", "pade", "matrix_norm1",
-    "expm_plan", "pade_theta", "expm_bufferSize", "pade_bufferSize", "horner",
+    "expm_plan", "pade_theta", "expm_bufferSize", "pade_bufferSize", "expm_vjp",
+    "expm_vjp_bufferSize", "expm_ad", "horner",
     "horner_bufferSize", "paterson_stockmeyer", "paterson_stockmeyer_plan",
     "paterson_stockmeyer_bufferSize", "paterson_stockmeyer_cost",
     "paterson_stockmeyer_block_size", "to_colmajor", "from_colmajor", "lib",
@@ -170,6 +171,70 @@ def expm(a, handle: Handle | None = None, out=None, return_plan: bool = False):
     _check("expm", st)
     res = from_colmajor(E, n)
     return (res, plan) if return_plan else res
+
+
+def expm_vjp_bufferSize(n: int, dtype) -> int:
+    b = ctypes.c_size_t()
+    _check("expm_vjp_bufferSize",
+           getattr(lib(), f"calaman_expm_vjp_bufferSize_{_suffix(dtype)}")(None, n, ctypes.byref(b)))
+    return b.value
+
+
+def expm_vjp(a, g, handle: Handle | None = None, return_expm: bool = False,
+             return_plan: bool = False):
+    """dL/dA for a real loss L of E = expm(A), given G = dL/dE.
+
+    L(A^H, G): the Frechet derivative at A^H (A^T for real dtypes), in
+    direction G, of the Pade-based function expm evaluates for A -- the
+    convention of torch.matrix_exp's backward. With return_expm, also returns
+    expm(A) from the same evaluation. Synchronises the stream once.
+    """
+    torch = _torch()
+    n = a.shape[0]
+    if g.shape != a.shape or g.dtype != a.dtype:
+        raise ValueError("expm_vjp: G must match A in shape and dtype")
+    h = handle or default_handle()
+    A = to_colmajor(a)
+    G = to_colmajor(g)
+    D = torch.empty_like(A)
+    E = torch.empty_like(A) if return_expm else None
+    bufs = _buffers(expm_vjp_bufferSize(n, a.dtype), a.device)
+    plan = ExpmPlan()
+    st = getattr(lib(), f"calaman_expm_vjp_{_suffix(a.dtype)}")(
+        h.ptr, h.ptr, ctypes.c_void_p(h.stream), n, _vp(A), n, _vp(G), n, _vp(D), n,
+        _vp(E) if E is not None else None, n, _vp(bufs.work), bufs.work.numel(),
+        ctypes.cast(bufs.info.data_ptr(), capi.c_int_p), ctypes.byref(plan))
+    _check("expm_vjp", st)
+    out = [from_colmajor(D, n)]
+    if return_expm:
+        out.append(from_colmajor(E, n))
+    if return_plan:
+        out.append(plan)
+    return out[0] if len(out) == 1 else tuple(out)
+
+
+_ExpmFn = None
+
+
+def expm_ad(a):
+    """expm(A) as a differentiable torch op: forward through calaman expm,
+    backward through calaman expm_vjp."""
+    global _ExpmFn
+    torch = _torch()
+    if _ExpmFn is None:
+        class _Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, x):
+                ctx.save_for_backward(x)
+                return expm(x)
+
+            @staticmethod
+            def backward(ctx, grad):
+                (x,) = ctx.saved_tensors
+                return expm_vjp(x, grad.contiguous())
+
+        _ExpmFn = _Fn
+    return _ExpmFn.apply(a)
 
 
 def pade(a, m: int, handle: Handle | None = None):

@@ -80,6 +80,9 @@ _EXPM = [_H, _H, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_
          ctypes.POINTER(ExpmPlan)]
 _PADE = [_H, _H, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_size_t,
          c_int_p]
+# expm_vjp: blas, solver, stream, n, A, lda, G, ldg, gradA, ldga, expA, lde, work, bytes, info, plan
+_VJP = [_H, _H, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int,
+        c_void_p, c_size_t, c_int_p, ctypes.POINTER(ExpmPlan)]
 _HORNER = [_H, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p, c_size_t]
 _PS = _HORNER + [c_int]
 
@@ -120,6 +123,8 @@ for _suf, _real in (("s", c_float), ("d", c_double), ("c", c_float), ("z", c_dou
     SIGNATURES[f"calaman_expm_bufferSize_{_suf}"] = (Status, [_H, c_int, c_size_t_p])
     SIGNATURES[f"calaman_pade_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int, c_size_t_p])
     SIGNATURES[f"calaman_expm_{_suf}"] = (Status, _EXPM)
+    SIGNATURES[f"calaman_expm_vjp_bufferSize_{_suf}"] = (Status, [_H, c_int, c_size_t_p])
+    SIGNATURES[f"calaman_expm_vjp_{_suf}"] = (Status, _VJP)
     SIGNATURES[f"calaman_pade_{_suf}"] = (Status, _PADE)
     SIGNATURES[f"calaman_matrix_norm1_{_suf}"] = (_real, [c_void_p, c_int, c_void_p, c_int, c_void_p])
     SIGNATURES[f"calaman_gemm_{_suf}"] = (Status, _GEMM)

@@ -9,7 +9,7 @@
 #include <cstring>
 #include <utility>
 
-#include "kernels.cuh"
+#include "expm_common.cuh"
 
 namespace clm {
 
@@ -17,91 +17,7 @@ unsigned long long g_launch_count();
 
 namespace {
 
-inline KernelTimer *timer_of(calamanHandle_t h) { return h ? &h->timer : nullptr; }
-inline int split_terms_of(calamanHandle_t h) { return h ? h->split_terms : 6; }
-
-constexpr int kMaxDim = 46340;  // flat int indexing bound, src/expm/detail.cppm:25-28
-
-// ---- Pade tables (src/expm/expm_bridge.h:58-91; Higham 2005 eq. 2.2) -------
-constexpr double kB3[4] = {1.0, 1.0 / 2.0, 1.0 / 10.0, 1.0 / 120.0};
-constexpr double kB5[6] = {1.0, 1.0 / 2.0, 1.0 / 9.0, 1.0 / 72.0, 1.0 / 1008.0, 1.0 / 30240.0};
-constexpr double kB7[8] = {1.0,          1.0 / 2.0,     3.0 / 26.0,     5.0 / 312.0,
-                           5.0 / 3432.0, 1.0 / 11440.0, 1.0 / 308880.0, 1.0 / 17297280.0};
-constexpr double kB9[10] = {1.0,            1.0 / 2.0,        2.0 / 17.0,       7.0 / 408.0,
-                            7.0 / 4080.0,   1.0 / 8160.0,     1.0 / 159120.0,   1.0 / 4455360.0,
-                            1.0 / 196035840.0, 1.0 / 17643225600.0};
-constexpr double kB13[14] = {1.0,
-                             1.0 / 2.0,
-                             3.0 / 25.0,
-                             11.0 / 600.0,
-                             11.0 / 5520.0,
-                             3.0 / 18400.0,
-                             1.0 / 96600.0,
-                             1.0 / 1932000.0,
-                             1.0 / 48944000.0,
-                             1.0 / 1585785600.0,
-                             1.0 / 67395888000.0,
-                             1.0 / 3953892096000.0,
-                             1.0 / 355850288640000.0,
-                             1.0 / 64764752532480000.0};
-
-const double *pade_coeffs(int m) {
-  switch (m) {
-  case 3: return kB3;
-  case 5: return kB5;
-  case 7: return kB7;
-  case 9: return kB9;
-  case 13: return kB13;
-  default: return nullptr;
-  }
-}
-int pade_num_powers(int m) { return (m == 13) ? 3 : (m - 1) / 2; }
-int pade_num_gemms(int m) { return pade_num_powers(m) + 1 + ((m == 13) ? 2 : 0); }
-
-// theta_m, src/expm/plan.cppm:51-85: u = 2^-53 and u = 2^-24 columns.
-double theta_double(int m) {
-  switch (m) {
-  case 3: return 1.495585217958292e-2;
-  case 5: return 2.539398330063232e-1;
-  case 7: return 9.504178996162932e-1;
-  case 9: return 2.097847961257067;
-  case 13: return 5.371920351148152;
-  default: return 0.0;
-  }
-}
-float theta_single(int m) {
-  switch (m) {
-  case 3: return 4.258730034897931e-1f;
-  case 5: return 1.880152698533769f;
-  case 7: return 3.925724846433284f;
-  case 9: return 6.249156334514102f;
-  case 13: return 1.124873763647540e1f;
-  default: return 0.0f;
-  }
-}
-
-// expm_plan<T>, src/expm/plan.cppm:112-130 (the single column is compared and
-// log2'd in float, as the reference's float instantiation does).
-template <typename R>
-calamanExpmPlan_t plan_for(R norm1) {
-  static const int degrees[5] = {3, 5, 7, 9, 13};
-  for (int m : degrees) {
-    const R th = sizeof(R) == 4 ? (R)theta_single(m) : (R)theta_double(m);
-    if (norm1 <= th) return calamanExpmPlan_t{m, 0, pade_num_gemms(m)};
-  }
-  const R theta = sizeof(R) == 4 ? (R)theta_single(13) : (R)theta_double(13);
-  int s = (int)std::ceil(std::log2(norm1 / theta));
-  if (s < 0) s = 0;
-  return calamanExpmPlan_t{13, s, pade_num_gemms(13) + s};
-}
-
 // ---- workspaces --------------------------------------------------------
-// FP32 products run as split-BF16 tensor-core GEMMs and need operand-part
-// scratch sized for the largest (n x n x n) product of the evaluation.
-template <typename T> std::size_t tc_scratch_bytes(int n) {
-  return std::is_same<T, float>::value ? tc_gemm_workspace_bytes(n, n, n, 6) : 0;
-}
-
 // pade(): [P0 .. P_{np-1} | X (m = 13) | V | W | LU scratch | (FP32: tensor-core
 // operand parts)], all 256-aligned. P0 doubles as U = A W and then as the
 // numerator p = V + U; V becomes the denominator q = V - U and is factored in
@@ -127,12 +43,6 @@ struct PadeWs {
     return L.used;
   }
 };
-
-// The FP64 twin of a single-precision element type: the single tiers run
-// their final squarings in FP64.
-template <typename T> struct Wide { using type = T; };
-template <> struct Wide<float> { using type = double; };
-template <> struct Wide<float2> { using type = double2; };
 
 // expm(): [As (also the squaring scratch) | colsum | norm | (single tiers: two
 // FP64 n x n squaring buffers) | pade region]
@@ -168,20 +78,6 @@ std::size_t expm_bytes(int n) {
   for (int m : {3, 5, 7, 9, 13}) worst = std::max(worst, pade_bytes<T>(n, m));
   return e.carve(nullptr, n) + worst;
 }
-
-struct PointerModeScope {  // save / force host / restore, src/expm/expm.cppm:107-115
-  calamanHandle_t h;
-  int saved;
-  explicit PointerModeScope(calamanHandle_t handle) : h(handle), saved(CALAMAN_POINTER_MODE_HOST) {
-    if (h) {
-      saved = h->pointer_mode;
-      h->pointer_mode = CALAMAN_POINTER_MODE_HOST;
-    }
-  }
-  ~PointerModeScope() {
-    if (h) h->pointer_mode = saved;
-  }
-};
 
 // ---- pade<T>, src/expm/pade.cppm:77-191 -------------------------------------
 template <typename T>

@@ -274,6 +274,49 @@ cudaError_t launch_scale_copy(cudaStream_t s, int n, double f, const T *A, int l
   return launched();
 }
 
+__device__ __forceinline__ float conj_if(float x, bool) { return x; }
+__device__ __forceinline__ double conj_if(double x, bool) { return x; }
+__device__ __forceinline__ float2 conj_if(float2 x, bool c) { return c ? make_float2(x.x, -x.y) : x; }
+__device__ __forceinline__ double2 conj_if(double2 x, bool c) { return c ? make_double2(x.x, -x.y) : x; }
+
+// B (cols x rows) = f A^T or f A^H, through a 32 x 33 shared tile so both the
+// read and the write are coalesced.
+template <typename T>
+__global__ void transpose_kernel(int rows, int cols, double f, const T *__restrict__ A, int lda,
+                                 T *__restrict__ B, int ldb, bool conj) {
+  using R = typename elem<T>::real;
+  __shared__ T tile[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int j = ty; j < 32; j += 8) {
+    const int r = r0 + tx, c = c0 + j;
+    if (r < rows && c < cols) tile[j][tx] = A[(std::size_t)c * lda + r];
+  }
+  __syncthreads();
+  for (int j = ty; j < 32; j += 8) {
+    const int c = c0 + tx, r = r0 + j;  // B(c, r) = f op(A(r, c))
+    if (r < rows && c < cols) B[(std::size_t)r * ldb + c] = scale(conj_if(tile[tx][j], conj), (R)f);
+  }
+}
+
+template <typename T>
+cudaError_t launch_transpose(cudaStream_t s, int rows, int cols, double f, const T *A, int lda, T *B,
+                             int ldb, bool conj) {
+  if (rows < 1 || cols < 1) return cudaSuccess;
+  // rows, cols <= 46340, so both grid extents stay far below their limits
+  transpose_kernel<T><<<dim3((rows + 31) / 32, (cols + 31) / 32), 256, 0, s>>>(rows, cols, f, A, lda, B,
+                                                                              ldb, conj);
+  return launched();
+}
+
+#define CLM_INST_T(T) \
+  template cudaError_t launch_transpose<T>(cudaStream_t, int, int, double, const T *, int, T *, int, bool);
+CLM_INST_T(float)
+CLM_INST_T(double)
+CLM_INST_T(float2)
+CLM_INST_T(double2)
+#undef CLM_INST_T
+
 template <typename Ti, typename To>
 cudaError_t launch_convert(cudaStream_t s, int n, const Ti *A, int lda, To *B, int ldb) {
   if (n < 1) return cudaSuccess;

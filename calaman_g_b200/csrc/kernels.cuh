@@ -82,4 +82,10 @@ template <typename T>
 cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const void *scratch,
                   const T *B, int ldb, T *X, int ldx, int *info_dev);
 
+// B = f op(A) for an rows x cols matrix A: op is the transpose, conjugated
+// when `conj` (complex types); B is cols x rows. A and B may not alias.
+template <typename T>
+cudaError_t launch_transpose(cudaStream_t s, int rows, int cols, double f, const T *A, int lda, T *B,
+                             int ldb, bool conj);
+
 }  // namespace clm

@@ -137,6 +137,41 @@ calamanStatus_t calaman_expm_z(calamanBlasHandle_t blas, calamanSolverHandle_t s
                                void *d_expA, int lde, void *d_work, size_t lwork_bytes,
                                int *d_info, calamanExpmPlan_t *plan);
 
+/* ---- expm_vjp: the adjoint of expm --------------------------------------
+ * New entry point: calaman_G has no derivative of expm. For a real loss
+ * L(E), E = expm(A), d_G = dL/dE, writes d_gradA = dL/dA = L(A^H, G): the
+ * Frechet derivative, at A^H in direction G, of the function expm evaluates
+ * for A (r_m(X / 2^s)^(2^s) with (m, s) = expm_plan(||A||_1), returned in
+ * *plan). A^T for the real types; the convention of torch.matrix_exp's
+ * backward; equal to the upper-right n x n block of expm([[A^H, G], [0, A^H]]).
+ * d_expA (may be NULL) receives expm(A) from the same evaluation. d_gradA may
+ * overlap d_A or d_G. d_info: 2 ints as for expm. Synchronises `stream` once.
+ * Work for m = 13: 19 + 3 s GEMMs, one LU, two n-RHS solves. */
+calamanStatus_t calaman_expm_vjp_bufferSize_s(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_vjp_bufferSize_d(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_vjp_bufferSize_c(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_vjp_bufferSize_z(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_vjp_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                   calamanStream_t stream, int n, const float *d_A, int lda,
+                                   const float *d_G, int ldg, float *d_gradA, int ldga,
+                                   float *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                   int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_vjp_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                   calamanStream_t stream, int n, const double *d_A, int lda,
+                                   const double *d_G, int ldg, double *d_gradA, int ldga,
+                                   double *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                   int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_vjp_c(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                   calamanStream_t stream, int n, const void *d_A, int lda,
+                                   const void *d_G, int ldg, void *d_gradA, int ldga,
+                                   void *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                   int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_vjp_z(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                   calamanStream_t stream, int n, const void *d_A, int lda,
+                                   const void *d_G, int ldg, void *d_gradA, int ldga,
+                                   void *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                   int *d_info, calamanExpmPlan_t *plan);
+
 /* ---- expm without a caller workspace ----------------------------------
  * No counterpart in the reference: calaman_G's expm always takes a caller
  * workspace. For callers that cannot call cudaMalloc (code hosted by a

@@ -246,3 +246,76 @@ def horner(a, coeffs) -> np.ndarray:
     if rc != 0:
         raise ValueError("oracle horner rejected its arguments")
     return p
+
+
+def expm_vjp_block(a, g) -> np.ndarray:
+    """dL/dA = L(A^H, G) for L = Re<G, expm(A)>, as the upper-right n x n block
+    of expm([[A^H, G], [0, A^H]]) (Mathias' block formula; the form of
+    torch.matrix_exp's backward), evaluated by the oracle's expm in FP64.
+    This is the exact derivative up to the oracle expm's own accuracy; it does
+    not depend on the (m, s) that expm picks for A."""
+    a = _as_f64(a)
+    g = _as_f64(g)
+    n = a.shape[0]
+    ah = a.conj().T
+    blk = np.zeros((2 * n, 2 * n), dtype=a.dtype, order="F")
+    blk[:n, :n] = ah
+    blk[n:, n:] = ah
+    blk[:n, n:] = g
+    e, _, _ = expm(blk)
+    return np.asfortranarray(e[:n, n:])
+
+
+def expm_vjp_frechet(a, g, single: bool = False):
+    """The adjoint the library computes, restated in numpy FP64: the forward-mode
+    Frechet derivative (Al-Mohy and Higham 2009, Algorithm 6.4) at A^H in
+    direction G of r_m(X / 2^s)^(2^s), (m, s) = expm_plan(||A||_1) (``single``:
+    the single-precision theta ladder). Products in the library's order
+    (A4 = A2 A2, A6 = A4 A2, A8 = A4 A4; degree 13 in the nested form of the
+    oracle's pade). Returns (dL/dA, expm(A), ExpmPlan)."""
+    a = _as_f64(a)
+    g = _as_f64(g)
+    n = a.shape[0]
+    plan = expm_plan(norm1(a), single)
+    m, s = plan.m, plan.s
+    b = pade_coeffs(m)
+    f = 2.0 ** (-s)
+    x = f * a.conj().T
+    d = f * g
+    eye = np.eye(n, dtype=a.dtype)
+    p = [x @ x]
+    dm = [x @ d + d @ x]
+    np_ = pade_num_powers(m)
+    if np_ >= 2:
+        p.append(p[0] @ p[0])
+        dm.append(p[0] @ dm[0] + dm[0] @ p[0])
+    if np_ >= 3:
+        p.append(p[1] @ p[0])
+        dm.append(dm[1] @ p[0] + p[1] @ dm[0])
+    if np_ >= 4:
+        p.append(p[1] @ p[1])
+        dm.append(p[1] @ dm[1] + dm[1] @ p[1])
+    if m != 13:
+        v = b[0] * eye + sum(b[2 * (k + 1)] * p[k] for k in range(np_))
+        w = b[1] * eye + sum(b[2 * (k + 1) + 1] * p[k] for k in range(np_))
+        lv = sum(b[2 * (k + 1)] * dm[k] for k in range(np_))
+        lw = sum(b[2 * (k + 1) + 1] * dm[k] for k in range(np_))
+    else:
+        w1 = b[9] * p[0] + b[11] * p[1] + b[13] * p[2]
+        lw1 = b[9] * dm[0] + b[11] * dm[1] + b[13] * dm[2]
+        w = b[1] * eye + b[3] * p[0] + b[5] * p[1] + b[7] * p[2] + p[2] @ w1
+        lw = b[3] * dm[0] + b[5] * dm[1] + b[7] * dm[2] + p[2] @ lw1 + dm[2] @ w1
+        z1 = b[8] * p[0] + b[10] * p[1] + b[12] * p[2]
+        lz1 = b[8] * dm[0] + b[10] * dm[1] + b[12] * dm[2]
+        v = b[0] * eye + b[2] * p[0] + b[4] * p[1] + b[6] * p[2] + p[2] @ z1
+        lv = b[2] * dm[0] + b[4] * dm[1] + b[6] * dm[2] + p[2] @ lz1 + dm[2] @ z1
+    u = x @ w
+    lu = x @ lw + d @ w
+    num, den = v + u, v - u
+    dnum, dden = lv + lu, lv - lu
+    r = np.linalg.solve(den, num)
+    dr = np.linalg.solve(den, dnum - dden @ r)
+    for _ in range(s):
+        dr = r @ dr + dr @ r
+        r = r @ r
+    return np.asfortranarray(dr), np.asfortranarray(r.conj().T), plan

@@ -169,3 +169,28 @@ class Runner:
         self.torch.cuda.synchronize()
         full = dP.cpu().numpy()
         return st, from_buffer(full, n, ldp), full
+
+    def vjp(self, a: np.ndarray, g: np.ndarray, suf: str, ld: int | None = None,
+            want_expm: bool = True, out_fill=-123.5, lwork: int | None = None,
+            alias_g: bool = False):
+        """calaman_expm_vjp_<suf>: returns (status, plan, gradA, expA or None,
+        flat gradA buffer, info). ``alias_g`` writes the gradient over G."""
+        n = a.shape[0]
+        ld = ld or n
+        dA = _dev(colmajor_buffer(a, ld, suf))
+        dG = _dev(colmajor_buffer(g, ld, suf))
+        dD = dG if alias_g else _dev(np.full(n * ld, out_fill, dtype=NP_DTYPE[suf]))
+        dE = _dev(np.full(n * ld, out_fill, dtype=NP_DTYPE[suf])) if want_expm else None
+        b = ctypes.c_size_t()
+        assert getattr(self.lib, f"calaman_expm_vjp_bufferSize_{suf}")(self.h, n, ctypes.byref(b)).ok
+        w = self.workspace(b.value)
+        info = self.torch.full((2,), -99, dtype=self.torch.int32, device="cuda")
+        plan = self.capi.ExpmPlan()
+        st = getattr(self.lib, f"calaman_expm_vjp_{suf}")(
+            self.h, self.h, ctypes.c_void_p(self.stream), n, vp(dA), ld, vp(dG), ld, vp(dD), ld,
+            vp(dE) if dE is not None else None, ld, vp(w), b.value if lwork is None else lwork,
+            ctypes.cast(info.data_ptr(), self.capi.c_int_p), ctypes.byref(plan))
+        self.torch.cuda.synchronize()
+        full = dD.cpu().numpy()
+        e = from_buffer(dE.cpu().numpy(), n, ld) if dE is not None else None
+        return st, plan, from_buffer(full, n, ld), e, full, info.cpu().numpy()
