@@ -52,6 +52,17 @@ CONFIGS = {
                           desc="float64 2048x2048, N(0,1) rescaled to ||A||_1=6"),
     "expm_f32_4096": dict(n=4096, suf="s", norm=8.0, gen="gauss",
                           desc="float32 4096x4096, N(0,1)/sqrt(n) rescaled to ||A||_1=8"),
+    "expm_batched_f32_8192": dict(kind="batched", count=8192, nmax=256, suf="s",
+                                  desc="8192 float32 matrices, n uniform on {16,32,...,256}, "
+                                       "N(0,1) rescaled to ||A||_1 log-uniform in [0.1,100]"),
+    "expm_batched_f64_8192": dict(kind="batched", count=8192, nmax=256, suf="d",
+                                  desc="the same 8192 matrices in float64 (plain FP64 tier)"),
+    "expm_vjp_f64_2048": dict(kind="vjp", n=2048, suf="d", norm=6.0,
+                              desc="loss <G, expm(A)>, float64 2048x2048, A and G N(0,1), "
+                                   "A rescaled to ||A||_1=6"),
+    "expm_vjp_f32_128x512": dict(kind="vjp", n=128, count=512, suf="s", norm=6.0,
+                                 desc="loss <G, expm(A)>, 512 float32 128x128 pairs, A and G "
+                                      "N(0,1), A rescaled to ||A||_1=6"),
 }
 NP = {"s": np.float32, "d": np.float64, "c": np.complex64, "z": np.complex128}
 ELEM_BYTES = {"s": 4, "d": 8, "c": 8, "z": 16}
@@ -67,6 +78,38 @@ def make_matrix(cfg, seed=20261203):
         a = rng.standard_normal((n, n)) / np.sqrt(n)
     a = a * (cfg["norm"] / np.abs(a).sum(axis=0).max())
     return np.asfortranarray(a.astype(NP[cfg["suf"]]))
+
+
+def batched_workload(cfg, seed=20261204):
+    """The batched workload: n uniform on {16, 32, ..., nmax}, N(0,1) entries
+    rescaled to a 1-norm log-uniform in [0.1, 100] (float32 values; the
+    float64 tier gets the same values widened)."""
+    rng = np.random.default_rng(seed)
+    count, nmax = cfg["count"], cfg["nmax"]
+    sizes = rng.integers(1, nmax // 16 + 1, count) * 16
+    norms = np.exp(rng.uniform(np.log(0.1), np.log(100.0), count))
+    mats = []
+    for n, t in zip(sizes, norms):
+        a = rng.standard_normal((n, n))
+        a = (a * (t / np.abs(a).sum(axis=0).max())).astype(np.float32)
+        mats.append(a)
+    return mats
+
+
+def vjp_pair(n, norm, seed):
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((n, n))
+    a = a * (norm / np.abs(a).sum(axis=0).max())
+    g = rng.standard_normal((n, n))
+    return a, g
+
+
+def vjp_flops(n, m, s):
+    """Algorithmic flops of one adjoint: (19 + 3s) products at m = 13 (else
+    3 per power + 3), one LU, two n-RHS solves."""
+    pim = {3: 1, 5: 2, 7: 3, 9: 4, 13: 3}[m]
+    gemms = 3 * pim + (6 if m == 13 else 0) + 4 + 3 * s
+    return gemms * 2.0 * n ** 3 + (2.0 / 3.0) * n ** 3 + 2 * 2.0 * n ** 3
 
 
 def expm_flops(n, m, s, cplx):
@@ -153,36 +196,72 @@ def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
 
 
 def run_reference(args, cfg):
+    """The reference algorithm's CPU restatement (the C oracle, all host
+    threads) on the same workload; rank 0 only. Batched: each step is the
+    first 32 matrices of the batch; adjoint: each step is one numpy
+    restatement of the adjoint (FP64, threaded BLAS)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    a = make_matrix(cfg)
     from oracle import oracle as O
 
     cores = os.cpu_count() or 1
     O.set_threads(cores)
-    x = a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
+    kind = cfg.get("kind", "single")
+    dtype = {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[cfg["suf"]]
+    single = cfg["suf"] in "sc"
+    if kind == "batched":
+        mats = [m.astype(np.float64) for m in batched_workload(cfg)[:32]]
+        per_step, unit = len(mats), "expm/s"
+
+        def one():
+            for m in mats:
+                O.expm(m, single=single)
+        sample = "the first 32 matrices of the batch per step"
+        plan_info = None
+    elif kind == "vjp":
+        k = 1 if cfg["n"] > 512 else 8
+        pairs = [vjp_pair(cfg["n"], cfg["norm"], 7000 + i) for i in range(k)]
+        per_step, unit = k, "vjp/s"
+
+        def one():
+            for a, g in pairs:
+                O.expm_vjp_frechet(a, g, single=single)
+        sample = f"{k} adjoint(s) per step (numpy restatement of the adjoint)"
+        plan_info = None
+    else:
+        x = make_matrix(cfg).astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
+        per_step, unit = 1, "expm/s"
+        holder = {}
+
+        def one():
+            holder["plan"] = O.expm(x, single=single)[1]
+        sample = "one full expm of the benchmark matrix per step"
+        plan_info = holder
     for _ in range(args.warmup):
-        O.expm(x, single=cfg["suf"] in "sc")
+        one()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        _, plan, _ = O.expm(x, single=cfg["suf"] in "sc")
+        one()
     el = time.perf_counter() - t0
-    value = args.steps / el
+    value = per_step * args.steps / el
+    config = {"workload": args.config, "desc": cfg["desc"]}
+    if plan_info:
+        config["plan"] = {"m": plan_info["plan"].m, "s": plan_info["plan"].s}
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "expm/s",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": unit,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[cfg["suf"]],
-        "data": "synthetic (seeded)",
-        "config": {"workload": args.config, "desc": cfg["desc"], "plan": {"m": plan.m, "s": plan.s}},
-        "tflops": expm_flops(cfg["n"], plan.m, plan.s, cfg["suf"] in "cz") * value / 1e12,
-        "cpu_baseline": {"value": value, "unit": "expm/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} timed expm calls after {args.warmup} warm-up, "
-                                   f"C oracle (FP64 restatement of the reference algorithm), "
-                                   f"{cores} threads"},
-        "e2e": {"value": value, "unit": "expm/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": config,
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
+                         "sample": f"{sample}; {args.steps} timed steps after {args.warmup} "
+                                   f"warm-up, C oracle (FP64 restatement of the reference "
+                                   f"algorithm), {cores} threads"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if kind == "single":
+        line["tflops"] = expm_flops(cfg["n"], plan_info["plan"].m, plan_info["plan"].s,
+                                    cfg["suf"] in "cz") * value / 1e12
     print(json.dumps(line), flush=True)
 
 
@@ -373,6 +452,347 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def _init_dist():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    return torch, world, rank, local, dev, dist
+
+
+def _max_over_ranks(torch, dist, dev, values):
+    t = torch.tensor(values, dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def _bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback 1.59 PFLOP/s (no MEASURED_PEAKS.json)"
+
+
+def run_batched(args, cfg):
+    """One step = one calaman_expm_batched_<t> call over the whole batch.
+    Under torchrun the batch is split across ranks (matrices are
+    independent; balanced by sum n^3), no collective on the data path."""
+    torch, world, rank, local, dev, dist = _init_dist()
+    from calaman_g_b200 import capi
+
+    lib = capi.load()
+    suf = cfg["suf"]
+    mats_all = batched_workload(cfg)
+    # weak scaling: every rank gets the full per-GPU batch
+    mats = mats_all
+    count = len(mats)
+    ns = [m.shape[0] for m in mats]
+    tdt = torch.float32 if suf == "s" else torch.float64
+    npdt = np.float32 if suf == "s" else np.float64
+    offs, at = [], 0
+    for n in ns:
+        offs.append(at)
+        at += ((n * n + 63) // 64) * 64
+    host_in = torch.empty(at, dtype=tdt).pin_memory()
+    hv = host_in.numpy()
+    for m, o in zip(mats, offs):
+        n = m.shape[0]
+        hv[o:o + n * n] = np.ascontiguousarray(m.T).reshape(-1).astype(npdt)
+    host_out = torch.empty_like(host_in).pin_memory()
+    dA = host_in.to(dev)
+    dE = torch.empty_like(dA)
+    esz = dA.element_size()
+    IntArr = ctypes.c_int * count
+    PtrArr = ctypes.c_void_p * count
+    h_n = IntArr(*ns)
+    h_A = PtrArr(*[dA.data_ptr() + o * esz for o in offs])
+    h_E = PtrArr(*[dE.data_ptr() + o * esz for o in offs])
+    stream = torch.cuda.Stream(device=dev)
+    h = ctypes.c_void_p()
+    assert lib.calamanCreate(ctypes.byref(h)).ok
+    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
+    nb = ctypes.c_size_t()
+    intp = ctypes.cast(h_n, capi.c_int_p)
+    assert getattr(lib, f"calaman_expm_batched_bufferSize_{suf}")(h, count, intp, ctypes.byref(nb)).ok
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    info = torch.zeros(2 * count, dtype=torch.int32, device=dev)
+    plans = (capi.ExpmPlan * count)()
+    fn = getattr(lib, f"calaman_expm_batched_{suf}")
+
+    def step():
+        st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), count, intp,
+                ctypes.cast(h_A, ctypes.POINTER(ctypes.c_void_p)), intp,
+                ctypes.cast(h_E, ctypes.POINTER(ctypes.c_void_p)), intp,
+                ctypes.c_void_p(work.data_ptr()), nb.value,
+                ctypes.cast(info.data_ptr(), capi.c_int_p), plans)
+        if not st.ok:
+            raise RuntimeError(f"expm_batched failed: {st!r}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.calamanGetLaunchCount()
+    assert lib.calamanSetKernelTiming(h, 1).ok
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                starts[i].record(stream)
+                step()
+                ends[i].record(stream)
+        torch.cuda.synchronize()
+        launches = lib.calamanGetLaunchCount() - launches0
+        kt = capi.KernelTiming()
+        assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
+        lib.calamanSetKernelTiming(h, 0)
+        total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+        e2e_ms = 0.0
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a_ev.record(stream)
+                dA.copy_(host_in, non_blocking=True)
+                step()
+                host_out.copy_(dE, non_blocking=True)
+                b_ev.record(stream)
+                b_ev.synchronize()
+                e2e_ms += a_ev.elapsed_time(b_ev)
+    torch.cuda.synchronize()
+    if any(info.cpu().tolist()):
+        raise RuntimeError("an LU reported a zero pivot")
+    total_ms, e2e_ms = _max_over_ranks(torch, dist, dev, [total_ms, e2e_ms])
+    value = world * count * args.steps / (total_ms * 1e-3)
+    e2e_value = world * count * args.steps / (e2e_ms * 1e-3)
+    if rank == 0:
+        pl = list(plans)
+        flops = sum(expm_flops(n, p.m, p.s, False) for n, p in zip(ns, pl))
+        peak, peak_src = _bf16_peak()
+        achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
+        acc = {}
+        if suf == "s":
+            # the FP32 tier against the FP64 tier (same widened values), all matrices
+            out32 = host_out.numpy()
+            h64 = torch.from_numpy(host_in.numpy().astype(np.float64)).to(dev)
+            e64 = torch.empty_like(h64)
+            nb64 = ctypes.c_size_t()
+            assert lib.calaman_expm_batched_bufferSize_d(h, count, intp, ctypes.byref(nb64)).ok
+            w64 = torch.empty(nb64.value, dtype=torch.uint8, device=dev)
+            A64 = PtrArr(*[h64.data_ptr() + o * 8 for o in offs])
+            E64 = PtrArr(*[e64.data_ptr() + o * 8 for o in offs])
+            st = lib.calaman_expm_batched_d(h, h, ctypes.c_void_p(stream.cuda_stream), count, intp,
+                                            ctypes.cast(A64, ctypes.POINTER(ctypes.c_void_p)), intp,
+                                            ctypes.cast(E64, ctypes.POINTER(ctypes.c_void_p)), intp,
+                                            ctypes.c_void_p(w64.data_ptr()), nb64.value,
+                                            ctypes.cast(info.data_ptr(), capi.c_int_p), None)
+            assert st.ok, st
+            torch.cuda.synchronize()
+            ref = e64.cpu().numpy()
+            del w64, h64, e64
+            worst = 0.0
+            for n, o in zip(ns, offs):
+                x, y = out32[o:o + n * n].astype(np.float64), ref[o:o + n * n]
+                worst = max(worst, float(np.linalg.norm(x - y) / np.linalg.norm(y)))
+            acc["max_rel_frob_vs_fp64_tier"] = worst
+        baseline = None
+        if world == 1 and not args.no_cpu:
+            baseline = batched_cpu_sample(mats, suf, seconds=10.0)
+        n_s_pos = sum(1 for p in pl if p.s > 0)
+        line = {
+            "metric": METRIC, "value": value, "unit": "expm/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if suf == "s" else "f64", "data": "synthetic (seeded)",
+            "config": {"workload": args.config, "desc": cfg["desc"], "matrices": count,
+                       "algorithmic_flops_per_batch": flops,
+                       "matrices_with_squarings": n_s_pos,
+                       "l2": "inputs (%.0f MB) larger than L2" % (host_in.numel() * esz / 1e6),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "tflops": flops * value / count / 1e12,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if achieved else None, "traffic": None,
+                         "kernel": "grouped dense-product phases (every grouped GEMM launch)",
+                         "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
+                         "peak_source": peak_src},
+            "cpu_baseline": baseline,
+            "e2e": {"value": e2e_value, "unit": "expm/s",
+                    "h2d_bytes_per_step": sum(n * n for n in ns) * esz,
+                    "d2h_bytes_per_step": sum(n * n for n in ns) * esz},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    lib.calamanDestroy(h)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def batched_cpu_sample(mats, suf, seconds=10.0):
+    """The oracle on the first matrices of the batch until `seconds` pass."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    done, t0 = 0, time.perf_counter()
+    for m in mats:
+        O.expm(m.astype(np.float64), single=suf == "s")
+        done += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": done / el, "unit": "expm/s", "cores": cores, "kind": "port",
+            "sample": f"the first {done} matrices of the batch ({el:.1f} s), C oracle with "
+                      f"{cores} threads"}
+
+
+def run_vjp(args, cfg):
+    """One step = the adjoint of expm for the whole workload through the C ABI
+    (calaman_expm_vjp_<t>): one 2048^2 call, or 512 calls of 128^2."""
+    torch, world, rank, local, dev, dist = _init_dist()
+    from calaman_g_b200 import capi
+
+    lib = capi.load()
+    suf, n = cfg["suf"], cfg["n"]
+    count = cfg.get("count", 1)
+    tdt = torch.float32 if suf == "s" else torch.float64
+    pairs = [vjp_pair(n, cfg["norm"], 7000 + i) for i in range(count)]
+    host_a = torch.stack([torch.from_numpy(np.ascontiguousarray(a.T)) for a, _ in pairs]).to(tdt).pin_memory()
+    host_g = torch.stack([torch.from_numpy(np.ascontiguousarray(g.T)) for _, g in pairs]).to(tdt).pin_memory()
+    host_d = torch.empty_like(host_a).pin_memory()
+    dA, dG = host_a.to(dev), host_g.to(dev)
+    dD = torch.empty_like(dA)
+    stream = torch.cuda.Stream(device=dev)
+    h = ctypes.c_void_p()
+    assert lib.calamanCreate(ctypes.byref(h)).ok
+    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
+    nb = ctypes.c_size_t()
+    assert getattr(lib, f"calaman_expm_vjp_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    info = torch.zeros(2, dtype=torch.int32, device=dev)
+    plan = capi.ExpmPlan()
+    fn = getattr(lib, f"calaman_expm_vjp_{suf}")
+    esz = dA.element_size()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        for i in range(count):
+            st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), n,
+                    ctypes.c_void_p(dA.data_ptr() + i * n * n * esz), n,
+                    ctypes.c_void_p(dG.data_ptr() + i * n * n * esz), n,
+                    ctypes.c_void_p(dD.data_ptr() + i * n * n * esz), n, None, n,
+                    ctypes.c_void_p(work.data_ptr()), nb.value,
+                    ctypes.cast(info.data_ptr(), capi.c_int_p), ctypes.byref(plan))
+            if not st.ok:
+                raise RuntimeError(f"expm_vjp failed: {st!r}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.calamanGetLaunchCount()
+    assert lib.calamanSetKernelTiming(h, 1).ok
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                starts[i].record(stream)
+                step()
+                ends[i].record(stream)
+        torch.cuda.synchronize()
+        launches = lib.calamanGetLaunchCount() - launches0
+        kt = capi.KernelTiming()
+        assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
+        lib.calamanSetKernelTiming(h, 0)
+        total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+        e2e_ms = 0.0
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a_ev.record(stream)
+                dA.copy_(host_a, non_blocking=True)
+                dG.copy_(host_g, non_blocking=True)
+                step()
+                host_d.copy_(dD, non_blocking=True)
+                b_ev.record(stream)
+                b_ev.synchronize()
+                e2e_ms += a_ev.elapsed_time(b_ev)
+    torch.cuda.synchronize()
+    total_ms, e2e_ms = _max_over_ranks(torch, dist, dev, [total_ms, e2e_ms])
+    value = world * count * args.steps / (total_ms * 1e-3)
+    e2e_value = world * count * args.steps / (e2e_ms * 1e-3)
+    if rank == 0:
+        flops = vjp_flops(n, plan.m, plan.s)
+        if suf == "s":
+            peak, peak_src = _bf16_peak()
+        else:
+            peak, peak_src = measure_fp64_peak(torch, dev, False), "cuBLAS float64 GEMM 4096^3 in this run"
+        achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
+        acc = {}
+        from oracle import oracle as O
+
+        k = 0 if n > 512 else min(count, 4)
+        for i in range(k):
+            a, g = pairs[i]
+            ref, _, _ = O.expm_vjp_frechet(a.astype(np.float32).astype(np.float64) if suf == "s" else a,
+                                           g.astype(np.float32).astype(np.float64) if suf == "s" else g,
+                                           single=suf == "s")
+            got = host_d[i].numpy().T.astype(np.float64)
+            acc.setdefault("rel_frob_vs_oracle", []).append(
+                float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+        line = {
+            "metric": METRIC.replace("expm/s", "vjp/s"), "value": value, "unit": "vjp/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if suf == "s" else "f64", "data": "synthetic (seeded)",
+            "config": {"workload": args.config, "desc": cfg["desc"], "pairs": count,
+                       "plan": {"m": plan.m, "s": plan.s},
+                       "algorithmic_flops_per_vjp": flops,
+                       "l2": "flushed before every timed step (256 MiB write, untimed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "tflops": flops * value / 1e12,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if achieved else None, "traffic": None,
+                         "kernel": "dense products (every GEMM launch in the timed steps)",
+                         "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
+                         "peak_source": peak_src},
+            "cpu_baseline": None,
+            "e2e": {"value": e2e_value, "unit": "vjp/s",
+                    "h2d_bytes_per_step": 2 * count * n * n * esz,
+                    "d2h_bytes_per_step": count * n * n * esz},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    lib.calamanDestroy(h)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -383,8 +803,13 @@ def main():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     args = p.parse_args()
     cfg = CONFIGS[args.config]
+    kind = cfg.get("kind", "single")
     if args.impl == "reference":
         run_reference(args, cfg)
+    elif kind == "batched":
+        run_batched(args, cfg)
+    elif kind == "vjp":
+        run_vjp(args, cfg)
     else:
         run_ours(args, cfg)
 

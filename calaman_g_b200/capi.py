@@ -22,6 +22,7 @@ SUCCESS = 0
 NOT_INITIALIZED = 1
 ALLOC_FAILED = 3
 INVALID_VALUE = 7
+NOT_SUPPORTED = 15
 DOMAIN_BLAS, DOMAIN_SOLVER, DOMAIN_RUNTIME = 0, 1, 2
 POINTER_MODE_HOST, POINTER_MODE_DEVICE = 0, 1
 
@@ -138,6 +139,12 @@ SIGNATURES["calaman_gemm_bf16x_bufferSize"] = (Status, [c_int, c_int, c_int, c_i
 SIGNATURES["calaman_gemm_bf16x_s"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
 SIGNATURES["calaman_expm_noalloc_d"] = (Status, [_H, c_void_p, c_int, c_void_p, c_int, c_void_p,
                                                  c_int, c_int_p, ctypes.POINTER(ExpmPlan)])
+# expm_batched: blas, solver, stream, batch, h_n, h_A, h_lda, h_E, h_lde, work, bytes, info, plans
+_BATCHED = [_H, _H, c_void_p, c_int, c_int_p, ctypes.POINTER(c_void_p), c_int_p,
+            ctypes.POINTER(c_void_p), c_int_p, c_void_p, c_size_t, c_int_p, ctypes.POINTER(ExpmPlan)]
+for _suf in ("s", "d"):
+    SIGNATURES[f"calaman_expm_batched_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int_p, c_size_t_p])
+    SIGNATURES[f"calaman_expm_batched_{_suf}"] = (Status, _BATCHED)
 SIGNATURES["calamanSetFloatSplit"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetFloatSplit"] = (Status, [_H, c_int_p])
 

@@ -1,0 +1,1004 @@
+// batched.cu -- expm of many small matrices (n <= 256) in one call.
+//
+// New entry point (calaman_G evaluates one matrix per call): every matrix of
+// the batch gets its own (m, s) from its own 1-norm, exactly as expm would
+// pick, and the whole batch advances phase by phase -- one kernel launch per
+// phase covers every matrix, whatever its size and degree:
+//
+//   norm -> (one readback, plans on the host) -> scale -> A2 -> A4 -> A6 -> A8
+//   -> even/odd combinations -> [m = 13: W += A6 T, V += A6 Z] -> U = X W
+//   -> p = V + U, q = V - U -> LU(q) + solve (fused, one CTA per matrix)
+//   -> s squarings (FP64 for the single tier) -> write-back
+//
+// Each kernel reads a per-matrix descriptor table (pointers, n, ld, plan) and
+// derives its own operands, so a phase in which a matrix takes no part costs
+// that matrix nothing but an early exit. The dense products run on a grouped
+// GEMM: one CTA per 64 x 64 output tile, tiles of all matrices numbered
+// consecutively, each CTA finding its matrix by binary search on the tile
+// prefix sums. The LU and the n-right-hand-side solve of a matrix run in one
+// CTA of 256 threads in which thread i owns row i (pivot search, swaps,
+// rank-updates) or column i (swap gathers, triangular solves of the diagonal
+// blocks), with panels of 32 columns.
+#include <cfloat>
+#include <vector>
+
+#include "expm_common.cuh"
+
+namespace clm {
+namespace {
+
+constexpr int kBatchedMaxN = 256;
+constexpr int kBThreads = 256;  // = kBatchedMaxN: one thread per row / column
+constexpr int kBPanel = 32;
+constexpr int kGTile = 64;      // grouped GEMM output tile
+constexpr int kGK = 16;         // grouped GEMM k-chunk
+constexpr int kEwChunk = 16384; // elements per elementwise CTA
+
+// Per-matrix buffers (ld = n): X (scaled input, later the Pade quotient),
+// P0..P3 (even powers; P0 is also U and p), T (m = 13 odd temp), V, W, and
+// for the squarings two buffers of the wide type.
+template <typename T, typename Wd>
+struct BItem {
+  const T *A;
+  T *E;
+  T *X, *P0, *P1, *P2, *P3, *Tt, *V, *W;
+  Wd *wa, *wb;
+  int n, lda, lde, id;  // id: the matrix's index in the caller's batch (d_info)
+};
+
+struct BPlan {
+  int m, s, np, pad;
+};
+
+enum BPhase { kPhA2 = 0, kPhA4, kPhA6, kPhA8, kPhM13, kPhU, kPhSq };
+
+// Pade coefficients b_0..b_13 of each degree, indexed by (m - 3) / 2 for
+// m < 13 and 4 for m = 13.
+__constant__ double c_pade[5][14];
+
+template <typename To> __device__ __forceinline__ To convert_elem(float x);
+template <> __device__ __forceinline__ float convert_elem<float>(float x) { return x; }
+template <> __device__ __forceinline__ double convert_elem<double>(float x) { return (double)x; }
+template <typename To> __device__ __forceinline__ To convert_elem(double x);
+template <> __device__ __forceinline__ double convert_elem<double>(double x) { return x; }
+template <> __device__ __forceinline__ float convert_elem<float>(double x) { return (float)x; }
+
+__device__ __forceinline__ int degree_slot(int m) { return m == 13 ? 4 : (m - 3) / 2; }
+
+// ---- 1-norm of every matrix: one CTA per matrix --------------------------
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) b_norm_kernel(const BItem<T, Wd> *__restrict__ items,
+                                                     double *__restrict__ norms) {
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double best = 0.0;
+  bool nan = false;
+  for (int c = warp; c < it.n; c += 8) {
+    double sum = 0.0;
+    for (int r = lane; r < it.n; r += 32) sum += modulus(it.A[(std::size_t)c * it.lda + r]);
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    nan |= sum != sum;
+    best = fmax(best, sum);
+  }
+  __shared__ double red[8];
+  __shared__ int red_nan[8];
+  if (lane == 0) {
+    red[warp] = best;
+    red_nan[warp] = nan;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    int anynan = 0;
+    for (int w = 0; w < 8; ++w) {
+      b = fmax(b, red[w]);
+      anynan |= red_nan[w];
+    }
+    norms[blockIdx.x] = anynan ? (double)NAN : b;
+  }
+}
+
+// ---- elementwise phases: CTA (chunk, matrix) ------------------------------
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) b_scale_kernel(const BItem<T, Wd> *__restrict__ items,
+                                                      const BPlan *__restrict__ plans) {
+  using R = typename elem<T>::real;
+  const BPlan pl = plans[blockIdx.x];
+  if (pl.s == 0) return;
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const int nn = it.n * it.n;
+  const R f = (R)ldexp(1.0, -pl.s);
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / it.n, r = e - c * it.n;
+    it.X[e] = scale(it.A[(std::size_t)c * it.lda + r], f);
+  }
+}
+
+// V, W from the even powers (m < 13); for m = 13 also the odd temp T and the
+// even temp (into P3, unused at m = 13):
+//   T = b9 A2 + b11 A4 + b13 A6,  W = b1 I + b3 A2 + b5 A4 + b7 A6,
+//   Z = b8 A2 + b10 A4 + b12 A6,  V = b0 I + b2 A2 + b4 A4 + b6 A6.
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) b_even_odd_kernel(const BItem<T, Wd> *__restrict__ items,
+                                                         const BPlan *__restrict__ plans) {
+  using R = typename elem<T>::real;
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const BPlan pl = plans[blockIdx.x];
+  const double *b = c_pade[degree_slot(pl.m)];
+  const int n = it.n, nn = n * n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  const T *P[4] = {it.P0, it.P1, it.P2, it.P3};
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    const bool diag = r == c;
+    if (pl.m != 13) {
+      T v = elem<T>::zero(), w = elem<T>::zero();
+      for (int k = 0; k < pl.np; ++k) {
+        const T x = P[k][e];
+        v = rfma((R)b[2 * k + 2], x, v);
+        w = rfma((R)b[2 * k + 3], x, w);
+      }
+      if (diag) {
+        v = add_real(v, (R)b[0]);
+        w = add_real(w, (R)b[1]);
+      }
+      it.V[e] = v;
+      it.W[e] = w;
+    } else {
+      const T x1 = it.P0[e], x2 = it.P1[e], x3 = it.P2[e];
+      T t = scale(x1, (R)b[9]), w = scale(x1, (R)b[3]), z = scale(x1, (R)b[8]), v = scale(x1, (R)b[2]);
+      t = rfma((R)b[11], x2, t);
+      w = rfma((R)b[5], x2, w);
+      z = rfma((R)b[10], x2, z);
+      v = rfma((R)b[4], x2, v);
+      t = rfma((R)b[13], x3, t);
+      w = rfma((R)b[7], x3, w);
+      z = rfma((R)b[12], x3, z);
+      v = rfma((R)b[6], x3, v);
+      if (diag) {
+        w = add_real(w, (R)b[1]);
+        v = add_real(v, (R)b[0]);
+      }
+      it.Tt[e] = t;
+      it.W[e] = w;
+      it.P3[e] = z;
+      it.V[e] = v;
+    }
+  }
+}
+
+// p = V + U over P0 (which holds U), q = V - U over V
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) b_split_kernel(const BItem<T, Wd> *__restrict__ items) {
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const int nn = it.n * it.n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const T u = it.P0[e], v = it.V[e];
+    it.P0[e] = add(v, u);
+    it.V[e] = sub(v, u);
+  }
+}
+
+// s > 0: wa = (Wd) X, the Pade quotient
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) b_widen_kernel(const BItem<T, Wd> *__restrict__ items,
+                                                      const BPlan *__restrict__ plans) {
+  if (plans[blockIdx.x].s == 0) return;
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const int nn = it.n * it.n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x)
+    it.wa[e] = convert_elem<Wd>(it.X[e]);
+}
+
+// s > 0: E = (T) the last square (wa for even s, wb for odd s)
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) b_narrow_kernel(const BItem<T, Wd> *__restrict__ items,
+                                                       const BPlan *__restrict__ plans) {
+  const int s = plans[blockIdx.x].s;
+  if (s == 0) return;
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const Wd *src = (s & 1) ? it.wb : it.wa;
+  const int n = it.n, nn = n * n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    it.E[(std::size_t)c * it.lde + r] = convert_elem<T>(src[e]);
+  }
+}
+
+// ---- grouped GEMM: C = A B (+ C), n x n x n per matrix, one 64 x 64 tile per CTA
+template <typename U>
+struct GOps {
+  const U *A, *B;
+  U *C;
+  int lda, ldb, ldc;
+  bool acc;
+};
+
+template <typename T, typename Wd>
+__device__ __forceinline__ bool phase_ops_t(const BItem<T, Wd> &it, const BPlan &pl, int phase, int sub,
+                                            GOps<T> &o) {
+  const T *X = pl.s > 0 ? it.X : it.A;
+  const int ldx = pl.s > 0 ? it.n : it.lda;
+  o.lda = o.ldb = o.ldc = it.n;
+  o.acc = false;
+  switch (phase) {
+  case kPhA2:
+    o.A = X; o.lda = ldx; o.B = X; o.ldb = ldx; o.C = it.P0;
+    return true;
+  case kPhA4:
+    o.A = it.P0; o.B = it.P0; o.C = it.P1;
+    return pl.np >= 2;
+  case kPhA6:
+    o.A = it.P1; o.B = it.P0; o.C = it.P2;
+    return pl.np >= 3;
+  case kPhA8:
+    o.A = it.P1; o.B = it.P1; o.C = it.P3;
+    return pl.np >= 4;
+  case kPhM13:
+    o.A = it.P2; o.B = sub ? it.P3 : it.Tt; o.C = sub ? it.V : it.W; o.acc = true;
+    return pl.m == 13;
+  case kPhU:
+    o.A = X; o.lda = ldx; o.B = it.W; o.C = it.P0;
+    return true;
+  default:
+    return false;
+  }
+}
+
+template <typename T, typename Wd, typename U, bool kSquare>
+__global__ void __launch_bounds__(256)
+    b_gemm_kernel(const BItem<T, Wd> *__restrict__ items, const BPlan *__restrict__ plans,
+                  const int *__restrict__ tile_prefix, int batch, int phase, int ksq) {
+  // the matrix of this tile: last i with tile_prefix[i] <= blockIdx.x
+  const int tile = blockIdx.x;
+  int lo = 0, hi = batch - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_prefix[mid] <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const BItem<T, Wd> it = items[lo];
+  const BPlan pl = plans[lo];
+  GOps<U> o;
+  if constexpr (kSquare) {
+    if (pl.s < ksq) return;
+    // square k reads wa for odd k, wb for even k
+    o.A = o.B = (ksq & 1) ? it.wa : it.wb;
+    o.C = (ksq & 1) ? it.wb : it.wa;
+    o.lda = o.ldb = o.ldc = it.n;
+    o.acc = false;
+  } else {
+    if (!phase_ops_t<T, Wd>(it, pl, phase, blockIdx.y, o)) return;
+  }
+  const int n = it.n;
+  const int tn = (n + kGTile - 1) / kGTile;
+  const int local = tile - tile_prefix[lo];
+  const int m0 = (local % tn) * kGTile, n0 = (local / tn) * kGTile;
+
+  __shared__ U As[kGK][kGTile + 4];
+  __shared__ U Bs[kGK][kGTile + 4];
+  const int t = threadIdx.x;
+  const int tx = t & 15, ty = t >> 4;  // rows tx + 16 i, columns ty + 16 j
+  U acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = elem<U>::zero();
+
+  // global -> register staging: A tile (64 rows x 16 k), B tile (16 k x 64 cols)
+  const int ar = t & 63, ak = t >> 6;   // A: rows ar, k = ak + 4 q
+  const int bk = t & 15, bc = t >> 4;   // B: k = bk, columns bc + 16 q
+  U ra[4], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = m0 + ar, k = k0 + ak + 4 * q;
+      ra[q] = (r < n && k < n) ? o.A[(std::size_t)k * o.lda + r] : elem<U>::zero();
+      const int c = n0 + bc + 16 * q, kb = k0 + bk;
+      rb[q] = (c < n && kb < n) ? o.B[(std::size_t)c * o.ldb + kb] : elem<U>::zero();
+    }
+  };
+  load(0);
+  for (int k0 = 0; k0 < n; k0 += kGK) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      As[ak + 4 * q][ar] = ra[q];
+      Bs[bk][bc + 16 * q] = rb[q];
+    }
+    __syncthreads();
+    if (k0 + kGK < n) load(k0 + kGK);
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      U a[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmac(a[i], bv[j], acc[i][j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = n0 + ty + 16 * j;
+    if (c >= n) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = m0 + tx + 16 * i;
+      if (r >= n) continue;
+      U *dst = o.C + (std::size_t)c * o.ldc + r;
+      *dst = o.acc ? add(*dst, acc[i][j]) : acc[i][j];
+    }
+  }
+}
+
+// ---- LU with partial pivoting of q and the solve q R = p: one CTA per matrix
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(kBThreads)
+    b_lu_solve_kernel(const BItem<T, Wd> *__restrict__ items, const BPlan *__restrict__ plans,
+                      int *__restrict__ info) {
+  using R = typename elem<T>::real;
+  const BItem<T, Wd> it = items[blockIdx.x];
+  const BPlan pl = plans[blockIdx.x];
+  const int n = it.n;
+  T *Q = it.V;         // factored in place (ld n)
+  const T *B = it.P0;  // right-hand side p (ld n)
+  T *D = pl.s > 0 ? it.X : it.E;
+  const int ldd = pl.s > 0 ? n : it.lde;
+  const int t = threadIdx.x;
+
+  // dynamic: blk[kBPanel][kBThreads] (U12 rows / solved right-hand-side block
+  // rows), then diag[kBPanel][kBPanel + 1] (L11 / U11 of the current block)
+  extern __shared__ __align__(16) unsigned char b_smem[];
+  auto blk = reinterpret_cast<T(*)[kBThreads]>(b_smem);
+  auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * kBThreads);
+  __shared__ T prow[kBPanel];               // pivot row of the current column
+  __shared__ T xrow[2][kBPanel];            // row exchange slots
+  __shared__ int perm[kBThreads];           // P: row i of P q is row perm[i] of q
+  __shared__ int pos[kBThreads];            // panel-local composite of the swaps
+  __shared__ int piv[kBPanel];
+  __shared__ double rv[8];
+  __shared__ int ri[8];
+  __shared__ int first_zero;
+
+  if (t < n) perm[t] = t;
+  if (t == 0) first_zero = 0;
+
+  T r[kBPanel];
+  for (int k = 0; k < n; k += kBPanel) {
+    const int jb = min(kBPanel, n - k);
+    // my row of the panel (rows >= k take part)
+    const bool mine = t >= k && t < n;
+#pragma unroll
+    for (int j = 0; j < kBPanel; ++j)
+      r[j] = (mine && j < jb) ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
+    if (t < n) pos[t] = t;
+    __syncthreads();
+#pragma unroll 1
+    for (int j = 0; j < jb; ++j) {
+      // pivot: largest |Re| + |Im| among rows >= k + j, first index on ties
+      T rj = elem<T>::zero();
+#pragma unroll
+      for (int c = 0; c < kBPanel; ++c)
+        if (c == j) rj = r[c];
+      double v = (mine && t >= k + j) ? abs1(rj) : -1.0;
+      int idx = t;
+      for (int o = 16; o; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi < idx)) {
+          v = ov;
+          idx = oi;
+        }
+      }
+      if ((t & 31) == 0) {
+        rv[t >> 5] = v;
+        ri[t >> 5] = idx;
+      }
+      __syncthreads();
+      if (t == 0) {
+        double bv = rv[0];
+        int bi = ri[0];
+        for (int w = 1; w < 8; ++w)
+          if (rv[w] > bv || (rv[w] == bv && ri[w] < bi)) {
+            bv = rv[w];
+            bi = ri[w];
+          }
+        piv[j] = bi;
+        const int a = k + j;
+        if (bi != a) {
+          const int tp = perm[a];
+          perm[a] = perm[bi];
+          perm[bi] = tp;
+          const int tq = pos[a];
+          pos[a] = pos[bi];
+          pos[bi] = tq;
+        }
+      }
+      __syncthreads();
+      const int p = piv[j], a = k + j;
+      if (p != a) {
+        if (t == a) {
+#pragma unroll
+          for (int c = 0; c < kBPanel; ++c) xrow[0][c] = r[c];
+        }
+        if (t == p) {
+#pragma unroll
+          for (int c = 0; c < kBPanel; ++c) xrow[1][c] = r[c];
+        }
+        __syncthreads();
+        if (t == a) {
+#pragma unroll
+          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[1][c];
+        }
+        if (t == p) {
+#pragma unroll
+          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[0][c];
+        }
+      }
+      if (t == a) {
+#pragma unroll
+        for (int c = 0; c < kBPanel; ++c) prow[c] = r[c];
+      }
+      __syncthreads();
+      const T pv = prow[j];
+      if (t == 0 && is_zero(pv) && first_zero == 0) first_zero = a + 1;
+      if (mine && t > a && !is_zero(pv)) {
+        const bool use_recip = abs1(pv) >= (sizeof(R) == 4 ? (double)FLT_MIN : DBL_MIN);
+        const T rcp = divide(elem<T>::one(), pv);
+        T l = elem<T>::zero();
+#pragma unroll
+        for (int c = 0; c < kBPanel; ++c)
+          if (c == j) l = use_recip ? mul(r[c], rcp) : divide(r[c], pv);
+#pragma unroll
+        for (int c = 0; c < kBPanel; ++c) {
+          if (c == j) r[c] = l;
+          else if (c > j && c < jb) r[c] = sub(r[c], mul(l, prow[c]));
+        }
+      }
+    }
+    // panel back to memory; L11 / U11 block to shared memory
+    if (mine) {
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j)
+        if (j < jb) Q[(std::size_t)(k + j) * n + t] = r[j];
+    }
+    if (t >= k && t < k + jb) {
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j)
+        if (j < jb) diag[t - k][j] = r[j];
+    }
+    __syncthreads();
+    // columns outside the panel: apply the panel's swaps (rows >= k + jb only
+    // ever receive rows of the top block [k, k + jb)); right of the panel, also
+    // solve the top block with the unit-lower L11
+    if (t < n - jb) {
+      const int c = t < k ? t : t + jb;
+      T *col = Q + (std::size_t)c * n;
+      T top[kBPanel];
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j) top[j] = j < jb ? col[k + j] : elem<T>::zero();
+      T x[kBPanel];
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j) {
+        x[j] = elem<T>::zero();
+        if (j < jb) {
+          const int src = pos[k + j];
+          if (src >= k + jb) x[j] = col[src];
+          else {
+#pragma unroll
+            for (int q = 0; q < kBPanel; ++q)
+              if (q == src - k) x[j] = top[q];
+          }
+        }
+      }
+      // displaced rows below the block take their top-block row
+#pragma unroll 1
+      for (int j = 0; j < jb; ++j) {
+        const int d = piv[j];
+        if (d >= k + jb) {
+          const int src = pos[d] - k;
+          T v = elem<T>::zero();
+#pragma unroll
+          for (int q = 0; q < kBPanel; ++q)
+            if (q == src) v = top[q];
+          col[d] = v;
+        }
+      }
+      if (c >= k + jb) {
+#pragma unroll
+        for (int j = 0; j < kBPanel; ++j)
+#pragma unroll
+          for (int q = 0; q < kBPanel; ++q)
+            if (q < j && j < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+#pragma unroll
+        for (int j = 0; j < kBPanel; ++j)
+          if (j < jb) blk[j][c] = x[j];
+      }
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j)
+        if (j < jb) col[k + j] = x[j];
+    }
+    __syncthreads();
+    // trailing update A22 -= L21 U12, thread i owns row i
+    if (t >= k + jb && t < n) {
+      for (int c = k + jb; c < n; ++c) {
+        T acc = Q[(std::size_t)c * n + t];
+#pragma unroll
+        for (int j = 0; j < kBPanel; ++j)
+          if (j < jb) acc = sub(acc, mul(r[j], blk[j][c]));
+        Q[(std::size_t)c * n + t] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    info[2 * it.id] = first_zero;
+    info[2 * it.id + 1] = 0;
+  }
+
+  // ---- solve q R = p:  R = U^-1 L^-1 (P p) -------------------------------
+  if (t < n) {
+    const int src = perm[t];
+    for (int c = 0; c < n; ++c) D[(std::size_t)c * ldd + t] = B[(std::size_t)c * n + src];
+  }
+  __syncthreads();
+  // forward, unit lower
+  for (int k = 0; k < n; k += kBPanel) {
+    const int jb = min(kBPanel, n - k);
+    for (int e = t; e < jb * jb; e += kBThreads) {
+      const int j = e / jb, q = e - j * jb;  // row j, column q of the block
+      diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
+    }
+    __syncthreads();
+    if (t < n) {
+      T *col = D + (std::size_t)t * ldd;
+      T x[kBPanel];
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? col[k + j] : elem<T>::zero();
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j)
+#pragma unroll
+        for (int q = 0; q < kBPanel; ++q)
+          if (q < j && j < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j)
+        if (j < jb) {
+          blk[j][t] = x[j];
+          col[k + j] = x[j];
+        }
+    }
+    __syncthreads();
+    if (t >= k + jb && t < n) {
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j) r[j] = j < jb ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
+      for (int c = 0; c < n; ++c) {
+        T acc = D[(std::size_t)c * ldd + t];
+#pragma unroll
+        for (int j = 0; j < kBPanel; ++j)
+          if (j < jb) acc = sub(acc, mul(r[j], blk[j][c]));
+        D[(std::size_t)c * ldd + t] = acc;
+      }
+    }
+    __syncthreads();
+  }
+  // backward, non-unit upper
+  for (int k = ((n - 1) / kBPanel) * kBPanel; k >= 0; k -= kBPanel) {
+    const int jb = min(kBPanel, n - k);
+    for (int e = t; e < jb * jb; e += kBThreads) {
+      const int j = e / jb, q = e - j * jb;
+      diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
+    }
+    __syncthreads();
+    if (t < jb) prow[t] = divide(elem<T>::one(), diag[t][t]);
+    __syncthreads();
+    if (t < n) {
+      T *col = D + (std::size_t)t * ldd;
+      T x[kBPanel];
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? col[k + j] : elem<T>::zero();
+#pragma unroll
+      for (int j = kBPanel - 1; j >= 0; --j) {
+        if (j < jb) {
+#pragma unroll
+          for (int q = 0; q < kBPanel; ++q)
+            if (q > j && q < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+          x[j] = mul(x[j], prow[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j)
+        if (j < jb) {
+          blk[j][t] = x[j];
+          col[k + j] = x[j];
+        }
+    }
+    __syncthreads();
+    if (t < k) {
+#pragma unroll
+      for (int j = 0; j < kBPanel; ++j) r[j] = j < jb ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
+      for (int c = 0; c < n; ++c) {
+        T acc = D[(std::size_t)c * ldd + t];
+#pragma unroll
+        for (int j = 0; j < kBPanel; ++j)
+          if (j < jb) acc = sub(acc, mul(r[j], blk[j][c]));
+        D[(std::size_t)c * ldd + t] = acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---- precision conversion between the caller's buffers and FP64 copies ----
+struct BConv {
+  const void *src;
+  void *dst;
+  int n, lds, ldd, pad;
+};
+
+template <typename Ti, typename To>
+__global__ void __launch_bounds__(256) b_conv_kernel(const BConv *__restrict__ conv) {
+  const BConv cv = conv[blockIdx.x];
+  const Ti *src = static_cast<const Ti *>(cv.src);
+  To *dst = static_cast<To *>(cv.dst);
+  const int n = cv.n, nn = n * n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    dst[(std::size_t)c * cv.ldd + r] = convert_elem<To>(src[(std::size_t)c * cv.lds + r]);
+  }
+}
+
+// ---- host side -------------------------------------------------------------
+// Workspace: [items (compute type T) | items (FP64) | plans x2 | tile prefixes
+// x2 | norms | conversion tables x2 | one slab per matrix]. A matrix's slab is
+// large enough for whichever precision its plan sends it to: the single tier
+// keeps matrices with s = 0 in FP32 and evaluates matrices with s > 0 wholly
+// in FP64 (their FP32 Pade quotient would carry ~1e-7 relative error into s
+// squarings, each of which doubles it), from an FP64 copy of the input into
+// an FP64 result that is rounded once into the caller's output.
+template <typename T>
+struct BLayout {
+  using Hi = typename Wide<T>::type;
+  static constexpr bool kSplit = !std::is_same<T, Hi>::value;
+  std::size_t items_lo = 0, items_hi = 0, plans_lo = 0, plans_hi = 0, prefix_lo = 0, prefix_hi = 0,
+              norms = 0, conv_in = 0, conv_out = 0, total = 0;
+  std::vector<std::size_t> slab;
+  template <typename C> static std::size_t slab_of(int n) {
+    using W = typename Wide<C>::type;
+    const std::size_t nn = (std::size_t)n * n;
+    return 8 * align_up(nn * sizeof(C), 256) + 2 * align_up(nn * sizeof(W), 256);
+  }
+  static std::size_t slab_bytes(int n) {
+    if (!kSplit) return slab_of<T>(n);
+    const std::size_t nn = (std::size_t)n * n;
+    return std::max(slab_of<T>(n), slab_of<Hi>(n) + 2 * align_up(nn * sizeof(Hi), 256));
+  }
+  void plan(int batch, const int *h_n) {
+    Layout L(nullptr);
+    items_lo = L.used;  L.take<BItem<T, Hi>>(batch);
+    items_hi = L.used;  L.take<BItem<Hi, Hi>>(kSplit ? batch : 0);
+    plans_lo = L.used;  L.take<BPlan>(batch);
+    plans_hi = L.used;  L.take<BPlan>(kSplit ? batch : 0);
+    prefix_lo = L.used; L.take<int>(batch + 1);
+    prefix_hi = L.used; L.take<int>(kSplit ? batch + 1 : 0);
+    norms = L.used;     L.take<double>(batch);
+    conv_in = L.used;   L.take<BConv>(kSplit ? batch : 0);
+    conv_out = L.used;  L.take<BConv>(kSplit ? batch : 0);
+    slab.resize(batch);
+    std::size_t at = L.used;
+    for (int i = 0; i < batch; ++i) {
+      slab[i] = at;
+      at += slab_bytes(h_n[i]);
+    }
+    total = at;
+  }
+};
+
+bool g_pade_uploaded[64] = {};
+
+cudaError_t upload_pade_table(int device) {
+  if (device >= 0 && device < 64 && g_pade_uploaded[device]) return cudaSuccess;
+  double tab[5][14] = {};
+  const int ms[5] = {3, 5, 7, 9, 13};
+  for (int k = 0; k < 5; ++k)
+    for (int i = 0; i <= ms[k]; ++i) tab[k][i] = pade_coeffs(ms[k])[i];
+  const cudaError_t e = cudaMemcpyToSymbol(c_pade, tab, sizeof(tab));
+  if (e == cudaSuccess && device >= 0 && device < 64) g_pade_uploaded[device] = true;
+  return e;
+}
+
+// The slab buffers of one matrix in compute type C.
+template <typename C>
+void carve_item(BItem<C, typename Wide<C>::type> &it, char *slab, int n) {
+  using W = typename Wide<C>::type;
+  const std::size_t nn = (std::size_t)n * n;
+  Layout L(slab);
+  it.X = L.take<C>(nn);
+  it.P0 = L.take<C>(nn);
+  it.P1 = L.take<C>(nn);
+  it.P2 = L.take<C>(nn);
+  it.P3 = L.take<C>(nn);
+  it.Tt = L.take<C>(nn);
+  it.V = L.take<C>(nn);
+  it.W = L.take<C>(nn);
+  it.wa = L.take<W>(nn);
+  it.wb = L.take<W>(nn);
+  it.n = n;
+}
+
+// Every phase over `count` matrices whose descriptors, plans and tile prefix
+// sums are on the device.
+// With kernel timing on (calamanSetKernelTiming), CUDA events bracket every
+// grouped-GEMM launch, recorded with the launch's algorithmic flops.
+template <typename F>
+cudaError_t timed_group(cudaStream_t s, double flops, F &&run) {
+  KernelTimer *t = tl_timer;
+  if (t == nullptr || flops <= 0.0) return run();
+  cudaEvent_t a = t->take(), b = t->take();
+  if (a == nullptr || b == nullptr) return run();
+  cudaEventRecord(a, s);
+  const cudaError_t e = run();
+  cudaEventRecord(b, s);
+  t->starts.push_back(a);
+  t->stops.push_back(b);
+  t->flops.push_back(flops);
+  return e;
+}
+
+// Algorithmic flops of a grouped-GEMM phase (k: the squaring index).
+double phase_flops(const std::vector<int> &ns, const std::vector<BPlan> &pls, int phase, int k) {
+  double f = 0.0;
+  for (std::size_t i = 0; i < ns.size(); ++i) {
+    const double cube = 2.0 * ns[i] * (double)ns[i] * ns[i];
+    const BPlan &p = pls[i];
+    switch (phase) {
+    case kPhA2: case kPhU: f += cube; break;
+    case kPhA4: f += p.np >= 2 ? cube : 0.0; break;
+    case kPhA6: f += p.np >= 3 ? cube : 0.0; break;
+    case kPhA8: f += p.np >= 4 ? cube : 0.0; break;
+    case kPhM13: f += p.m == 13 ? 2.0 * cube : 0.0; break;
+    case kPhSq: f += p.s >= k ? cube : 0.0; break;
+    default: break;
+    }
+  }
+  return f;
+}
+
+template <typename C>
+cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *d_items,
+                       const BPlan *d_plans, const int *d_prefix, int count, int tiles, int max_n,
+                       int max_s, int *d_info, const std::vector<int> &ns,
+                       const std::vector<BPlan> &pls) {
+  using W = typename Wide<C>::type;
+  cudaError_t e;
+  const dim3 ew((unsigned)count, (unsigned)((max_n * max_n + kEwChunk - 1) / kEwChunk));
+  auto gemm = [&](int phase, int ysub) -> cudaError_t {
+    return timed_group(st, phase_flops(ns, pls, phase, 0), [&] {
+      b_gemm_kernel<C, W, C, false><<<dim3(tiles, ysub), 256, 0, st>>>(d_items, d_plans, d_prefix,
+                                                                        count, phase, 0);
+      return launched();
+    });
+  };
+  b_scale_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+  if ((e = launched()) != cudaSuccess) return e;
+  for (int ph : {kPhA2, kPhA4, kPhA6, kPhA8})
+    if ((e = gemm(ph, 1)) != cudaSuccess) return e;
+  b_even_odd_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+  if ((e = launched()) != cudaSuccess) return e;
+  if ((e = gemm(kPhM13, 2)) != cudaSuccess) return e;
+  if ((e = gemm(kPhU, 1)) != cudaSuccess) return e;
+  b_split_kernel<C, W><<<ew, 256, 0, st>>>(d_items);
+  if ((e = launched()) != cudaSuccess) return e;
+  {
+    const std::size_t smem = sizeof(C) * (kBPanel * kBThreads + kBPanel * (kBPanel + 1));
+    auto kern = b_lu_solve_kernel<C, W>;
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+      return e;
+    kern<<<count, kBThreads, smem, st>>>(d_items, d_plans, d_info);
+    if ((e = launched()) != cudaSuccess) return e;
+  }
+  if (max_s > 0) {
+    b_widen_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+    if ((e = launched()) != cudaSuccess) return e;
+    for (int k = 1; k <= max_s; ++k) {
+      e = timed_group(st, phase_flops(ns, pls, kPhSq, k), [&] {
+        b_gemm_kernel<C, W, W, true><<<tiles, 256, 0, st>>>(d_items, d_plans, d_prefix, count, kPhSq, k);
+        return launched();
+      });
+      if (e != cudaSuccess) return e;
+    }
+    b_narrow_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+    if ((e = launched()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+inline int tiles_of(int n) {
+  const int t = (n + kGTile - 1) / kGTile;
+  return t * t;
+}
+
+template <typename T>
+calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int batch, const int *h_n,
+                            const T *const *h_A, const int *h_lda, T *const *h_E, const int *h_lde,
+                            void *work, std::size_t lwork, int *d_info, calamanExpmPlan_t *h_plans) {
+  using R = typename elem<T>::real;
+  using Hi = typename Wide<T>::type;
+  using Lay = BLayout<T>;
+  if (batch < 0) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (batch == 0) return ok_status();
+  if (h_n == nullptr || h_A == nullptr || h_lda == nullptr || h_E == nullptr || h_lde == nullptr ||
+      work == nullptr || d_info == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  for (int i = 0; i < batch; ++i) {
+    if (h_n[i] < 1 || h_lda[i] < h_n[i] || h_lde[i] < h_n[i] || h_A[i] == nullptr || h_E[i] == nullptr)
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+    if (h_n[i] > kBatchedMaxN) return blas_status(CALAMAN_STATUS_NOT_SUPPORTED);
+  }
+  Lay lay;
+  lay.plan(batch, h_n);
+  if (lwork < lay.total) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  PointerModeScope pm(blas);
+  TimerScope ts(timer_of(blas));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int dev = 0;
+  CLM_CUDA(cudaGetDevice(&dev));
+  CLM_CUDA(upload_pade_table(dev));
+
+  char *base = static_cast<char *>(work);
+  auto *d_lo = reinterpret_cast<BItem<T, Hi> *>(base + lay.items_lo);
+  auto *d_hi = reinterpret_cast<BItem<Hi, Hi> *>(base + lay.items_hi);
+  auto *d_plo = reinterpret_cast<BPlan *>(base + lay.plans_lo);
+  auto *d_phi = reinterpret_cast<BPlan *>(base + lay.plans_hi);
+  auto *d_xlo = reinterpret_cast<int *>(base + lay.prefix_lo);
+  auto *d_xhi = reinterpret_cast<int *>(base + lay.prefix_hi);
+  auto *d_norms = reinterpret_cast<double *>(base + lay.norms);
+  auto *d_cin = reinterpret_cast<BConv *>(base + lay.conv_in);
+  auto *d_cout = reinterpret_cast<BConv *>(base + lay.conv_out);
+
+  // 1. every 1-norm, one readback, every plan on the host
+  std::vector<BItem<T, Hi>> lo(batch);
+  for (int i = 0; i < batch; ++i) {
+    BItem<T, Hi> &it = lo[i];
+    carve_item<T>(it, base + lay.slab[i], h_n[i]);
+    it.A = h_A[i];
+    it.E = h_E[i];
+    it.lda = h_lda[i];
+    it.lde = h_lde[i];
+    it.id = i;
+  }
+  // pageable sources: each copy returns once its data is staged
+  CLM_CUDA(cudaMemcpyAsync(d_lo, lo.data(), sizeof(BItem<T, Hi>) * batch, cudaMemcpyHostToDevice, st));
+  b_norm_kernel<T, Hi><<<batch, 256, 0, st>>>(d_lo, d_norms);
+  CLM_CUDA(launched());
+  std::vector<double> norms(batch);
+  CLM_CUDA(cudaMemcpyAsync(norms.data(), d_norms, sizeof(double) * batch, cudaMemcpyDeviceToHost, st));
+  CLM_CUDA(cudaStreamSynchronize(st));
+  std::vector<calamanExpmPlan_t> plans(batch);
+  for (int i = 0; i < batch; ++i) {
+    if (!std::isfinite(norms[i])) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+    plans[i] = plan_for<R>((R)norms[i]);
+  }
+  if (h_plans)
+    for (int i = 0; i < batch; ++i) h_plans[i] = plans[i];
+
+  // 2. partition: the single tier sends s > 0 to FP64
+  std::vector<BItem<T, Hi>> lo_items;
+  std::vector<BItem<Hi, Hi>> hi_items;
+  std::vector<BPlan> lo_plans, hi_plans;
+  std::vector<int> lo_prefix(1, 0), hi_prefix(1, 0), lo_n, hi_n;
+  std::vector<BConv> cin, cout;
+  int lo_max_n = 0, hi_max_n = 0, lo_max_s = 0, hi_max_s = 0;
+  for (int i = 0; i < batch; ++i) {
+    const calamanExpmPlan_t &p = plans[i];
+    const BPlan bp{p.m, p.s, pade_num_powers(p.m), 0};
+    const int n = h_n[i];
+    if (!Lay::kSplit || p.s == 0) {
+      lo_items.push_back(lo[i]);
+      lo_plans.push_back(bp);
+      lo_prefix.push_back(lo_prefix.back() + tiles_of(n));
+      lo_n.push_back(n);
+      lo_max_n = std::max(lo_max_n, n);
+      lo_max_s = std::max(lo_max_s, p.s);
+    } else {
+      BItem<Hi, Hi> it{};
+      carve_item<Hi>(it, base + lay.slab[i], n);
+      const std::size_t nn = (std::size_t)n * n;
+      char *extra = base + lay.slab[i] + Lay::template slab_of<Hi>(n);
+      Hi *a64 = reinterpret_cast<Hi *>(extra);
+      Hi *e64 = reinterpret_cast<Hi *>(extra + align_up(nn * sizeof(Hi), 256));
+      it.A = a64;
+      it.lda = n;
+      it.E = e64;
+      it.lde = n;
+      it.id = i;
+      hi_items.push_back(it);
+      hi_plans.push_back(bp);
+      hi_prefix.push_back(hi_prefix.back() + tiles_of(n));
+      hi_n.push_back(n);
+      hi_max_n = std::max(hi_max_n, n);
+      hi_max_s = std::max(hi_max_s, p.s);
+      cin.push_back(BConv{h_A[i], a64, n, h_lda[i], n, 0});
+      cout.push_back(BConv{e64, h_E[i], n, n, h_lde[i], 0});
+    }
+  }
+  const int nlo = (int)lo_items.size(), nhi = (int)hi_items.size();
+  if (nlo > 0) {
+    CLM_CUDA(cudaMemcpyAsync(d_lo, lo_items.data(), sizeof(BItem<T, Hi>) * nlo, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_plo, lo_plans.data(), sizeof(BPlan) * nlo, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_xlo, lo_prefix.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
+    CLM_CUDA(run_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info, lo_n,
+                               lo_plans));
+  }
+  if (nhi > 0) {
+    CLM_CUDA(cudaMemcpyAsync(d_hi, hi_items.data(), sizeof(BItem<Hi, Hi>) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_phi, hi_plans.data(), sizeof(BPlan) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_xhi, hi_prefix.data(), sizeof(int) * (nhi + 1), cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_cin, cin.data(), sizeof(BConv) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_cout, cout.data(), sizeof(BConv) * nhi, cudaMemcpyHostToDevice, st));
+    const dim3 ew((unsigned)nhi, (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk));
+    b_conv_kernel<T, Hi><<<ew, 256, 0, st>>>(d_cin);
+    CLM_CUDA(launched());
+    CLM_CUDA(run_phases<Hi>(st, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info, hi_n,
+                                hi_plans));
+    b_conv_kernel<Hi, T><<<ew, 256, 0, st>>>(d_cout);
+    CLM_CUDA(launched());
+  }
+  return ok_status();
+}
+
+template <typename T>
+calamanStatus_t batched_bytes(int batch, const int *h_n, std::size_t *bytes) {
+  if (batch < 0 || bytes == nullptr || (batch > 0 && h_n == nullptr))
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  for (int i = 0; i < batch; ++i) {
+    if (h_n[i] < 1) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+    if (h_n[i] > kBatchedMaxN) return blas_status(CALAMAN_STATUS_NOT_SUPPORTED);
+  }
+  BLayout<T> lay;
+  lay.plan(batch, h_n);
+  *bytes = batch > 0 ? lay.total : 0;
+  return ok_status();
+}
+
+}  // namespace
+}  // namespace clm
+
+using namespace clm;
+
+extern "C" {
+
+calamanStatus_t calaman_expm_batched_bufferSize_s(calamanSolverHandle_t, int batch, const int *h_n,
+                                                  size_t *bytes) {
+  return batched_bytes<float>(batch, h_n, bytes);
+}
+calamanStatus_t calaman_expm_batched_bufferSize_d(calamanSolverHandle_t, int batch, const int *h_n,
+                                                  size_t *bytes) {
+  return batched_bytes<double>(batch, h_n, bytes);
+}
+calamanStatus_t calaman_expm_batched_s(calamanBlasHandle_t blas, calamanSolverHandle_t,
+                                       calamanStream_t stream, int batch, const int *h_n,
+                                       const float *const *h_A, const int *h_lda, float *const *h_E,
+                                       const int *h_lde, void *d_work, size_t lwork, int *d_info,
+                                       calamanExpmPlan_t *h_plans) {
+  return batched_api<float>(blas, stream, batch, h_n, h_A, h_lda, h_E, h_lde, d_work, lwork, d_info,
+                            h_plans);
+}
+calamanStatus_t calaman_expm_batched_d(calamanBlasHandle_t blas, calamanSolverHandle_t,
+                                       calamanStream_t stream, int batch, const int *h_n,
+                                       const double *const *h_A, const int *h_lda, double *const *h_E,
+                                       const int *h_lde, void *d_work, size_t lwork, int *d_info,
+                                       calamanExpmPlan_t *h_plans) {
+  return batched_api<double>(blas, stream, batch, h_n, h_A, h_lda, h_E, h_lde, d_work, lwork, d_info,
+                             h_plans);
+}
+
+}  // extern "C"

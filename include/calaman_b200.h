@@ -172,6 +172,33 @@ calamanStatus_t calaman_expm_vjp_z(calamanBlasHandle_t blas, calamanSolverHandle
                                    void *d_expA, int lde, void *d_work, size_t lwork_bytes,
                                    int *d_info, calamanExpmPlan_t *plan);
 
+/* ---- expm_batched: many small matrices in one call ----------------------
+ * New entry point: calaman_G evaluates one matrix per call. exp(A_i) for
+ * i < batch, every matrix with its own n_i (1 <= n_i <= 256; larger returns
+ * CALAMAN_STATUS_NOT_SUPPORTED -- use calaman_expm_* for those), leading
+ * dimensions and its own plan (m_i, s_i) = expm_plan(||A_i||_1), exactly the
+ * plan calaman_expm_* picks for that matrix. h_n, h_lda, h_lde are host arrays;
+ * h_A / h_expA are host arrays of device pointers. d_info: 2 * batch device
+ * ints ([2i] LU info of matrix i, [2i + 1] solve info). h_plans (host, may be
+ * NULL) receives every plan. Synchronises `stream` once (one readback of all
+ * norms); a non-finite norm anywhere fails the whole call with
+ * INVALID_VALUE before any output is written. The _s tier multiplies in FP32
+ * and squares in FP64, like calaman_expm_s. */
+calamanStatus_t calaman_expm_batched_bufferSize_s(calamanSolverHandle_t h, int batch,
+                                                  const int *h_n, size_t *bytes);
+calamanStatus_t calaman_expm_batched_bufferSize_d(calamanSolverHandle_t h, int batch,
+                                                  const int *h_n, size_t *bytes);
+calamanStatus_t calaman_expm_batched_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                       calamanStream_t stream, int batch, const int *h_n,
+                                       const float *const *h_A, const int *h_lda,
+                                       float *const *h_expA, const int *h_lde, void *d_work,
+                                       size_t lwork_bytes, int *d_info, calamanExpmPlan_t *h_plans);
+calamanStatus_t calaman_expm_batched_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                       calamanStream_t stream, int batch, const int *h_n,
+                                       const double *const *h_A, const int *h_lda,
+                                       double *const *h_expA, const int *h_lde, void *d_work,
+                                       size_t lwork_bytes, int *d_info, calamanExpmPlan_t *h_plans);
+
 /* ---- expm without a caller workspace ----------------------------------
  * No counterpart in the reference: calaman_G's expm always takes a caller
  * workspace. For callers that cannot call cudaMalloc (code hosted by a
