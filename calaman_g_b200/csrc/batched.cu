@@ -325,6 +325,14 @@ __global__ void __launch_bounds__(256)
         for (int j = 0; j < 4; ++j) acc[i][j] = fmac(a[i], bv[j], acc[i][j]);
     }
   }
+  U old[4][4];  // accumulate: every old C value in flight before the first store
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int c = n0 + ty + 16 * j, r = m0 + tx + 16 * i;
+      old[i][j] = (o.acc && c < n && r < n) ? o.C[(std::size_t)c * o.ldc + r] : elem<U>::zero();
+    }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int c = n0 + ty + 16 * j;
@@ -333,15 +341,63 @@ __global__ void __launch_bounds__(256)
     for (int i = 0; i < 4; ++i) {
       const int r = m0 + tx + 16 * i;
       if (r >= n) continue;
-      U *dst = o.C + (std::size_t)c * o.ldc + r;
-      *dst = o.acc ? add(*dst, acc[i][j]) : acc[i][j];
+      o.C[(std::size_t)c * o.ldc + r] = o.acc ? add(old[i][j], acc[i][j]) : acc[i][j];
     }
   }
 }
 
 // ---- LU with partial pivoting of q and the solve q R = p: one CTA per matrix
+// Row loops update 8 columns at a time: eight independent loads are issued
+// before the first store, so the L2 latency is paid once per eight elements.
+constexpr int kBU = 8;
+
+template <typename T> struct BLuOcc { static constexpr int kMinBlocks = 1; };
+template <> struct BLuOcc<float> { static constexpr int kMinBlocks = 2; };
+
+// kBU consecutive elements of a shared-memory row as 16-byte vector loads
+// (one load instruction per 16 bytes instead of one per element).
+template <typename T>
+__device__ __forceinline__ void lds_chunk(const T *src, T (&dst)[kBU]) {
+  static_assert((kBU * sizeof(T)) % 16 == 0, "chunk must be whole 16-byte vectors");
+  union {
+    float4 v[kBU * sizeof(T) / 16];
+    T e[kBU];
+  } u;
+  const float4 *s4 = reinterpret_cast<const float4 *>(src);
+#pragma unroll
+  for (int i = 0; i < (int)(kBU * sizeof(T) / 16); ++i) u.v[i] = s4[i];
+#pragma unroll
+  for (int i = 0; i < kBU; ++i) dst[i] = u.e[i];
+}
+
+// M(t, c) -= sum_j w[j] * blk[j][c] for c in [c0, n), element t of each
+// column (one row per thread). c0 is a multiple of kBU and n <= kBThreads, so
+// every chunk of blk lies inside its 16-byte-aligned row.
+template <typename T>
+__device__ __forceinline__ void row_update(T *__restrict__ M, int ld, int t, int c0, int n,
+                                           const T (&w)[kBPanel], int jb,
+                                           const T (*__restrict__ blk)[kBThreads]) {
+  for (int c = c0; c < n; c += kBU) {
+    T v[kBU];
+#pragma unroll
+    for (int u = 0; u < kBU; ++u) v[u] = c + u < n ? M[(std::size_t)(c + u) * ld + t] : elem<T>::zero();
+#pragma unroll
+    for (int j = 0; j < kBPanel; ++j) {
+      if (j < jb) {
+        T b[kBU];
+        lds_chunk(&blk[j][c], b);
+#pragma unroll
+        for (int u = 0; u < kBU; ++u) v[u] = sub(v[u], mul(w[j], b[u]));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kBU; ++u)
+      if (c + u < n) M[(std::size_t)(c + u) * ld + t] = v[u];
+  }
+}
+
 template <typename T, typename Wd>
-__global__ void __launch_bounds__(kBThreads)
+__global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
     b_lu_solve_kernel(const BItem<T, Wd> *__restrict__ items, const BPlan *__restrict__ plans,
                       int *__restrict__ info) {
   using R = typename elem<T>::real;
@@ -352,29 +408,29 @@ __global__ void __launch_bounds__(kBThreads)
   const T *B = it.P0;  // right-hand side p (ld n)
   T *D = pl.s > 0 ? it.X : it.E;
   const int ldd = pl.s > 0 ? n : it.lde;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
 
-  // dynamic: blk[kBPanel][kBThreads] (U12 rows / solved right-hand-side block
-  // rows), then diag[kBPanel][kBPanel + 1] (L11 / U11 of the current block)
+  // dynamic: blk[kBPanel][kBThreads] (per-column staging, U12 rows, solved
+  // right-hand-side block rows), then diag[kBPanel][kBPanel + 1]
   extern __shared__ __align__(16) unsigned char b_smem[];
   auto blk = reinterpret_cast<T(*)[kBThreads]>(b_smem);
   auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * kBThreads);
-  __shared__ T prow[kBPanel];               // pivot row of the current column
-  __shared__ T xrow[2][kBPanel];            // row exchange slots
-  __shared__ int perm[kBThreads];           // P: row i of P q is row perm[i] of q
-  __shared__ int pos[kBThreads];            // panel-local composite of the swaps
+  __shared__ T xrow[2][kBPanel];   // [0]: old row a, [1]: the pivot row
+  __shared__ T rdiag[kBPanel];     // reciprocals of U's diagonal block
+  __shared__ int perm[kBThreads];  // P: row i of P q is row perm[i] of q
+  __shared__ int pos[kBThreads];   // panel-local composite of the swaps
   __shared__ int piv[kBPanel];
-  __shared__ double rv[8];
-  __shared__ int ri[8];
+  __shared__ double red_v[kBThreads / 32];
+  __shared__ int red_i[kBThreads / 32];
   __shared__ int first_zero;
 
   if (t < n) perm[t] = t;
   if (t == 0) first_zero = 0;
+  const double sfmin = sizeof(R) == 4 ? (double)FLT_MIN : DBL_MIN;
 
   T r[kBPanel];
   for (int k = 0; k < n; k += kBPanel) {
     const int jb = min(kBPanel, n - k);
-    // my row of the panel (rows >= k take part)
     const bool mine = t >= k && t < n;
 #pragma unroll
     for (int j = 0; j < kBPanel; ++j)
@@ -383,13 +439,15 @@ __global__ void __launch_bounds__(kBThreads)
     __syncthreads();
 #pragma unroll 1
     for (int j = 0; j < jb; ++j) {
-      // pivot: largest |Re| + |Im| among rows >= k + j, first index on ties
+      const int a = k + j;
       T rj = elem<T>::zero();
 #pragma unroll
       for (int c = 0; c < kBPanel; ++c)
         if (c == j) rj = r[c];
-      double v = (mine && t >= k + j) ? abs1(rj) : -1.0;
+      // pivot: largest |Re| + |Im| among rows >= a, first index on ties
+      double v = (mine && t >= a) ? abs1(rj) : -1.0;
       int idx = t;
+#pragma unroll
       for (int o = 16; o; o >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, v, o);
         const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
@@ -398,73 +456,67 @@ __global__ void __launch_bounds__(kBThreads)
           idx = oi;
         }
       }
-      if ((t & 31) == 0) {
-        rv[t >> 5] = v;
-        ri[t >> 5] = idx;
+      if (lane == 0) {
+        red_v[warp] = v;
+        red_i[warp] = idx;
       }
       __syncthreads();
-      if (t == 0) {
-        double bv = rv[0];
-        int bi = ri[0];
-        for (int w = 1; w < 8; ++w)
-          if (rv[w] > bv || (rv[w] == bv && ri[w] < bi)) {
-            bv = rv[w];
-            bi = ri[w];
-          }
-        piv[j] = bi;
-        const int a = k + j;
-        if (bi != a) {
-          const int tp = perm[a];
-          perm[a] = perm[bi];
-          perm[bi] = tp;
-          const int tq = pos[a];
-          pos[a] = pos[bi];
-          pos[bi] = tq;
-        }
-      }
-      __syncthreads();
-      const int p = piv[j], a = k + j;
-      if (p != a) {
-        if (t == a) {
+      double bv = red_v[0];
+      int p = red_i[0];
 #pragma unroll
-          for (int c = 0; c < kBPanel; ++c) xrow[0][c] = r[c];
-        }
-        if (t == p) {
-#pragma unroll
-          for (int c = 0; c < kBPanel; ++c) xrow[1][c] = r[c];
-        }
-        __syncthreads();
-        if (t == a) {
-#pragma unroll
-          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[1][c];
-        }
-        if (t == p) {
-#pragma unroll
-          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[0][c];
+      for (int w = 1; w < kBThreads / 32; ++w) {
+        const double wv = red_v[w];
+        const int wi = red_i[w];
+        if (wv > bv || (wv == bv && wi < p)) {
+          bv = wv;
+          p = wi;
         }
       }
       if (t == a) {
 #pragma unroll
-        for (int c = 0; c < kBPanel; ++c) prow[c] = r[c];
+        for (int c = 0; c < kBPanel; ++c) xrow[0][c] = r[c];
+      }
+      if (t == p) {
+#pragma unroll
+        for (int c = 0; c < kBPanel; ++c) xrow[1][c] = r[c];
+      }
+      if (t == 0) {
+        piv[j] = p;
+        if (p != a) {
+          const int tp = perm[a];
+          perm[a] = perm[p];
+          perm[p] = tp;
+          const int tq = pos[a];
+          pos[a] = pos[p];
+          pos[p] = tq;
+        }
+        if (!(bv > 0.0) && first_zero == 0) first_zero = a + 1;
       }
       __syncthreads();
-      const T pv = prow[j];
-      if (t == 0 && is_zero(pv) && first_zero == 0) first_zero = a + 1;
+      if (p != a) {
+        if (t == a) {
+#pragma unroll
+          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[1][c];
+        } else if (t == p) {
+#pragma unroll
+          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[0][c];
+        }
+      }
+      const T pv = xrow[1][j];
       if (mine && t > a && !is_zero(pv)) {
-        const bool use_recip = abs1(pv) >= (sizeof(R) == 4 ? (double)FLT_MIN : DBL_MIN);
-        const T rcp = divide(elem<T>::one(), pv);
         T l = elem<T>::zero();
 #pragma unroll
         for (int c = 0; c < kBPanel; ++c)
-          if (c == j) l = use_recip ? mul(r[c], rcp) : divide(r[c], pv);
+          if (c == j) l = r[c];
+        l = abs1(pv) >= sfmin ? mul(l, divide(elem<T>::one(), pv)) : divide(l, pv);
 #pragma unroll
         for (int c = 0; c < kBPanel; ++c) {
           if (c == j) r[c] = l;
-          else if (c > j && c < jb) r[c] = sub(r[c], mul(l, prow[c]));
+          else if (c > j && c < jb) r[c] = sub(r[c], mul(l, xrow[1][c]));
         }
       }
     }
-    // panel back to memory; L11 / U11 block to shared memory
+    // panel back to memory; L11 to shared memory
     if (mine) {
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
@@ -477,39 +529,28 @@ __global__ void __launch_bounds__(kBThreads)
     }
     __syncthreads();
     // columns outside the panel: apply the panel's swaps (rows >= k + jb only
-    // ever receive rows of the top block [k, k + jb)); right of the panel, also
-    // solve the top block with the unit-lower L11
+    // ever receive rows of the top block [k, k + jb)), then, right of the
+    // panel, solve the top block with the unit-lower L11
     if (t < n - jb) {
       const int c = t < k ? t : t + jb;
       T *col = Q + (std::size_t)c * n;
-      T top[kBPanel];
 #pragma unroll
-      for (int j = 0; j < kBPanel; ++j) top[j] = j < jb ? col[k + j] : elem<T>::zero();
+      for (int j = 0; j < kBPanel; ++j)
+        if (j < jb) blk[j][c] = col[k + j];  // the old top block, staged
       T x[kBPanel];
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j) {
         x[j] = elem<T>::zero();
         if (j < jb) {
           const int src = pos[k + j];
-          if (src >= k + jb) x[j] = col[src];
-          else {
-#pragma unroll
-            for (int q = 0; q < kBPanel; ++q)
-              if (q == src - k) x[j] = top[q];
-          }
+          x[j] = src >= k + jb ? col[src] : blk[src - k][c];
         }
       }
-      // displaced rows below the block take their top-block row
-#pragma unroll 1
-      for (int j = 0; j < jb; ++j) {
-        const int d = piv[j];
-        if (d >= k + jb) {
-          const int src = pos[d] - k;
-          T v = elem<T>::zero();
 #pragma unroll
-          for (int q = 0; q < kBPanel; ++q)
-            if (q == src) v = top[q];
-          col[d] = v;
+      for (int j = 0; j < kBPanel; ++j) {
+        if (j < jb) {
+          const int d = piv[j];
+          if (d >= k + jb) col[d] = blk[pos[d] - k][c];
         }
       }
       if (c >= k + jb) {
@@ -518,25 +559,17 @@ __global__ void __launch_bounds__(kBThreads)
 #pragma unroll
           for (int q = 0; q < kBPanel; ++q)
             if (q < j && j < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
-#pragma unroll
-        for (int j = 0; j < kBPanel; ++j)
-          if (j < jb) blk[j][c] = x[j];
       }
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
-        if (j < jb) col[k + j] = x[j];
+        if (j < jb) {
+          blk[j][c] = x[j];
+          col[k + j] = x[j];
+        }
     }
     __syncthreads();
     // trailing update A22 -= L21 U12, thread i owns row i
-    if (t >= k + jb && t < n) {
-      for (int c = k + jb; c < n; ++c) {
-        T acc = Q[(std::size_t)c * n + t];
-#pragma unroll
-        for (int j = 0; j < kBPanel; ++j)
-          if (j < jb) acc = sub(acc, mul(r[j], blk[j][c]));
-        Q[(std::size_t)c * n + t] = acc;
-      }
-    }
+    if (t >= k + jb && t < n) row_update(Q, n, t, k + jb, n, r, jb, blk);
     __syncthreads();
   }
   if (t == 0) {
@@ -547,7 +580,14 @@ __global__ void __launch_bounds__(kBThreads)
   // ---- solve q R = p:  R = U^-1 L^-1 (P p) -------------------------------
   if (t < n) {
     const int src = perm[t];
-    for (int c = 0; c < n; ++c) D[(std::size_t)c * ldd + t] = B[(std::size_t)c * n + src];
+    for (int c = 0; c < n; c += kBU) {
+      T v[kBU];
+#pragma unroll
+      for (int u = 0; u < kBU; ++u) v[u] = c + u < n ? B[(std::size_t)(c + u) * n + src] : elem<T>::zero();
+#pragma unroll
+      for (int u = 0; u < kBU; ++u)
+        if (c + u < n) D[(std::size_t)(c + u) * ldd + t] = v[u];
+    }
   }
   __syncthreads();
   // forward, unit lower
@@ -579,13 +619,7 @@ __global__ void __launch_bounds__(kBThreads)
     if (t >= k + jb && t < n) {
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j) r[j] = j < jb ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
-      for (int c = 0; c < n; ++c) {
-        T acc = D[(std::size_t)c * ldd + t];
-#pragma unroll
-        for (int j = 0; j < kBPanel; ++j)
-          if (j < jb) acc = sub(acc, mul(r[j], blk[j][c]));
-        D[(std::size_t)c * ldd + t] = acc;
-      }
+      row_update(D, ldd, t, 0, n, r, jb, blk);
     }
     __syncthreads();
   }
@@ -597,7 +631,7 @@ __global__ void __launch_bounds__(kBThreads)
       diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
     }
     __syncthreads();
-    if (t < jb) prow[t] = divide(elem<T>::one(), diag[t][t]);
+    if (t < jb) rdiag[t] = divide(elem<T>::one(), diag[t][t]);
     __syncthreads();
     if (t < n) {
       T *col = D + (std::size_t)t * ldd;
@@ -610,7 +644,7 @@ __global__ void __launch_bounds__(kBThreads)
 #pragma unroll
           for (int q = 0; q < kBPanel; ++q)
             if (q > j && q < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
-          x[j] = mul(x[j], prow[j]);
+          x[j] = mul(x[j], rdiag[j]);
         }
       }
 #pragma unroll
@@ -624,13 +658,7 @@ __global__ void __launch_bounds__(kBThreads)
     if (t < k) {
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j) r[j] = j < jb ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
-      for (int c = 0; c < n; ++c) {
-        T acc = D[(std::size_t)c * ldd + t];
-#pragma unroll
-        for (int j = 0; j < kBPanel; ++j)
-          if (j < jb) acc = sub(acc, mul(r[j], blk[j][c]));
-        D[(std::size_t)c * ldd + t] = acc;
-      }
+      row_update(D, ldd, t, 0, n, r, jb, blk);
     }
     __syncthreads();
   }

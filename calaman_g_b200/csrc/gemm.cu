@@ -172,9 +172,20 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   }
   cp_wait<0>();
 
-  // epilogue: C = alpha acc + beta C (beta == 0 never reads C)
+  // epilogue: C = alpha acc + beta C (beta == 0 never reads C). Per row
+  // block, every old C value is loaded before the first store, so the loads
+  // are in flight together instead of one round trip per element.
 #pragma unroll
-  for (int i = 0; i < MI; ++i)
+  for (int i = 0; i < MI; ++i) {
+    double old[NI][4];
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
+        const int n = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        old[j][r] = (beta != 0.0 && m < M && n < N) ? C[(std::size_t)n * ldc + m] : 0.0;
+      }
 #pragma unroll
     for (int j = 0; j < NI; ++j)
 #pragma unroll
@@ -182,11 +193,11 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
         const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
         const int n = n0 + wn0 + j * 8 + 2 * t + (r & 1);
         if (m < M && n < N) {
-          double *c = C + (std::size_t)n * ldc + m;
           const double v = alpha * acc[i][j][r];
-          *c = (beta == 0.0) ? v : fma(beta, *c, v);
+          C[(std::size_t)n * ldc + m] = (beta == 0.0) ? v : fma(beta, old[j][r], v);
         }
       }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -302,8 +313,18 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   }
   cp_wait<0>();
 
+  // epilogue: all old C values of a row block are loaded before any store
 #pragma unroll
-  for (int i = 0; i < MI; ++i)
+  for (int i = 0; i < MI; ++i) {
+    double2 old[NI][4];
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
+        const int n = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        old[j][r] = (beta != 0.0 && m < M && n < N) ? C[(std::size_t)n * ldc + m] : make_double2(0.0, 0.0);
+      }
 #pragma unroll
     for (int j = 0; j < NI; ++j)
 #pragma unroll
@@ -311,16 +332,15 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
         const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
         const int n = n0 + wn0 + j * 8 + 2 * t + (r & 1);
         if (m < M && n < N) {
-          double2 *c = C + (std::size_t)n * ldc + m;
           double2 v = make_double2(alpha * re[i][j][r], alpha * im[i][j][r]);
           if (beta != 0.0) {
-            const double2 o = *c;
-            v.x = fma(beta, o.x, v.x);
-            v.y = fma(beta, o.y, v.y);
+            v.x = fma(beta, old[j][r].x, v.x);
+            v.y = fma(beta, old[j][r].y, v.y);
           }
-          *c = v;
+          C[(std::size_t)n * ldc + m] = v;
         }
       }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -377,16 +397,23 @@ __global__ void __launch_bounds__(256)
     }
     __syncthreads();
   }
+  T old[4][4];  // every old C value in flight before the first store
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
+      old[i][j] = (beta != 0.0 && m < M && n < N) ? C[(std::size_t)n * ldc + m] : elem<T>::zero();
+    }
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
       if (m < M && n < N) {
-        T *c = C + (std::size_t)n * ldc + m;
         T v = scale(acc[i][j], (R)alpha);
-        if (beta != 0.0) v = add(v, scale(*c, (R)beta));
-        *c = v;
+        if (beta != 0.0) v = add(v, scale(old[i][j], (R)beta));
+        C[(std::size_t)n * ldc + m] = v;
       }
     }
 }

@@ -745,6 +745,301 @@ __global__ void __launch_bounds__(256)
   if (lane + 32 < kb) col[lane + 32] = x1;
 }
 
+// ---------------------------------------------------------------------------
+// One-CTA panel, two levels: the h x kb panel (kb <= 64) stays in global
+// memory (L2) and is factored in sub-panels of KBS columns; a sub-panel's rows
+// live in registers (thread t keeps rows t, t + NT, ... -- RPT of them), so a
+// pivot column costs one CTA-wide argmax and two barriers, with no cluster
+// barrier and no distributed shared memory. After each sub-panel the CTA
+// applies its swaps to the panel's other columns, solves the sub-panel's
+// U12 rows with the unit-lower L11, and updates the rest of the panel.
+// ---------------------------------------------------------------------------
+constexpr int kCtaChunk = 8;  // columns per register chunk of the in-panel update
+
+template <typename T>
+__device__ __forceinline__ void lds_vec8(const T *src, T (&dst)[kCtaChunk]) {
+  // 8 consecutive elements as 16-byte shared loads (src 16-byte aligned)
+  union {
+    float4 v[kCtaChunk * sizeof(T) / 16];
+    T e[kCtaChunk];
+  } u;
+  const float4 *s4 = reinterpret_cast<const float4 *>(src);
+#pragma unroll
+  for (int i = 0; i < (int)(kCtaChunk * sizeof(T) / 16); ++i) u.v[i] = s4[i];
+#pragma unroll
+  for (int i = 0; i < kCtaChunk; ++i) dst[i] = u.e[i];
+}
+
+template <typename T, int KBS, int RPT>
+__global__ void __launch_bounds__(512, 1)
+    lu_panel_cta_kernel(int n, T *__restrict__ A, int lda, int k, int kb, int *__restrict__ ipiv,
+                        int *__restrict__ perm, int *__restrict__ g_map_pos, int *__restrict__ g_map_src,
+                        int *__restrict__ g_map_count, int *__restrict__ info) {
+  cg::cluster_group cluster = cg::this_cluster();  // launched as a cluster of one
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int NT = blockDim.x, nwarps = NT >> 5;
+  const int h = n - k;
+  T *P = A + (std::size_t)k * lda + k;  // the panel: P[c * lda + i], i < h, c < kb
+  __shared__ T xrow[2][KBS];            // [0]: old row a, [1]: the pivot row
+  __shared__ T l11[KBS][KBS + 1];
+  __shared__ __align__(16) T u12[KBS][kMaxKb];
+  __shared__ double red_v[16];
+  __shared__ int red_i[16];
+  __shared__ int plist[kMaxKb];
+  __shared__ int flags[1];
+  __shared__ int mpos[2 * kMaxKb], morg[2 * kMaxKb];
+  __shared__ int src_top[KBS], disp_row[KBS], disp_src[KBS], ndisp[1];
+
+  if (tid == 0) flags[0] = -1;
+  T r[RPT][KBS];
+  for (int sb = 0; sb < kb; sb += KBS) {
+    const int w = min(KBS, kb - sb);
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int gi = tid + q * NT;
+#pragma unroll
+      for (int c = 0; c < KBS; ++c)
+        r[q][c] = (gi >= sb && gi < h && c < w) ? P[(std::size_t)(sb + c) * lda + gi] : elem<T>::zero();
+    }
+    // ---- factor the sub-panel, one pivot column at a time ----
+#pragma unroll
+    for (int j = 0; j < KBS; ++j) {
+      if (j >= w) break;
+      const int a = sb + j;
+      double bv = -1.0;
+      int bi = INT_MAX;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int gi = tid + q * NT;
+        if (gi >= a && gi < h) argmax_merge(bv, bi, abs1(r[q][j]), gi);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        argmax_merge(bv, bi, ov, oi);
+      }
+      if (lane == 0) {
+        red_v[warp] = bv;
+        red_i[warp] = bi;
+      }
+      __syncthreads();
+      double pv = lane < nwarps ? red_v[lane] : -1.0;
+      int p = lane < nwarps ? red_i[lane] : INT_MAX;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, pv, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, p, off);
+        argmax_merge(pv, p, ov, oi);
+      }
+      bool forced = false;
+      if (p == INT_MAX || p < a) {  // no comparable candidate (NaN column): keep row a
+        p = a;
+        pv = 0.0;
+        forced = true;
+      }
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int gi = tid + q * NT;
+        if (gi == a) {
+#pragma unroll
+          for (int c = 0; c < KBS; ++c) xrow[0][c] = r[q][c];
+        }
+        if (gi == p) {
+#pragma unroll
+          for (int c = 0; c < KBS; ++c) xrow[1][c] = r[q][c];
+        }
+      }
+      if (tid == 0) {
+        plist[a] = p;
+        if (pv == 0.0 && flags[0] < 0) flags[0] = a;
+      }
+      __syncthreads();
+      const T piv = xrow[1][j];
+      const bool singular = forced || is_zero(piv);
+      const bool use_recip = abs1(piv) >= safe_min<T>();
+      const T rpiv = singular ? elem<T>::one() : divide(elem<T>::one(), piv);
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int gi = tid + q * NT;
+        if (gi < a || gi >= h) continue;
+        if (gi == a) {
+          if (p != a) {
+#pragma unroll
+            for (int c = 0; c < KBS; ++c) r[q][c] = xrow[1][c];
+          }
+          continue;
+        }
+        if (gi == p) {
+#pragma unroll
+          for (int c = 0; c < KBS; ++c) r[q][c] = xrow[0][c];
+        }
+        const T l = singular ? r[q][j] : (use_recip ? mul(r[q][j], rpiv) : divide(r[q][j], piv));
+        r[q][j] = l;
+#pragma unroll
+        for (int c = j + 1; c < KBS; ++c)
+          if (c < w) r[q][c] = sub(r[q][c], mul(l, xrow[1][c]));
+      }
+    }
+    // ---- sub-panel back to memory, L11 to shared memory ----
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int gi = tid + q * NT;
+      if (gi >= sb && gi < h) {
+#pragma unroll
+        for (int c = 0; c < KBS; ++c)
+          if (c < w) P[(std::size_t)(sb + c) * lda + gi] = r[q][c];
+      }
+      if (gi >= sb && gi < sb + w) {
+#pragma unroll
+        for (int c = 0; c < KBS; ++c) l11[gi - sb][c] = r[q][c];
+      }
+    }
+    // ---- where the sub-panel's swaps moved rows: position sb + j now holds
+    // old row src_top[j]; a row d below the block holds old top-block row
+    // disp_src[e] (rows below only ever receive rows of the top block) ----
+    if (warp == 0) {
+      int *keys = mpos, *vals = morg;  // scratch, reused by panel_finish later
+      for (int e = lane; e < w; e += 32) {
+        keys[e] = sb + e;
+        vals[e] = sb + e;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        int count = w;
+        for (int j = 0; j < w; ++j) {
+          const int b = plist[sb + j];
+          int bidx = -1;
+          if (b < sb + w) bidx = b - sb;
+          else {
+            for (int e = w; e < count; ++e)
+              if (keys[e] == b) bidx = e;
+            if (bidx < 0) {
+              bidx = count++;
+              keys[bidx] = b;
+              vals[bidx] = b;
+            }
+          }
+          if (bidx != j) {
+            const int t = vals[j];
+            vals[j] = vals[bidx];
+            vals[bidx] = t;
+          }
+        }
+        for (int j = 0; j < w; ++j) src_top[j] = vals[j];
+        for (int e = w; e < count; ++e) {
+          disp_row[e - w] = keys[e];
+          disp_src[e - w] = vals[e];
+        }
+        ndisp[0] = count - w;
+      }
+    }
+    __syncthreads();
+    // ---- the panel's other columns: swap, and right of the sub-panel solve
+    // the top block with L11 (U12 rows into shared memory) ----
+    if (tid < kb - w) {
+      const int c = tid < sb ? tid : tid + w;
+      T *col = P + (std::size_t)c * lda;
+      T top[KBS], x[KBS];
+#pragma unroll
+      for (int j = 0; j < KBS; ++j) top[j] = j < w ? col[sb + j] : elem<T>::zero();
+#pragma unroll
+      for (int j = 0; j < KBS; ++j) {
+        x[j] = elem<T>::zero();
+        if (j < w) {
+          const int src = src_top[j];
+          if (src >= sb + w) x[j] = col[src];
+          else {
+#pragma unroll
+            for (int q = 0; q < KBS; ++q)
+              if (q == src - sb) x[j] = top[q];
+          }
+        }
+      }
+      for (int e = 0; e < ndisp[0]; ++e) {
+        const int srcq = disp_src[e] - sb;
+        T v = elem<T>::zero();
+#pragma unroll
+        for (int q = 0; q < KBS; ++q)
+          if (q == srcq) v = top[q];
+        col[disp_row[e]] = v;
+      }
+      if (c >= sb + w) {
+#pragma unroll
+        for (int j = 1; j < KBS; ++j)
+#pragma unroll
+          for (int q = 0; q < j; ++q)
+            if (j < w) x[j] = sub(x[j], mul(l11[j][q], x[q]));
+#pragma unroll
+        for (int j = 0; j < KBS; ++j)
+          if (j < w) u12[j][c] = x[j];
+      }
+#pragma unroll
+      for (int j = 0; j < KBS; ++j)
+        if (j < w) col[sb + j] = x[j];
+    }
+    __syncthreads();
+    // ---- update the rest of the panel: rows below the block, columns right
+    // of the sub-panel (the multipliers are reloaded from the written-back
+    // sub-panel, so no panel registers stay live through the column phase) ----
+    const int c0 = sb + w;
+    if (c0 < kb) {
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int gi = tid + q * NT;
+        if (gi < c0 || gi >= h) continue;
+#pragma unroll
+        for (int j = 0; j < KBS; ++j) r[q][j] = j < w ? P[(std::size_t)(sb + j) * lda + gi] : elem<T>::zero();
+        for (int c = c0; c < kb; c += kCtaChunk) {
+          T v[kCtaChunk];
+#pragma unroll
+          for (int u = 0; u < kCtaChunk; ++u)
+            v[u] = c + u < kb ? P[(std::size_t)(c + u) * lda + gi] : elem<T>::zero();
+#pragma unroll
+          for (int j = 0; j < KBS; ++j) {
+            T b[kCtaChunk];
+            lds_vec8(&u12[j][c], b);
+#pragma unroll
+            for (int u = 0; u < kCtaChunk; ++u) v[u] = sub(v[u], mul(r[q][j], b[u]));
+          }
+#pragma unroll
+          for (int u = 0; u < kCtaChunk; ++u)
+            if (c + u < kb) P[(std::size_t)(c + u) * lda + gi] = v[u];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  panel_finish(cluster, 0, k, kb, plist, flags, mpos, morg, ipiv, perm, g_map_pos, g_map_src, g_map_count,
+               info);
+}
+
+// One-CTA panel configurations by height: RPT rows per thread for heights up
+// to 512 RPT, sub-panel width KBS (64 registers of sub-panel per thread at
+// most), outer panel width KB.
+template <typename T> struct CtaPanel;
+template <> struct CtaPanel<double2> {
+  static constexpr int KBS1 = 8, KBS2 = 8, KBS4 = 4, KBS8 = 0, KB = 32;
+};
+template <> struct CtaPanel<double> {
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, KB = 32;
+};
+template <> struct CtaPanel<float2> {
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, KB = 32;
+};
+template <> struct CtaPanel<float> {
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, KB = 64;
+};
+
+// Panel width of the one-CTA path for an n x n factorisation, 0 if n is too
+// tall for it.
+template <typename T>
+int cta_panel_kb(int n) {
+  const int kbs = n <= 512 ? CtaPanel<T>::KBS1 : n <= 1024 ? CtaPanel<T>::KBS2
+                : n <= 2048 ? CtaPanel<T>::KBS4 : n <= 4096 ? CtaPanel<T>::KBS8 : 0;
+  return kbs > 0 ? CtaPanel<T>::KB : 0;
+}
+
 // Register-panel configurations: KB columns, NCPH lanes per row, NT threads
 // per CTA (so NT / NCPH rows per CTA). Each lane keeps KB / NCPH elements,
 // 64 (RegPanel) or 128 (RegPanelWide, more rows per CTA) 32-bit registers.
@@ -806,6 +1101,43 @@ cudaError_t launch_reg_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb
   note_launch();
   return cudaLaunchKernelEx(&cfg, kern, n, A, lda, k, kb, rpc, sc.ipiv, sc.perm, sc.map_pos,
                             sc.map_src, sc.map_count, info);
+}
+
+template <typename T, int KBS, int RPT>
+cudaError_t launch_cta_panel_cfg(cudaStream_t s, int n, T *A, int lda, int k, int kb, const LuScratch &sc,
+                                 int *info) {
+  const int h = n - k;
+  int nt = (h + RPT - 1) / RPT;
+  nt = ((nt + 31) / 32) * 32;
+  if (nt < 64) nt = 64;  // >= kb - KBS column threads
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1, 1, 1);
+  cfg.blockDim = dim3(nt, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1] = {cluster_attr(1)};
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, lu_panel_cta_kernel<T, KBS, RPT>, n, A, lda, k, kb, sc.ipiv, sc.perm,
+                            sc.map_pos, sc.map_src, sc.map_count, info);
+}
+
+// The one-CTA panel for a step of an n x n factorisation (kb = cta_panel_kb).
+template <typename T>
+cudaError_t launch_cta_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb, const LuScratch &sc,
+                             int *info) {
+  using C = CtaPanel<T>;
+  if (n <= 512) {
+    if constexpr (C::KBS1 > 0) return launch_cta_panel_cfg<T, C::KBS1, 1>(s, n, A, lda, k, kb, sc, info);
+  } else if (n <= 1024) {
+    if constexpr (C::KBS2 > 0) return launch_cta_panel_cfg<T, C::KBS2, 2>(s, n, A, lda, k, kb, sc, info);
+  } else if (n <= 2048) {
+    if constexpr (C::KBS4 > 0) return launch_cta_panel_cfg<T, C::KBS4, 4>(s, n, A, lda, k, kb, sc, info);
+  } else {
+    if constexpr (C::KBS8 > 0) return launch_cta_panel_cfg<T, C::KBS8, 8>(s, n, A, lda, k, kb, sc, info);
+  }
+  return cudaErrorInvalidValue;
 }
 
 template <typename T>
@@ -874,7 +1206,8 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
   if (e != cudaSuccess) return e;
   iota_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, sc.perm);
   if ((e = launched()) != cudaSuccess) return e;
-  const int kbn = choose_kb<T>(n);
+  const int kb_cta = cta_panel_kb<T>(n);
+  const int kbn = kb_cta > 0 ? kb_cta : choose_kb<T>(n);
   auto swap_kern = lu_swap_trsm_kernel<T>;
   const std::size_t swap_smem = sizeof(T) * (std::size_t)kbn * kbn;
   if ((e = cudaFuncSetAttribute(swap_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)swap_smem)) !=
@@ -882,7 +1215,9 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
     return e;
   for (int k = 0; k < n; k += kbn) {
     const int kb = (k + kbn < n) ? kbn : n - k;
-    if ((e = launch_panel<T>(s, n, A, lda, k, kb, sc, info_dev)) != cudaSuccess) return e;
+    e = kb_cta > 0 ? launch_cta_panel<T>(s, n, A, lda, k, kb, sc, info_dev)
+                   : launch_panel<T>(s, n, A, lda, k, kb, sc, info_dev);
+    if (e != cudaSuccess) return e;
     const int others = n - kb;
     if (others > 0) {
       const int warps = 8;

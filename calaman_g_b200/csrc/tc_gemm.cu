@@ -230,13 +230,19 @@ __global__ void __launch_bounds__(kThreads, 1)
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
         if (m < prm.M) {
+          // the 32 old C values of this chunk are loaded before any store
+          float old[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int n = n0 + c0 + j;
+            old[j] = (prm.beta != 0.f && n < prm.N) ? prm.C[(std::size_t)n * prm.ldc + m] : 0.f;
+          }
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int n = n0 + c0 + j;
             if (n < prm.N) {
-              float *c = prm.C + (std::size_t)n * prm.ldc + m;
               const float x = prm.alpha * __uint_as_float(v[j]);
-              *c = (prm.beta == 0.f) ? x : fmaf(prm.beta, *c, x);
+              prm.C[(std::size_t)n * prm.ldc + m] = (prm.beta == 0.f) ? x : fmaf(prm.beta, old[j], x);
             }
           }
         }
