@@ -80,20 +80,27 @@ def make_matrix(cfg, seed=20261203):
     return np.asfortranarray(a.astype(NP[cfg["suf"]]))
 
 
-def batched_workload(cfg, seed=20261204):
-    """The batched workload: n uniform on {16, 32, ..., nmax}, N(0,1) entries
-    rescaled to a 1-norm log-uniform in [0.1, 100] (float32 values; the
-    float64 tier gets the same values widened)."""
+def batched_spec(cfg, count, seed=20261204):
+    """Sizes and 1-norms of the batched workload: n uniform on {16, 32, ...,
+    nmax}, 1-norm log-uniform in [0.1, 100]."""
     rng = np.random.default_rng(seed)
-    count, nmax = cfg["count"], cfg["nmax"]
-    sizes = rng.integers(1, nmax // 16 + 1, count) * 16
+    sizes = rng.integers(1, cfg["nmax"] // 16 + 1, count) * 16
     norms = np.exp(rng.uniform(np.log(0.1), np.log(100.0), count))
-    mats = []
-    for n, t in zip(sizes, norms):
-        a = rng.standard_normal((n, n))
-        a = (a * (t / np.abs(a).sum(axis=0).max())).astype(np.float32)
-        mats.append(a)
-    return mats
+    return sizes, norms
+
+
+def batched_matrix(n, norm, i, seed=20261204):
+    """Matrix i of the batched workload: N(0,1) entries from its own seeded
+    stream (so any rank can draw any matrix), rescaled to its 1-norm, float32
+    values (the float64 tier gets the same values widened)."""
+    a = np.random.default_rng([seed, int(i)]).standard_normal((n, n))
+    return (a * (norm / np.abs(a).sum(axis=0).max())).astype(np.float32)
+
+
+def batched_workload(cfg, indices=None, total=None):
+    sizes, norms = batched_spec(cfg, total or cfg["count"])
+    idx = range(len(sizes)) if indices is None else indices
+    return [batched_matrix(int(sizes[i]), float(norms[i]), i) for i in idx]
 
 
 def vjp_pair(n, norm, seed):
@@ -211,7 +218,7 @@ def run_reference(args, cfg):
     dtype = {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[cfg["suf"]]
     single = cfg["suf"] in "sc"
     if kind == "batched":
-        mats = [m.astype(np.float64) for m in batched_workload(cfg)[:32]]
+        mats = [m.astype(np.float64) for m in batched_workload(cfg, range(32))]
         per_step, unit = len(mats), "expm/s"
 
         def one():
@@ -494,9 +501,22 @@ def run_batched(args, cfg):
 
     lib = capi.load()
     suf = cfg["suf"]
-    mats_all = batched_workload(cfg)
-    # weak scaling: every rank gets the full per-GPU batch
-    mats = mats_all
+    if world > 1:
+        # weak scaling: a global batch of world x count matrices, partitioned
+        # across the ranks by algorithmic cost (no data-path collective)
+        from calaman_g_b200.shard import expm_cost, partition
+
+        total = world * cfg["count"]
+        sizes, norms = batched_spec(cfg, total)
+        plan_fn = lib.calaman_expm_plan_s if suf == "s" else lib.calaman_expm_plan_d
+        costs = []
+        for n_, t_ in zip(sizes, norms):
+            p_ = plan_fn(float(t_))
+            costs.append(expm_cost(int(n_), p_.m, p_.s))
+        mine = partition(costs, world)[rank]
+        mats = batched_workload(cfg, mine, total)
+    else:
+        mats = batched_workload(cfg)
     count = len(mats)
     ns = [m.shape[0] for m in mats]
     tdt = torch.float32 if suf == "s" else torch.float64
@@ -578,8 +598,13 @@ def run_batched(args, cfg):
     if any(info.cpu().tolist()):
         raise RuntimeError("an LU reported a zero pivot")
     total_ms, e2e_ms = _max_over_ranks(torch, dist, dev, [total_ms, e2e_ms])
-    value = world * count * args.steps / (total_ms * 1e-3)
-    e2e_value = world * count * args.steps / (e2e_ms * 1e-3)
+    total_count = count
+    if dist:
+        tc = torch.tensor([count], dtype=torch.float64, device=dev)
+        dist.all_reduce(tc)
+        total_count = int(tc.item())
+    value = total_count * args.steps / (total_ms * 1e-3)
+    e2e_value = total_count * args.steps / (e2e_ms * 1e-3)
     if rank == 0:
         pl = list(plans)
         flops = sum(expm_flops(n, p.m, p.s, False) for n, p in zip(ns, pl))
@@ -664,8 +689,9 @@ def batched_cpu_sample(mats, suf, seconds=10.0):
 
 
 def run_vjp(args, cfg):
-    """One step = the adjoint of expm for the whole workload through the C ABI
-    (calaman_expm_vjp_<t>): one 2048^2 call, or 512 calls of 128^2."""
+    """One step = the adjoint of expm for the whole workload through the C ABI:
+    one calaman_expm_vjp_<t> call (2048^2), or one calaman_expm_vjp_batched_<t>
+    call over the 512 pairs of 128^2."""
     torch, world, rank, local, dev, dist = _init_dist()
     from calaman_g_b200 import capi
 
@@ -684,24 +710,46 @@ def run_vjp(args, cfg):
     assert lib.calamanCreate(ctypes.byref(h)).ok
     assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
     nb = ctypes.c_size_t()
-    assert getattr(lib, f"calaman_expm_vjp_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
-    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
-    info = torch.zeros(2, dtype=torch.int32, device=dev)
-    plan = capi.ExpmPlan()
-    fn = getattr(lib, f"calaman_expm_vjp_{suf}")
     esz = dA.element_size()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    plan = capi.ExpmPlan()
+    if count == 1:
+        # one pair: calaman_expm_vjp_<t>
+        assert getattr(lib, f"calaman_expm_vjp_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
+        work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+        info = torch.zeros(2, dtype=torch.int32, device=dev)
+        fn = getattr(lib, f"calaman_expm_vjp_{suf}")
 
-    def step():
-        for i in range(count):
-            st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), n,
-                    ctypes.c_void_p(dA.data_ptr() + i * n * n * esz), n,
-                    ctypes.c_void_p(dG.data_ptr() + i * n * n * esz), n,
-                    ctypes.c_void_p(dD.data_ptr() + i * n * n * esz), n, None, n,
+        def step():
+            st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), n, ctypes.c_void_p(dA.data_ptr()), n,
+                    ctypes.c_void_p(dG.data_ptr()), n, ctypes.c_void_p(dD.data_ptr()), n, None, n,
                     ctypes.c_void_p(work.data_ptr()), nb.value,
                     ctypes.cast(info.data_ptr(), capi.c_int_p), ctypes.byref(plan))
             if not st.ok:
                 raise RuntimeError(f"expm_vjp failed: {st!r}")
+    else:
+        # many pairs: one calaman_expm_vjp_batched_<t> call per step
+        IntArr, PtrArr = ctypes.c_int * count, ctypes.c_void_p * count
+        PP = ctypes.POINTER(ctypes.c_void_p)
+        h_n = IntArr(*([n] * count))
+        ip = ctypes.cast(h_n, capi.c_int_p)
+        h_A = PtrArr(*[dA.data_ptr() + i * n * n * esz for i in range(count)])
+        h_G = PtrArr(*[dG.data_ptr() + i * n * n * esz for i in range(count)])
+        h_D = PtrArr(*[dD.data_ptr() + i * n * n * esz for i in range(count)])
+        assert getattr(lib, f"calaman_expm_vjp_batched_bufferSize_{suf}")(h, count, ip, ctypes.byref(nb)).ok
+        work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+        info = torch.zeros(2 * count, dtype=torch.int32, device=dev)
+        plans = (capi.ExpmPlan * count)()
+        fn = getattr(lib, f"calaman_expm_vjp_batched_{suf}")
+
+        def step():
+            st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), count, ip, ctypes.cast(h_A, PP), ip,
+                    ctypes.cast(h_G, PP), ip, ctypes.cast(h_D, PP), ip, None, ip,
+                    ctypes.c_void_p(work.data_ptr()), nb.value,
+                    ctypes.cast(info.data_ptr(), capi.c_int_p), plans)
+            if not st.ok:
+                raise RuntimeError(f"expm_vjp_batched failed: {st!r}")
+            plan.m, plan.s, plan.num_gemms = plans[0].m, plans[0].s, plans[0].num_gemms
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):

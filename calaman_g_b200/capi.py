@@ -142,9 +142,16 @@ SIGNATURES["calaman_expm_noalloc_d"] = (Status, [_H, c_void_p, c_int, c_void_p, 
 # expm_batched: blas, solver, stream, batch, h_n, h_A, h_lda, h_E, h_lde, work, bytes, info, plans
 _BATCHED = [_H, _H, c_void_p, c_int, c_int_p, ctypes.POINTER(c_void_p), c_int_p,
             ctypes.POINTER(c_void_p), c_int_p, c_void_p, c_size_t, c_int_p, ctypes.POINTER(ExpmPlan)]
+# expm_vjp_batched: blas, solver, stream, batch, h_n, h_A, h_lda, h_G, h_ldg, h_gradA, h_ldga,
+#                   h_expA, h_lde, work, bytes, info, plans
+_PP = ctypes.POINTER(c_void_p)
+_VJPB = [_H, _H, c_void_p, c_int, c_int_p, _PP, c_int_p, _PP, c_int_p, _PP, c_int_p, _PP, c_int_p,
+         c_void_p, c_size_t, c_int_p, ctypes.POINTER(ExpmPlan)]
 for _suf in ("s", "d"):
     SIGNATURES[f"calaman_expm_batched_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int_p, c_size_t_p])
     SIGNATURES[f"calaman_expm_batched_{_suf}"] = (Status, _BATCHED)
+    SIGNATURES[f"calaman_expm_vjp_batched_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int_p, c_size_t_p])
+    SIGNATURES[f"calaman_expm_vjp_batched_{_suf}"] = (Status, _VJPB)
 SIGNATURES["calamanSetFloatSplit"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetFloatSplit"] = (Status, [_H, c_int_p])
 

@@ -63,13 +63,16 @@ template <typename To> __device__ __forceinline__ To convert_elem(double x);
 template <> __device__ __forceinline__ double convert_elem<double>(double x) { return x; }
 template <> __device__ __forceinline__ float convert_elem<float>(double x) { return (float)x; }
 
+__device__ __forceinline__ float conj_elem(float x) { return x; }
+__device__ __forceinline__ double conj_elem(double x) { return x; }
+
 __device__ __forceinline__ int degree_slot(int m) { return m == 13 ? 4 : (m - 3) / 2; }
 
 // ---- 1-norm of every matrix: one CTA per matrix --------------------------
-template <typename T, typename Wd>
-__global__ void __launch_bounds__(256) b_norm_kernel(const BItem<T, Wd> *__restrict__ items,
+template <typename Item>
+__global__ void __launch_bounds__(256) b_norm_kernel(const Item *__restrict__ items,
                                                      double *__restrict__ norms) {
-  const BItem<T, Wd> it = items[blockIdx.x];
+  const Item it = items[blockIdx.x];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double best = 0.0;
   bool nan = false;
@@ -209,49 +212,63 @@ __global__ void __launch_bounds__(256) b_narrow_kernel(const BItem<T, Wd> *__res
   }
 }
 
-// ---- grouped GEMM: C = A B (+ C), n x n x n per matrix, one 64 x 64 tile per CTA
+// ---- grouped GEMM: C (+)= +-(A B [+ A2 B2]), n x n x n per matrix, one 64 x 64
+// output tile per CTA. What a phase multiplies is decided per matrix by an
+// operand policy (Ops::pade for the evaluation phases, Ops::square for the
+// squarings); blockIdx.y selects a sub-problem of the phase.
 template <typename U>
 struct GOps {
-  const U *A, *B;
-  U *C;
-  int lda, ldb, ldc;
-  bool acc;
+  const U *A = nullptr, *B = nullptr, *A2 = nullptr, *B2 = nullptr;
+  U *C = nullptr;
+  int lda = 0, ldb = 0, lda2 = 0, ldb2 = 0, ldc = 0;
+  bool acc = false, neg = false;
 };
 
-template <typename T, typename Wd>
-__device__ __forceinline__ bool phase_ops_t(const BItem<T, Wd> &it, const BPlan &pl, int phase, int sub,
-                                            GOps<T> &o) {
-  const T *X = pl.s > 0 ? it.X : it.A;
-  const int ldx = pl.s > 0 ? it.n : it.lda;
-  o.lda = o.ldb = o.ldc = it.n;
-  o.acc = false;
-  switch (phase) {
-  case kPhA2:
-    o.A = X; o.lda = ldx; o.B = X; o.ldb = ldx; o.C = it.P0;
-    return true;
-  case kPhA4:
-    o.A = it.P0; o.B = it.P0; o.C = it.P1;
-    return pl.np >= 2;
-  case kPhA6:
-    o.A = it.P1; o.B = it.P0; o.C = it.P2;
-    return pl.np >= 3;
-  case kPhA8:
-    o.A = it.P1; o.B = it.P1; o.C = it.P3;
-    return pl.np >= 4;
-  case kPhM13:
-    o.A = it.P2; o.B = sub ? it.P3 : it.Tt; o.C = sub ? it.V : it.W; o.acc = true;
-    return pl.m == 13;
-  case kPhU:
-    o.A = X; o.lda = ldx; o.B = it.W; o.C = it.P0;
-    return true;
-  default:
-    return false;
+// expm: the evaluation phases and the squarings of BItem matrices
+struct ExpmOps {
+  template <typename T, typename Wd>
+  static __device__ __forceinline__ bool pade(const BItem<T, Wd> &it, const BPlan &pl, int phase, int sub,
+                                              GOps<T> &o) {
+    const T *X = pl.s > 0 ? it.X : it.A;
+    const int ldx = pl.s > 0 ? it.n : it.lda;
+    o.lda = o.ldb = o.ldc = it.n;
+    switch (phase) {
+    case kPhA2:
+      o.A = X; o.lda = ldx; o.B = X; o.ldb = ldx; o.C = it.P0;
+      return true;
+    case kPhA4:
+      o.A = it.P0; o.B = it.P0; o.C = it.P1;
+      return pl.np >= 2;
+    case kPhA6:
+      o.A = it.P1; o.B = it.P0; o.C = it.P2;
+      return pl.np >= 3;
+    case kPhA8:
+      o.A = it.P1; o.B = it.P1; o.C = it.P3;
+      return pl.np >= 4;
+    case kPhM13:
+      o.A = it.P2; o.B = sub ? it.P3 : it.Tt; o.C = sub ? it.V : it.W; o.acc = true;
+      return pl.m == 13;
+    case kPhU:
+      o.A = X; o.lda = ldx; o.B = it.W; o.C = it.P0;
+      return true;
+    default:
+      return false;
+    }
   }
-}
+  // square k reads wa for odd k, wb for even k
+  template <typename T, typename Wd>
+  static __device__ __forceinline__ bool square(const BItem<T, Wd> &it, const BPlan &pl, int sub, int k,
+                                                GOps<Wd> &o) {
+    o.A = o.B = (k & 1) ? it.wa : it.wb;
+    o.C = (k & 1) ? it.wb : it.wa;
+    o.lda = o.ldb = o.ldc = it.n;
+    return pl.s >= k && sub == 0;
+  }
+};
 
-template <typename T, typename Wd, typename U, bool kSquare>
+template <typename Item, typename U, typename Ops, bool kSquare>
 __global__ void __launch_bounds__(256)
-    b_gemm_kernel(const BItem<T, Wd> *__restrict__ items, const BPlan *__restrict__ plans,
+    g_gemm_kernel(const Item *__restrict__ items, const BPlan *__restrict__ plans,
                   const int *__restrict__ tile_prefix, int batch, int phase, int ksq) {
   // the matrix of this tile: last i with tile_prefix[i] <= blockIdx.x
   const int tile = blockIdx.x;
@@ -261,18 +278,13 @@ __global__ void __launch_bounds__(256)
     if (tile_prefix[mid] <= tile) lo = mid;
     else hi = mid - 1;
   }
-  const BItem<T, Wd> it = items[lo];
+  const Item it = items[lo];
   const BPlan pl = plans[lo];
   GOps<U> o;
   if constexpr (kSquare) {
-    if (pl.s < ksq) return;
-    // square k reads wa for odd k, wb for even k
-    o.A = o.B = (ksq & 1) ? it.wa : it.wb;
-    o.C = (ksq & 1) ? it.wb : it.wa;
-    o.lda = o.ldb = o.ldc = it.n;
-    o.acc = false;
+    if (!Ops::square(it, pl, blockIdx.y, ksq, o)) return;
   } else {
-    if (!phase_ops_t<T, Wd>(it, pl, phase, blockIdx.y, o)) return;
+    if (!Ops::pade(it, pl, phase, blockIdx.y, o)) return;
   }
   const int n = it.n;
   const int tn = (n + kGTile - 1) / kGTile;
@@ -292,37 +304,43 @@ __global__ void __launch_bounds__(256)
   // global -> register staging: A tile (64 rows x 16 k), B tile (16 k x 64 cols)
   const int ar = t & 63, ak = t >> 6;   // A: rows ar, k = ak + 4 q
   const int bk = t & 15, bc = t >> 4;   // B: k = bk, columns bc + 16 q
-  U ra[4], rb[4];
-  auto load = [&](int k0) {
+  const int nprod = o.A2 ? 2 : 1;
+  for (int pr = 0; pr < nprod; ++pr) {
+    const U *Am = pr ? o.A2 : o.A;
+    const U *Bm = pr ? o.B2 : o.B;
+    const int lda = pr ? o.lda2 : o.lda, ldb = pr ? o.ldb2 : o.ldb;
+    U ra[4], rb[4];
+    auto load = [&](int k0) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int r = m0 + ar, k = k0 + ak + 4 * q;
-      ra[q] = (r < n && k < n) ? o.A[(std::size_t)k * o.lda + r] : elem<U>::zero();
-      const int c = n0 + bc + 16 * q, kb = k0 + bk;
-      rb[q] = (c < n && kb < n) ? o.B[(std::size_t)c * o.ldb + kb] : elem<U>::zero();
-    }
-  };
-  load(0);
-  for (int k0 = 0; k0 < n; k0 += kGK) {
-    __syncthreads();
+      for (int q = 0; q < 4; ++q) {
+        const int r = m0 + ar, k = k0 + ak + 4 * q;
+        ra[q] = (r < n && k < n) ? Am[(std::size_t)k * lda + r] : elem<U>::zero();
+        const int c = n0 + bc + 16 * q, kb = k0 + bk;
+        rb[q] = (c < n && kb < n) ? Bm[(std::size_t)c * ldb + kb] : elem<U>::zero();
+      }
+    };
+    load(0);
+    for (int k0 = 0; k0 < n; k0 += kGK) {
+      __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      As[ak + 4 * q][ar] = ra[q];
-      Bs[bk][bc + 16 * q] = rb[q];
-    }
-    __syncthreads();
-    if (k0 + kGK < n) load(k0 + kGK);
+      for (int q = 0; q < 4; ++q) {
+        As[ak + 4 * q][ar] = ra[q];
+        Bs[bk][bc + 16 * q] = rb[q];
+      }
+      __syncthreads();
+      if (k0 + kGK < n) load(k0 + kGK);
 #pragma unroll
-    for (int kk = 0; kk < kGK; ++kk) {
-      U a[4], bv[4];
+      for (int kk = 0; kk < kGK; ++kk) {
+        U a[4], bv[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+        for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][ty + 16 * j];
+        for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][ty + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmac(a[i], bv[j], acc[i][j]);
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmac(a[i], bv[j], acc[i][j]);
+      }
     }
   }
   U old[4][4];  // accumulate: every old C value in flight before the first store
@@ -341,7 +359,8 @@ __global__ void __launch_bounds__(256)
     for (int i = 0; i < 4; ++i) {
       const int r = m0 + tx + 16 * i;
       if (r >= n) continue;
-      o.C[(std::size_t)c * o.ldc + r] = o.acc ? add(old[i][j], acc[i][j]) : acc[i][j];
+      const U v = o.neg ? sub(old[i][j], acc[i][j]) : add(old[i][j], acc[i][j]);
+      o.C[(std::size_t)c * o.ldc + r] = v;
     }
   }
 }
@@ -354,67 +373,129 @@ constexpr int kBU = 8;
 template <typename T> struct BLuOcc { static constexpr int kMinBlocks = 1; };
 template <> struct BLuOcc<float> { static constexpr int kMinBlocks = 2; };
 
-// kBU consecutive elements of a shared-memory row as 16-byte vector loads
-// (one load instruction per 16 bytes instead of one per element).
-template <typename T>
-__device__ __forceinline__ void lds_chunk(const T *src, T (&dst)[kBU]) {
-  static_assert((kBU * sizeof(T)) % 16 == 0, "chunk must be whole 16-byte vectors");
-  union {
-    float4 v[kBU * sizeof(T) / 16];
-    T e[kBU];
-  } u;
-  const float4 *s4 = reinterpret_cast<const float4 *>(src);
-#pragma unroll
-  for (int i = 0; i < (int)(kBU * sizeof(T) / 16); ++i) u.v[i] = s4[i];
-#pragma unroll
-  for (int i = 0; i < kBU; ++i) dst[i] = u.e[i];
-}
+// D(r0 + i, c) -= sum_{j < jb} L(i, j) blk[j][c] for i < mrows, c in [c0, c0 + ncols),
+// with L(i, j) = L[j * ldl + r0 + i] (column-major, global). All threads take
+// part: 64 x 64 output blocks, thread (tr, tc) = (t % 16, t / 16) owns rows
+// tr + 16 a and columns 4 tc + b (a, b < 4) of a block; L's 64 rows of a block
+// are staged in shared memory. c0 is a multiple of 4 and blk rows are padded
+// by 64 columns, so the 4-wide shared loads never leave their row.
+constexpr int kBlkLd = kBThreads + 64;
 
-// M(t, c) -= sum_j w[j] * blk[j][c] for c in [c0, n), element t of each
-// column (one row per thread). c0 is a multiple of kBU and n <= kBThreads, so
-// every chunk of blk lies inside its 16-byte-aligned row.
 template <typename T>
-__device__ __forceinline__ void row_update(T *__restrict__ M, int ld, int t, int c0, int n,
-                                           const T (&w)[kBPanel], int jb,
-                                           const T (*__restrict__ blk)[kBThreads]) {
-  for (int c = c0; c < n; c += kBU) {
-    T v[kBU];
+__device__ __forceinline__ void lds4(const T *src, T (&dst)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4 *>(src);
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+  } else if constexpr (sizeof(T) == 8) {
+    const double2 *s2 = reinterpret_cast<const double2 *>(src);
+    union { double2 v[2]; T e[4]; } u;
+    u.v[0] = s2[0];
+    u.v[1] = s2[1];
 #pragma unroll
-    for (int u = 0; u < kBU; ++u) v[u] = c + u < n ? M[(std::size_t)(c + u) * ld + t] : elem<T>::zero();
+    for (int i = 0; i < 4; ++i) dst[i] = u.e[i];
+  } else {
 #pragma unroll
-    for (int j = 0; j < kBPanel; ++j) {
-      if (j < jb) {
-        T b[kBU];
-        lds_chunk(&blk[j][c], b);
-#pragma unroll
-        for (int u = 0; u < kBU; ++u) v[u] = sub(v[u], mul(w[j], b[u]));
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kBU; ++u)
-      if (c + u < n) M[(std::size_t)(c + u) * ld + t] = v[u];
+    for (int i = 0; i < 4; ++i) dst[i] = src[i];
   }
 }
 
-template <typename T, typename Wd>
+template <typename T>
+__device__ void cta_update(T *__restrict__ D, int ldd, int r0, int mrows, int c0, int ncols,
+                           const T *__restrict__ L, int ldl, int jb, const T (*__restrict__ blk)[kBlkLd],
+                           T (*__restrict__ Ls)[64]) {
+  const int t = threadIdx.x, tr = t & 15, tc = t >> 4;
+  for (int rb = 0; rb < mrows; rb += 64) {
+    __syncthreads();  // Ls is rewritten
+    for (int e = t; e < 64 * kBPanel; e += kBThreads) {
+      const int i = e & 63, j = e >> 6;
+      Ls[j][i] = (j < jb && rb + i < mrows) ? L[(std::size_t)j * ldl + r0 + rb + i] : elem<T>::zero();
+    }
+    __syncthreads();
+    for (int cb = 0; cb < ncols; cb += 64) {
+      T acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = elem<T>::zero();
+      const int cc = c0 + cb + 4 * tc;
+#pragma unroll 4
+      for (int j = 0; j < jb; ++j) {
+        T av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) av[a] = Ls[j][tr + 16 * a];
+        lds4(&blk[j][cc], bv);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fmac(av[a], bv[b], acc[a][b]);
+      }
+      T old[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int i = rb + tr + 16 * a, c = cc + b;
+          old[a][b] = (i < mrows && c < c0 + ncols) ? D[(std::size_t)c * ldd + r0 + i] : elem<T>::zero();
+        }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int i = rb + tr + 16 * a, c = cc + b;
+          if (i < mrows && c < c0 + ncols) D[(std::size_t)c * ldd + r0 + i] = sub(old[a][b], acc[a][b]);
+        }
+    }
+  }
+  __syncthreads();
+}
+
+// What the LU kernel factors and solves for one matrix: q (factored in place,
+// ld n), the right-hand side B (ld n), the solution D (ldd), where the row
+// permutation is kept for a later solve with the same factors (may be null),
+// and the matrix's index in the caller's batch (info).
+template <typename T>
+struct LuOps {
+  T *Q;
+  const T *B;
+  T *D;
+  int ldd;
+  int *perm;
+  int id;
+};
+
+// expm: factor q = V, solve for the quotient from p (in P0) into the output
+// (s = 0) or into X (s > 0, squared afterwards)
+struct ExpmLu {
+  template <typename T, typename Wd>
+  static __device__ __forceinline__ LuOps<T> ops(const BItem<T, Wd> &it, const BPlan &pl, int) {
+    return LuOps<T>{it.V, it.P0, pl.s > 0 ? it.X : it.E, pl.s > 0 ? it.n : it.lde, nullptr, it.id};
+  }
+};
+
+// kFactor: LU with partial pivoting of Q, then the solve; otherwise the solve
+// alone with factors and permutation from an earlier kFactor launch.
+template <typename Item, typename T, typename Lu, bool kFactor>
 __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
-    b_lu_solve_kernel(const BItem<T, Wd> *__restrict__ items, const BPlan *__restrict__ plans,
-                      int *__restrict__ info) {
+    g_lu_kernel(const Item *__restrict__ items, const BPlan *__restrict__ plans, int *__restrict__ info,
+                int mode) {
   using R = typename elem<T>::real;
-  const BItem<T, Wd> it = items[blockIdx.x];
+  const Item it = items[blockIdx.x];
   const BPlan pl = plans[blockIdx.x];
   const int n = it.n;
-  T *Q = it.V;         // factored in place (ld n)
-  const T *B = it.P0;  // right-hand side p (ld n)
-  T *D = pl.s > 0 ? it.X : it.E;
-  const int ldd = pl.s > 0 ? n : it.lde;
+  const LuOps<T> lo = Lu::ops(it, pl, mode);
+  T *Q = lo.Q;
+  const T *B = lo.B;
+  T *D = lo.D;
+  const int ldd = lo.ldd;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
 
-  // dynamic: blk[kBPanel][kBThreads] (per-column staging, U12 rows, solved
-  // right-hand-side block rows), then diag[kBPanel][kBPanel + 1]
+  // dynamic: blk[kBPanel][kBlkLd] (per-column staging, U12 rows, solved
+  // right-hand-side block rows), Ls[kBPanel][64] (staged L rows of the block
+  // updates), then diag[kBPanel][kBPanel + 1]
   extern __shared__ __align__(16) unsigned char b_smem[];
-  auto blk = reinterpret_cast<T(*)[kBThreads]>(b_smem);
-  auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * kBThreads);
+  auto blk = reinterpret_cast<T(*)[kBlkLd]>(b_smem);
+  auto Ls = reinterpret_cast<T(*)[64]>(b_smem + sizeof(T) * kBPanel * kBlkLd);
+  auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (kBlkLd + 64));
   __shared__ T xrow[2][kBPanel];   // [0]: old row a, [1]: the pivot row
   __shared__ T rdiag[kBPanel];     // reciprocals of U's diagonal block
   __shared__ int perm[kBThreads];  // P: row i of P q is row perm[i] of q
@@ -424,12 +505,12 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
   __shared__ int red_i[kBThreads / 32];
   __shared__ int first_zero;
 
-  if (t < n) perm[t] = t;
+  if (t < n) perm[t] = kFactor ? t : lo.perm[t];
   if (t == 0) first_zero = 0;
   const double sfmin = sizeof(R) == 4 ? (double)FLT_MIN : DBL_MIN;
 
   T r[kBPanel];
-  for (int k = 0; k < n; k += kBPanel) {
+  for (int k = 0; k < (kFactor ? n : 0); k += kBPanel) {
     const int jb = min(kBPanel, n - k);
     const bool mine = t >= k && t < n;
 #pragma unroll
@@ -568,14 +649,18 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         }
     }
     __syncthreads();
-    // trailing update A22 -= L21 U12, thread i owns row i
-    if (t >= k + jb && t < n) row_update(Q, n, t, k + jb, n, r, jb, blk);
+    // trailing update A22 -= L21 U12 by the whole CTA
+    cta_update(Q, n, k + jb, n - k - jb, k + jb, n - k - jb, Q + (std::size_t)k * n, n, jb, blk, Ls);
+  }
+  if (kFactor) {
+    if (t == 0) {
+      info[2 * lo.id] = first_zero;
+      info[2 * lo.id + 1] = 0;
+    }
     __syncthreads();
+    if (lo.perm != nullptr && t < n) lo.perm[t] = perm[t];
   }
-  if (t == 0) {
-    info[2 * it.id] = first_zero;
-    info[2 * it.id + 1] = 0;
-  }
+  __syncthreads();
 
   // ---- solve q R = p:  R = U^-1 L^-1 (P p) -------------------------------
   if (t < n) {
@@ -616,12 +701,7 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         }
     }
     __syncthreads();
-    if (t >= k + jb && t < n) {
-#pragma unroll
-      for (int j = 0; j < kBPanel; ++j) r[j] = j < jb ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
-      row_update(D, ldd, t, 0, n, r, jb, blk);
-    }
-    __syncthreads();
+    cta_update(D, ldd, k + jb, n - k - jb, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
   // backward, non-unit upper
   for (int k = ((n - 1) / kBPanel) * kBPanel; k >= 0; k -= kBPanel) {
@@ -655,12 +735,7 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         }
     }
     __syncthreads();
-    if (t < k) {
-#pragma unroll
-      for (int j = 0; j < kBPanel; ++j) r[j] = j < jb ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
-      row_update(D, ldd, t, 0, n, r, jb, blk);
-    }
-    __syncthreads();
+    cta_update(D, ldd, 0, k, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
 }
 
@@ -810,8 +885,8 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
   const dim3 ew((unsigned)count, (unsigned)((max_n * max_n + kEwChunk - 1) / kEwChunk));
   auto gemm = [&](int phase, int ysub) -> cudaError_t {
     return timed_group(st, phase_flops(ns, pls, phase, 0), [&] {
-      b_gemm_kernel<C, W, C, false><<<dim3(tiles, ysub), 256, 0, st>>>(d_items, d_plans, d_prefix,
-                                                                        count, phase, 0);
+      g_gemm_kernel<BItem<C, W>, C, ExpmOps, false><<<dim3(tiles, ysub), 256, 0, st>>>(
+          d_items, d_plans, d_prefix, count, phase, 0);
       return launched();
     });
   };
@@ -826,11 +901,11 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
   b_split_kernel<C, W><<<ew, 256, 0, st>>>(d_items);
   if ((e = launched()) != cudaSuccess) return e;
   {
-    const std::size_t smem = sizeof(C) * (kBPanel * kBThreads + kBPanel * (kBPanel + 1));
-    auto kern = b_lu_solve_kernel<C, W>;
+    const std::size_t smem = sizeof(C) * (kBPanel * (kBlkLd + 64) + kBPanel * (kBPanel + 1));
+    auto kern = g_lu_kernel<BItem<C, W>, C, ExpmLu, true>;
     if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
       return e;
-    kern<<<count, kBThreads, smem, st>>>(d_items, d_plans, d_info);
+    kern<<<count, kBThreads, smem, st>>>(d_items, d_plans, d_info, 0);
     if ((e = launched()) != cudaSuccess) return e;
   }
   if (max_s > 0) {
@@ -838,7 +913,8 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
     if ((e = launched()) != cudaSuccess) return e;
     for (int k = 1; k <= max_s; ++k) {
       e = timed_group(st, phase_flops(ns, pls, kPhSq, k), [&] {
-        b_gemm_kernel<C, W, W, true><<<tiles, 256, 0, st>>>(d_items, d_plans, d_prefix, count, kPhSq, k);
+        g_gemm_kernel<BItem<C, W>, W, ExpmOps, true><<<tiles, 256, 0, st>>>(d_items, d_plans, d_prefix,
+                                                                            count, kPhSq, k);
         return launched();
       });
       if (e != cudaSuccess) return e;
@@ -905,7 +981,7 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
   }
   // pageable sources: each copy returns once its data is staged
   CLM_CUDA(cudaMemcpyAsync(d_lo, lo.data(), sizeof(BItem<T, Hi>) * batch, cudaMemcpyHostToDevice, st));
-  b_norm_kernel<T, Hi><<<batch, 256, 0, st>>>(d_lo, d_norms);
+  b_norm_kernel<BItem<T, Hi>><<<batch, 256, 0, st>>>(d_lo, d_norms);
   CLM_CUDA(launched());
   std::vector<double> norms(batch);
   CLM_CUDA(cudaMemcpyAsync(norms.data(), d_norms, sizeof(double) * batch, cudaMemcpyDeviceToHost, st));
@@ -997,6 +1073,504 @@ calamanStatus_t batched_bytes(int batch, const int *h_n, std::size_t *bytes) {
   return ok_status();
 }
 
+// ===========================================================================
+// The adjoint of expm over a batch (new entry point, see vjp.cu for the
+// method): per pair (A, G), X = 2^-s A^H, D = 2^-s G, and every evaluation
+// phase carries its derivative -- grouped GEMM phases with two sub-problems
+// (value, derivative), the quotient and its derivative through one LU, and
+// (R, L) <- (R^2, R L + L R) squarings.
+// ===========================================================================
+template <typename T, typename Wd>
+struct BVItem {
+  const T *A, *G;  // inputs (lda, ldg)
+  T *Dg, *E;       // outputs: gradient (ldd), expm(A) or null (lde)
+  T *Xs, *Ds, *P0, *P1, *P2, *P3, *M0, *M1, *M2, *M3, *T1, *T2, *V, *W, *LV, *LW;
+  Wd *wr, *wl, *wr2, *wl2;
+  int *perm;
+  int n, lda, ldg, ldd, lde, id;
+};
+
+constexpr int kPhRhs = 10;  // dp - dq R into T2
+
+struct VjpOps {
+  template <typename T, typename Wd>
+  static __device__ __forceinline__ bool pade(const BVItem<T, Wd> &it, const BPlan &pl, int phase, int sub,
+                                              GOps<T> &o) {
+    const int n = it.n;
+    o.lda = o.ldb = o.lda2 = o.ldb2 = o.ldc = n;
+    auto two = [&](const T *a, const T *b, const T *a2, const T *b2, T *c) {
+      o.A = a; o.B = b; o.A2 = a2; o.B2 = b2; o.C = c;
+    };
+    switch (phase) {
+    case kPhA2:  // A2 = X X; dA2 = X D + D X
+      if (sub == 0) two(it.Xs, it.Xs, nullptr, nullptr, it.P0);
+      else two(it.Xs, it.Ds, it.Ds, it.Xs, it.M0);
+      return sub < 2;
+    case kPhA4:  // A4 = A2 A2; dA4 = A2 dA2 + dA2 A2
+      if (sub == 0) two(it.P0, it.P0, nullptr, nullptr, it.P1);
+      else two(it.P0, it.M0, it.M0, it.P0, it.M1);
+      return sub < 2 && pl.np >= 2;
+    case kPhA6:  // A6 = A4 A2; dA6 = dA4 A2 + A4 dA2
+      if (sub == 0) two(it.P1, it.P0, nullptr, nullptr, it.P2);
+      else two(it.M1, it.P0, it.P1, it.M0, it.M2);
+      return sub < 2 && pl.np >= 3;
+    case kPhA8:  // A8 = A4 A4; dA8 = A4 dA4 + dA4 A4
+      if (sub == 0) two(it.P1, it.P1, nullptr, nullptr, it.P3);
+      else two(it.P1, it.M1, it.M1, it.P1, it.M3);
+      return sub < 2 && pl.np >= 4;
+    case kPhM13:  // W += A6 W1, V += A6 Z1 and their derivatives
+      o.acc = true;
+      if (sub == 0) two(it.P2, it.T1, nullptr, nullptr, it.W);
+      else if (sub == 1) two(it.P2, it.P3, nullptr, nullptr, it.V);
+      else if (sub == 2) two(it.P2, it.T2, it.M2, it.T1, it.LW);
+      else two(it.P2, it.M3, it.M2, it.P3, it.LV);
+      return sub < 4 && pl.m == 13;
+    case kPhU:  // U = X W; dU = X dW + D W
+      if (sub == 0) two(it.Xs, it.W, nullptr, nullptr, it.T1);
+      else two(it.Xs, it.LW, it.Ds, it.W, it.T2);
+      return sub < 2;
+    case kPhRhs:  // dp - dq R (R in P0)
+      o.acc = true;
+      o.neg = true;
+      two(it.LV, it.P0, nullptr, nullptr, it.T2);
+      return sub == 0;
+    default:
+      return false;
+    }
+  }
+  // square k reads (wr, wl) for odd k, (wr2, wl2) for even k
+  template <typename T, typename Wd>
+  static __device__ __forceinline__ bool square(const BVItem<T, Wd> &it, const BPlan &pl, int sub, int k,
+                                                GOps<Wd> &o) {
+    const Wd *r = (k & 1) ? it.wr : it.wr2, *l = (k & 1) ? it.wl : it.wl2;
+    Wd *r2 = (k & 1) ? it.wr2 : it.wr, *l2 = (k & 1) ? it.wl2 : it.wl;
+    o.lda = o.ldb = o.lda2 = o.ldb2 = o.ldc = it.n;
+    if (sub == 0) {
+      o.A = r; o.B = r; o.C = r2;
+    } else {
+      o.A = r; o.B = l; o.A2 = l; o.B2 = r; o.C = l2;
+    }
+    return pl.s >= k && sub < 2;
+  }
+};
+
+// mode 0: factor q = V, R = q^-1 p (p in T1) into P0; mode 1: dR = q^-1 T2 into M0
+struct VjpLu {
+  template <typename T, typename Wd>
+  static __device__ __forceinline__ LuOps<T> ops(const BVItem<T, Wd> &it, const BPlan &, int mode) {
+    return mode == 0 ? LuOps<T>{it.V, it.T1, it.P0, it.n, it.perm, it.id}
+                     : LuOps<T>{it.V, it.T2, it.M0, it.n, it.perm, it.id};
+  }
+};
+
+// Xs = 2^-s A^H (the transpose for real types), Ds = 2^-s G
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) v_prep_kernel(const BVItem<T, Wd> *__restrict__ items,
+                                                     const BPlan *__restrict__ plans) {
+  using R = typename elem<T>::real;
+  const BVItem<T, Wd> it = items[blockIdx.x];
+  const R f = (R)ldexp(1.0, -plans[blockIdx.x].s);
+  const int n = it.n, nn = n * n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    it.Xs[e] = scale(conj_elem(it.A[(std::size_t)r * it.lda + c]), f);
+    it.Ds[e] = scale(it.G[(std::size_t)c * it.ldg + r], f);
+  }
+}
+
+// the Pade combinations of the powers (P) and of their derivatives (M)
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) v_even_odd_kernel(const BVItem<T, Wd> *__restrict__ items,
+                                                         const BPlan *__restrict__ plans) {
+  using R = typename elem<T>::real;
+  const BVItem<T, Wd> it = items[blockIdx.x];
+  const BPlan pl = plans[blockIdx.x];
+  const double *b = c_pade[degree_slot(pl.m)];
+  const int n = it.n, nn = n * n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  const T *P[4] = {it.P0, it.P1, it.P2, it.P3};
+  const T *M[4] = {it.M0, it.M1, it.M2, it.M3};
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    const bool diag = r == c;
+    if (pl.m != 13) {
+      T v = elem<T>::zero(), w = elem<T>::zero(), lv = elem<T>::zero(), lw = elem<T>::zero();
+      for (int k = 0; k < pl.np; ++k) {
+        const T x = P[k][e], y = M[k][e];
+        v = rfma((R)b[2 * k + 2], x, v);
+        w = rfma((R)b[2 * k + 3], x, w);
+        lv = rfma((R)b[2 * k + 2], y, lv);
+        lw = rfma((R)b[2 * k + 3], y, lw);
+      }
+      if (diag) {
+        v = add_real(v, (R)b[0]);
+        w = add_real(w, (R)b[1]);
+      }
+      it.V[e] = v;
+      it.W[e] = w;
+      it.LV[e] = lv;
+      it.LW[e] = lw;
+    } else {
+      const T x1 = it.P0[e], x2 = it.P1[e], x3 = it.P2[e];
+      const T y1 = it.M0[e], y2 = it.M1[e], y3 = it.M2[e];
+      auto comb = [&](T a1, T a2, T a3, int i1, int i2, int i3) {
+        return rfma((R)b[i3], a3, rfma((R)b[i2], a2, scale(a1, (R)b[i1])));
+      };
+      T w = comb(x1, x2, x3, 3, 5, 7), v = comb(x1, x2, x3, 2, 4, 6);
+      if (diag) {
+        w = add_real(w, (R)b[1]);
+        v = add_real(v, (R)b[0]);
+      }
+      it.T1[e] = comb(x1, x2, x3, 9, 11, 13);
+      it.W[e] = w;
+      it.P3[e] = comb(x1, x2, x3, 8, 10, 12);
+      it.V[e] = v;
+      it.T2[e] = comb(y1, y2, y3, 9, 11, 13);
+      it.LW[e] = comb(y1, y2, y3, 3, 5, 7);
+      it.M3[e] = comb(y1, y2, y3, 8, 10, 12);
+      it.LV[e] = comb(y1, y2, y3, 2, 4, 6);
+    }
+  }
+}
+
+// p = V + U over T1, q = V - U over V; dp = dV + dU over T2, dq = dV - dU over LV
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) v_split_kernel(const BVItem<T, Wd> *__restrict__ items) {
+  const BVItem<T, Wd> it = items[blockIdx.x];
+  const int nn = it.n * it.n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const T u = it.T1[e], v = it.V[e], du = it.T2[e], dv = it.LV[e];
+    it.T1[e] = add(v, u);
+    it.V[e] = sub(v, u);
+    it.T2[e] = add(dv, du);
+    it.LV[e] = sub(dv, du);
+  }
+}
+
+// s > 0: (wr, wl) = wide (R, dR)
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) v_widen_kernel(const BVItem<T, Wd> *__restrict__ items,
+                                                      const BPlan *__restrict__ plans) {
+  if (plans[blockIdx.x].s == 0) return;
+  const BVItem<T, Wd> it = items[blockIdx.x];
+  const int nn = it.n * it.n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    it.wr[e] = convert_elem<Wd>(it.P0[e]);
+    it.wl[e] = convert_elem<Wd>(it.M0[e]);
+  }
+}
+
+// outputs: the gradient (the last dR), and expm(A) = (the last R)^H if wanted
+template <typename T, typename Wd>
+__global__ void __launch_bounds__(256) v_out_kernel(const BVItem<T, Wd> *__restrict__ items,
+                                                    const BPlan *__restrict__ plans) {
+  const BVItem<T, Wd> it = items[blockIdx.x];
+  const int s = plans[blockIdx.x].s;
+  const int n = it.n, nn = n * n;
+  const int end = min(nn, (int)(blockIdx.y + 1) * kEwChunk);
+  for (int e = blockIdx.y * kEwChunk + threadIdx.x; e < end; e += blockDim.x) {
+    const int c = e / n, r = e - c * n;
+    T g, x;
+    if (s == 0) {
+      g = it.M0[e];
+      x = it.P0[(std::size_t)r * n + c];
+    } else {
+      const Wd *lf = (s & 1) ? it.wl2 : it.wl, *rf = (s & 1) ? it.wr2 : it.wr;
+      g = convert_elem<T>(lf[e]);
+      x = convert_elem<T>(rf[(std::size_t)r * n + c]);
+    }
+    it.Dg[(std::size_t)c * it.ldd + r] = g;
+    if (it.E) it.E[(std::size_t)c * it.lde + r] = conj_elem(x);
+  }
+}
+
+template <typename C>
+void carve_vitem(BVItem<C, typename Wide<C>::type> &it, char *slab, int n) {
+  using W = typename Wide<C>::type;
+  const std::size_t nn = (std::size_t)n * n;
+  Layout L(slab);
+  C **bufs[16] = {&it.Xs, &it.Ds, &it.P0, &it.P1, &it.P2, &it.P3, &it.M0, &it.M1,
+                  &it.M2, &it.M3, &it.T1, &it.T2, &it.V,  &it.W,  &it.LV, &it.LW};
+  for (C **b : bufs) *b = L.take<C>(nn);
+  it.wr = L.take<W>(nn);
+  it.wl = L.take<W>(nn);
+  it.wr2 = L.take<W>(nn);
+  it.wl2 = L.take<W>(nn);
+  it.perm = L.take<int>(n);
+  it.n = n;
+}
+
+template <typename C>
+std::size_t vslab_of(int n) {
+  using W = typename Wide<C>::type;
+  const std::size_t nn = (std::size_t)n * n;
+  return 16 * align_up(nn * sizeof(C), 256) + 4 * align_up(nn * sizeof(W), 256) + align_up(n * sizeof(int), 256);
+}
+
+template <typename C>
+cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::type> *d_items,
+                           const BPlan *d_plans, const int *d_prefix, int count, int tiles, int max_n,
+                           int max_s, int *d_info, const std::vector<int> &ns,
+                           const std::vector<BPlan> &pls) {
+  using W = typename Wide<C>::type;
+  using Item = BVItem<C, W>;
+  cudaError_t e;
+  const dim3 ew((unsigned)count, (unsigned)((max_n * max_n + kEwChunk - 1) / kEwChunk));
+  // flops of a phase: per matrix, the products its sub-problems carry
+  auto vflops = [&](int phase, int k) {
+    double f = 0.0;
+    for (std::size_t i = 0; i < ns.size(); ++i) {
+      const double cube = 2.0 * ns[i] * (double)ns[i] * ns[i];
+      const BPlan &p = pls[i];
+      switch (phase) {
+      case kPhA2: case kPhU: f += 3 * cube; break;
+      case kPhA4: f += p.np >= 2 ? 3 * cube : 0.0; break;
+      case kPhA6: f += p.np >= 3 ? 3 * cube : 0.0; break;
+      case kPhA8: f += p.np >= 4 ? 3 * cube : 0.0; break;
+      case kPhM13: f += p.m == 13 ? 6 * cube : 0.0; break;
+      case kPhRhs: f += cube; break;
+      case kPhSq: f += p.s >= k ? 3 * cube : 0.0; break;
+      default: break;
+      }
+    }
+    return f;
+  };
+  auto gemm = [&](int phase, int ysub) -> cudaError_t {
+    return timed_group(st, vflops(phase, 0), [&] {
+      g_gemm_kernel<Item, C, VjpOps, false><<<dim3(tiles, ysub), 256, 0, st>>>(d_items, d_plans, d_prefix,
+                                                                               count, phase, 0);
+      return launched();
+    });
+  };
+  const std::size_t lu_smem = sizeof(C) * (kBPanel * (kBlkLd + 64) + kBPanel * (kBPanel + 1));
+  auto lu_f = g_lu_kernel<Item, C, VjpLu, true>;
+  auto lu_s = g_lu_kernel<Item, C, VjpLu, false>;
+  if ((e = cudaFuncSetAttribute(lu_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(lu_s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem)) != cudaSuccess)
+    return e;
+
+  v_prep_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+  if ((e = launched()) != cudaSuccess) return e;
+  for (int ph : {kPhA2, kPhA4, kPhA6, kPhA8})
+    if ((e = gemm(ph, 2)) != cudaSuccess) return e;
+  v_even_odd_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+  if ((e = launched()) != cudaSuccess) return e;
+  if ((e = gemm(kPhM13, 4)) != cudaSuccess) return e;
+  if ((e = gemm(kPhU, 2)) != cudaSuccess) return e;
+  v_split_kernel<C, W><<<ew, 256, 0, st>>>(d_items);
+  if ((e = launched()) != cudaSuccess) return e;
+  lu_f<<<count, kBThreads, lu_smem, st>>>(d_items, d_plans, d_info, 0);
+  if ((e = launched()) != cudaSuccess) return e;
+  if ((e = gemm(kPhRhs, 1)) != cudaSuccess) return e;
+  lu_s<<<count, kBThreads, lu_smem, st>>>(d_items, d_plans, d_info, 1);
+  if ((e = launched()) != cudaSuccess) return e;
+  if (max_s > 0) {
+    v_widen_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+    if ((e = launched()) != cudaSuccess) return e;
+    for (int k = 1; k <= max_s; ++k) {
+      e = timed_group(st, vflops(kPhSq, k), [&] {
+        g_gemm_kernel<Item, W, VjpOps, true><<<dim3(tiles, 2), 256, 0, st>>>(d_items, d_plans, d_prefix,
+                                                                             count, kPhSq, k);
+        return launched();
+      });
+      if (e != cudaSuccess) return e;
+    }
+  }
+  v_out_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
+  return launched();
+}
+
+// Workspace: [items (T) | items (FP64) | plans x2 | tile prefixes x2 | norms |
+// conversion tables x4 | one slab per pair], as the forward batch; the single
+// tier evaluates pairs with s > 0 in FP64 from FP64 copies of A and G.
+template <typename T>
+struct BVLayout {
+  using Hi = typename Wide<T>::type;
+  static constexpr bool kSplit = !std::is_same<T, Hi>::value;
+  std::size_t items_lo = 0, items_hi = 0, plans_lo = 0, plans_hi = 0, prefix_lo = 0, prefix_hi = 0,
+              norms = 0, conv = 0, total = 0;
+  std::vector<std::size_t> slab;
+  static std::size_t slab_bytes(int n) {
+    if (!kSplit) return vslab_of<T>(n);
+    const std::size_t nn = (std::size_t)n * n;
+    return std::max(vslab_of<T>(n), vslab_of<Hi>(n) + 4 * align_up(nn * sizeof(Hi), 256));
+  }
+  void plan(int batch, const int *h_n) {
+    Layout L(nullptr);
+    items_lo = L.used;  L.take<BVItem<T, Hi>>(batch);
+    items_hi = L.used;  L.take<BVItem<Hi, Hi>>(kSplit ? batch : 0);
+    plans_lo = L.used;  L.take<BPlan>(batch);
+    plans_hi = L.used;  L.take<BPlan>(kSplit ? batch : 0);
+    prefix_lo = L.used; L.take<int>(batch + 1);
+    prefix_hi = L.used; L.take<int>(kSplit ? batch + 1 : 0);
+    norms = L.used;     L.take<double>(batch);
+    conv = L.used;      L.take<BConv>(kSplit ? 4 * (std::size_t)batch : 0);
+    slab.resize(batch);
+    std::size_t at = L.used;
+    for (int i = 0; i < batch; ++i) {
+      slab[i] = at;
+      at += slab_bytes(h_n[i]);
+    }
+    total = at;
+  }
+};
+
+template <typename T>
+calamanStatus_t vjp_batched_api(calamanHandle_t blas, calamanStream_t stream, int batch, const int *h_n,
+                                const T *const *h_A, const int *h_lda, const T *const *h_G,
+                                const int *h_ldg, T *const *h_D, const int *h_ldd, T *const *h_E,
+                                const int *h_lde, void *work, std::size_t lwork, int *d_info,
+                                calamanExpmPlan_t *h_plans) {
+  using R = typename elem<T>::real;
+  using Hi = typename Wide<T>::type;
+  using Lay = BVLayout<T>;
+  if (batch < 0) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (batch == 0) return ok_status();
+  if (h_n == nullptr || h_A == nullptr || h_lda == nullptr || h_G == nullptr || h_ldg == nullptr ||
+      h_D == nullptr || h_ldd == nullptr || work == nullptr || d_info == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  for (int i = 0; i < batch; ++i) {
+    const int n = h_n[i];
+    const bool want_e = h_E != nullptr && h_E[i] != nullptr;
+    if (n < 1 || h_lda[i] < n || h_ldg[i] < n || h_ldd[i] < n || h_A[i] == nullptr ||
+        h_G[i] == nullptr || h_D[i] == nullptr || (want_e && (h_lde == nullptr || h_lde[i] < n)))
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+    if (n > kBatchedMaxN) return blas_status(CALAMAN_STATUS_NOT_SUPPORTED);
+  }
+  Lay lay;
+  lay.plan(batch, h_n);
+  if (lwork < lay.total) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  PointerModeScope pm(blas);
+  TimerScope ts(timer_of(blas));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int dev = 0;
+  CLM_CUDA(cudaGetDevice(&dev));
+  CLM_CUDA(upload_pade_table(dev));
+
+  char *base = static_cast<char *>(work);
+  auto *d_lo = reinterpret_cast<BVItem<T, Hi> *>(base + lay.items_lo);
+  auto *d_hi = reinterpret_cast<BVItem<Hi, Hi> *>(base + lay.items_hi);
+  auto *d_plo = reinterpret_cast<BPlan *>(base + lay.plans_lo);
+  auto *d_phi = reinterpret_cast<BPlan *>(base + lay.plans_hi);
+  auto *d_xlo = reinterpret_cast<int *>(base + lay.prefix_lo);
+  auto *d_xhi = reinterpret_cast<int *>(base + lay.prefix_hi);
+  auto *d_norms = reinterpret_cast<double *>(base + lay.norms);
+  auto *d_conv = reinterpret_cast<BConv *>(base + lay.conv);
+
+  std::vector<BVItem<T, Hi>> lo(batch);
+  for (int i = 0; i < batch; ++i) {
+    BVItem<T, Hi> &it = lo[i];
+    carve_vitem<T>(it, base + lay.slab[i], h_n[i]);
+    it.A = h_A[i];
+    it.G = h_G[i];
+    it.Dg = h_D[i];
+    it.E = (h_E != nullptr) ? h_E[i] : nullptr;
+    it.lda = h_lda[i];
+    it.ldg = h_ldg[i];
+    it.ldd = h_ldd[i];
+    it.lde = it.E ? h_lde[i] : 0;
+    it.id = i;
+  }
+  CLM_CUDA(cudaMemcpyAsync(d_lo, lo.data(), sizeof(BVItem<T, Hi>) * batch, cudaMemcpyHostToDevice, st));
+  b_norm_kernel<BVItem<T, Hi>><<<batch, 256, 0, st>>>(d_lo, d_norms);
+  CLM_CUDA(launched());
+  std::vector<double> norms(batch);
+  CLM_CUDA(cudaMemcpyAsync(norms.data(), d_norms, sizeof(double) * batch, cudaMemcpyDeviceToHost, st));
+  CLM_CUDA(cudaStreamSynchronize(st));
+  std::vector<calamanExpmPlan_t> plans(batch);
+  for (int i = 0; i < batch; ++i) {
+    if (!std::isfinite(norms[i])) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+    plans[i] = plan_for<R>((R)norms[i]);
+  }
+  if (h_plans)
+    for (int i = 0; i < batch; ++i) h_plans[i] = plans[i];
+
+  std::vector<BVItem<T, Hi>> lo_items;
+  std::vector<BVItem<Hi, Hi>> hi_items;
+  std::vector<BPlan> lo_plans, hi_plans;
+  std::vector<int> lo_prefix(1, 0), hi_prefix(1, 0), lo_n, hi_n;
+  std::vector<BConv> cin, cout;
+  int lo_max_n = 0, hi_max_n = 0, lo_max_s = 0, hi_max_s = 0;
+  for (int i = 0; i < batch; ++i) {
+    const calamanExpmPlan_t &p = plans[i];
+    const BPlan bp{p.m, p.s, pade_num_powers(p.m), 0};
+    const int n = h_n[i];
+    if (!Lay::kSplit || p.s == 0) {
+      lo_items.push_back(lo[i]);
+      lo_plans.push_back(bp);
+      lo_prefix.push_back(lo_prefix.back() + tiles_of(n));
+      lo_n.push_back(n);
+      lo_max_n = std::max(lo_max_n, n);
+      lo_max_s = std::max(lo_max_s, p.s);
+    } else {
+      BVItem<Hi, Hi> it{};
+      carve_vitem<Hi>(it, base + lay.slab[i], n);
+      const std::size_t nn = (std::size_t)n * n, step = align_up(nn * sizeof(Hi), 256);
+      char *extra = base + lay.slab[i] + vslab_of<Hi>(n);
+      Hi *a64 = reinterpret_cast<Hi *>(extra), *g64 = reinterpret_cast<Hi *>(extra + step);
+      Hi *d64 = reinterpret_cast<Hi *>(extra + 2 * step), *e64 = reinterpret_cast<Hi *>(extra + 3 * step);
+      it.A = a64;
+      it.G = g64;
+      it.Dg = d64;
+      it.E = lo[i].E ? e64 : nullptr;
+      it.lda = it.ldg = it.ldd = it.lde = n;
+      it.id = i;
+      hi_items.push_back(it);
+      hi_plans.push_back(bp);
+      hi_prefix.push_back(hi_prefix.back() + tiles_of(n));
+      hi_n.push_back(n);
+      hi_max_n = std::max(hi_max_n, n);
+      hi_max_s = std::max(hi_max_s, p.s);
+      cin.push_back(BConv{h_A[i], a64, n, h_lda[i], n, 0});
+      cin.push_back(BConv{h_G[i], g64, n, h_ldg[i], n, 0});
+      cout.push_back(BConv{d64, h_D[i], n, n, h_ldd[i], 0});
+      if (lo[i].E) cout.push_back(BConv{e64, lo[i].E, n, n, h_lde[i], 0});
+    }
+  }
+  const int nlo = (int)lo_items.size(), nhi = (int)hi_items.size();
+  if (nlo > 0) {
+    CLM_CUDA(cudaMemcpyAsync(d_lo, lo_items.data(), sizeof(BVItem<T, Hi>) * nlo, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_plo, lo_plans.data(), sizeof(BPlan) * nlo, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_xlo, lo_prefix.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
+    CLM_CUDA(run_vjp_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info,
+                               lo_n, lo_plans));
+  }
+  if (nhi > 0) {
+    const int nin = (int)cin.size(), nout = (int)cout.size();
+    CLM_CUDA(cudaMemcpyAsync(d_hi, hi_items.data(), sizeof(BVItem<Hi, Hi>) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_phi, hi_plans.data(), sizeof(BPlan) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_xhi, hi_prefix.data(), sizeof(int) * (nhi + 1), cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_conv, cin.data(), sizeof(BConv) * nin, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_conv + nin, cout.data(), sizeof(BConv) * nout, cudaMemcpyHostToDevice, st));
+    const unsigned chunks = (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk);
+    b_conv_kernel<T, Hi><<<dim3((unsigned)nin, chunks), 256, 0, st>>>(d_conv);
+    CLM_CUDA(launched());
+    CLM_CUDA(run_vjp_phases<Hi>(st, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info,
+                                hi_n, hi_plans));
+    b_conv_kernel<Hi, T><<<dim3((unsigned)nout, chunks), 256, 0, st>>>(d_conv + nin);
+    CLM_CUDA(launched());
+  }
+  return ok_status();
+}
+
+template <typename T>
+calamanStatus_t vjp_batched_bytes(int batch, const int *h_n, std::size_t *bytes) {
+  if (batch < 0 || bytes == nullptr || (batch > 0 && h_n == nullptr))
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  for (int i = 0; i < batch; ++i) {
+    if (h_n[i] < 1) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+    if (h_n[i] > kBatchedMaxN) return blas_status(CALAMAN_STATUS_NOT_SUPPORTED);
+  }
+  BVLayout<T> lay;
+  lay.plan(batch, h_n);
+  *bytes = batch > 0 ? lay.total : 0;
+  return ok_status();
+}
+
 }  // namespace
 }  // namespace clm
 
@@ -1028,5 +1602,22 @@ calamanStatus_t calaman_expm_batched_d(calamanBlasHandle_t blas, calamanSolverHa
   return batched_api<double>(blas, stream, batch, h_n, h_A, h_lda, h_E, h_lde, d_work, lwork, d_info,
                              h_plans);
 }
+
+#define CLM_VJPB_API(SUF, T)                                                                       \
+  calamanStatus_t calaman_expm_vjp_batched_bufferSize_##SUF(calamanSolverHandle_t, int batch,        \
+                                                            const int *h_n, size_t *bytes) {         \
+    return vjp_batched_bytes<T>(batch, h_n, bytes);                                                  \
+  }                                                                                                  \
+  calamanStatus_t calaman_expm_vjp_batched_##SUF(                                                    \
+      calamanBlasHandle_t blas, calamanSolverHandle_t, calamanStream_t stream, int batch,            \
+      const int *h_n, const T *const *h_A, const int *h_lda, const T *const *h_G, const int *h_ldg,   \
+      T *const *h_gradA, const int *h_ldga, T *const *h_expA, const int *h_lde, void *d_work,        \
+      size_t lwork, int *d_info, calamanExpmPlan_t *h_plans) {                                       \
+    return vjp_batched_api<T>(blas, stream, batch, h_n, h_A, h_lda, h_G, h_ldg, h_gradA, h_ldga,     \
+                              h_expA, h_lde, d_work, lwork, d_info, h_plans);                        \
+  }
+CLM_VJPB_API(s, float)
+CLM_VJPB_API(d, double)
+#undef CLM_VJPB_API
 
 }  // extern "C"

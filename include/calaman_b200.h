@@ -199,6 +199,30 @@ calamanStatus_t calaman_expm_batched_d(calamanBlasHandle_t blas, calamanSolverHa
                                        double *const *h_expA, const int *h_lde, void *d_work,
                                        size_t lwork_bytes, int *d_info, calamanExpmPlan_t *h_plans);
 
+/* ---- expm_vjp_batched: the adjoint over many small pairs ------------------
+ * New entry point (no counterpart in the reference). calaman_expm_vjp_* for
+ * every pair (A_i, G_i) of a batch, n_i <= 256 (larger: NOT_SUPPORTED), each
+ * with its own plan (m_i, s_i) = expm_plan(||A_i||_1). Host arrays as for
+ * calaman_expm_batched_*; h_expA may be NULL, or hold NULL entries, where
+ * expm(A_i) is not wanted (h_lde is then only read where it is). d_info: 2 *
+ * batch device ints. The _s tier evaluates pairs with s_i = 0 in FP32 and
+ * pairs with s_i > 0 in FP64, like calaman_expm_batched_s. Synchronises
+ * `stream` once. */
+calamanStatus_t calaman_expm_vjp_batched_bufferSize_s(calamanSolverHandle_t h, int batch,
+                                                      const int *h_n, size_t *bytes);
+calamanStatus_t calaman_expm_vjp_batched_bufferSize_d(calamanSolverHandle_t h, int batch,
+                                                      const int *h_n, size_t *bytes);
+calamanStatus_t calaman_expm_vjp_batched_s(
+    calamanBlasHandle_t blas, calamanSolverHandle_t solver, calamanStream_t stream, int batch,
+    const int *h_n, const float *const *h_A, const int *h_lda, const float *const *h_G,
+    const int *h_ldg, float *const *h_gradA, const int *h_ldga, float *const *h_expA,
+    const int *h_lde, void *d_work, size_t lwork_bytes, int *d_info, calamanExpmPlan_t *h_plans);
+calamanStatus_t calaman_expm_vjp_batched_d(
+    calamanBlasHandle_t blas, calamanSolverHandle_t solver, calamanStream_t stream, int batch,
+    const int *h_n, const double *const *h_A, const int *h_lda, const double *const *h_G,
+    const int *h_ldg, double *const *h_gradA, const int *h_ldga, double *const *h_expA,
+    const int *h_lde, void *d_work, size_t lwork_bytes, int *d_info, calamanExpmPlan_t *h_plans);
+
 /* ---- expm without a caller workspace ----------------------------------
  * No counterpart in the reference: calaman_G's expm always takes a caller
  * workspace. For callers that cannot call cudaMalloc (code hosted by a

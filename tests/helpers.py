@@ -244,3 +244,45 @@ def c4_batch(count: int, seed: int, nmax: int = 256):
         a = rng.standard_normal((n, n))
         mats.append(a * (t / norm1(a)))
     return mats
+
+
+def run_vjp_batched(runner, pairs, suf: str, want_expm: bool = True, lds=None, out_fill=-123.5,
+                    lwork=None):
+    """calaman_expm_vjp_batched_<suf> over a list of (A, G) pairs. Returns
+    (status, plans, gradients, expms or None, flat gradient buffers, info[batch, 2])."""
+    torch = runner.torch
+    b = len(pairs)
+    ns = [a.shape[0] for a, _ in pairs]
+    lds = lds or ns
+    dt = NP_DTYPE[suf]
+    dA = [_dev(colmajor_buffer(a, ld, suf)) for (a, _), ld in zip(pairs, lds)]
+    dG = [_dev(colmajor_buffer(g, ld, suf)) for (_, g), ld in zip(pairs, lds)]
+    dD = [_dev(np.full(n * ld, out_fill, dtype=dt)) for n, ld in zip(ns, lds)]
+    dE = [_dev(np.full(n * ld, out_fill, dtype=dt)) for n, ld in zip(ns, lds)] if want_expm else None
+    IntArr = ctypes.c_int * max(b, 1)
+    PtrArr = ctypes.c_void_p * max(b, 1)
+    h_n, h_ld = IntArr(*ns), IntArr(*lds)
+    PP = ctypes.POINTER(ctypes.c_void_p)
+    h_A = PtrArr(*[t.data_ptr() for t in dA])
+    h_G = PtrArr(*[t.data_ptr() for t in dG])
+    h_D = PtrArr(*[t.data_ptr() for t in dD])
+    h_E = PtrArr(*[t.data_ptr() for t in dE]) if dE is not None else None
+    ip = ctypes.cast(h_n, runner.capi.c_int_p)
+    ldp = ctypes.cast(h_ld, runner.capi.c_int_p)
+    nb = ctypes.c_size_t()
+    st = getattr(runner.lib, f"calaman_expm_vjp_batched_bufferSize_{suf}")(runner.h, b, ip, ctypes.byref(nb))
+    if not st.ok:
+        return st, None, None, None, None, None
+    w = runner.workspace(nb.value)
+    info = torch.full((max(2 * b, 2),), -99, dtype=torch.int32, device="cuda")
+    plans = (runner.capi.ExpmPlan * max(b, 1))()
+    st = getattr(runner.lib, f"calaman_expm_vjp_batched_{suf}")(
+        runner.h, runner.h, ctypes.c_void_p(runner.stream), b, ip, ctypes.cast(h_A, PP), ldp,
+        ctypes.cast(h_G, PP), ldp, ctypes.cast(h_D, PP), ldp,
+        ctypes.cast(h_E, PP) if h_E is not None else None, ldp, vp(w),
+        nb.value if lwork is None else lwork, ctypes.cast(info.data_ptr(), runner.capi.c_int_p), plans)
+    torch.cuda.synchronize()
+    fulls = [t.cpu().numpy() for t in dD]
+    grads = [from_buffer(f, n, ld) for f, n, ld in zip(fulls, ns, lds)]
+    exps = [from_buffer(t.cpu().numpy(), n, ld) for t, n, ld in zip(dE, ns, lds)] if dE is not None else None
+    return st, list(plans)[:b], grads, exps, fulls, info.cpu().numpy()[: 2 * b].reshape(-1, 2)
