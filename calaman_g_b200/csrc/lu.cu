@@ -898,41 +898,29 @@ __global__ void __launch_bounds__(512, 1)
     // ---- where the sub-panel's swaps moved rows: position sb + j now holds
     // old row src_top[j]; a row d below the block holds old top-block row
     // disp_src[e] (rows below only ever receive rows of the top block) ----
+    // (every lane follows one final position back through the swaps, in
+    // reverse order, to the row it came from)
     if (warp == 0) {
-      int *keys = mpos, *vals = morg;  // scratch, reused by panel_finish later
-      for (int e = lane; e < w; e += 32) {
-        keys[e] = sb + e;
-        vals[e] = sb + e;
-      }
-      __syncwarp();
-      if (lane == 0) {
-        int count = w;
-        for (int j = 0; j < w; ++j) {
-          const int b = plist[sb + j];
-          int bidx = -1;
-          if (b < sb + w) bidx = b - sb;
-          else {
-            for (int e = w; e < count; ++e)
-              if (keys[e] == b) bidx = e;
-            if (bidx < 0) {
-              bidx = count++;
-              keys[bidx] = b;
-              vals[bidx] = b;
-            }
-          }
-          if (bidx != j) {
-            const int t = vals[j];
-            vals[j] = vals[bidx];
-            vals[bidx] = t;
-          }
+      const int e = lane;
+      int x = -1;
+      if (e < w) x = sb + e;                                                      // a top-block position
+      else if (e < 2 * w && plist[sb + e - w] >= sb + w) x = plist[sb + e - w];  // a displaced row
+      if (x >= 0) {
+        const int fin = x;
+        for (int j = w - 1; j >= 0; --j) {
+          const int pj = plist[sb + j];
+          if (x == sb + j) x = pj;
+          else if (x == pj) x = sb + j;
         }
-        for (int j = 0; j < w; ++j) src_top[j] = vals[j];
-        for (int e = w; e < count; ++e) {
-          disp_row[e - w] = keys[e];
-          disp_src[e - w] = vals[e];
+        if (e < w) src_top[e] = x;
+        else {
+          disp_row[e - w] = fin;
+          disp_src[e - w] = x;
         }
-        ndisp[0] = count - w;
+      } else if (e >= w && e < 2 * w) {
+        disp_row[e - w] = -1;
       }
+      if (lane == 0) ndisp[0] = w;
     }
     __syncthreads();
     // ---- the panel's other columns: swap, and right of the sub-panel solve
@@ -957,6 +945,7 @@ __global__ void __launch_bounds__(512, 1)
         }
       }
       for (int e = 0; e < ndisp[0]; ++e) {
+        if (disp_row[e] < 0) continue;
         const int srcq = disp_src[e] - sb;
         T v = elem<T>::zero();
 #pragma unroll
