@@ -399,6 +399,32 @@ __device__ __forceinline__ void lds4(const T *src, T (&dst)[4]) {
   }
 }
 
+// Triangular solves of one right-hand-side column against the diagonal block
+// in shared memory: unit lower (forward) and non-unit upper with the diagonal's
+// reciprocals (backward). kFull: jb == kBPanel, so every bound is static.
+template <typename T, bool kFull>
+__device__ __forceinline__ void trsv_lower_unit(T (&x)[kBPanel], const T (*diag)[kBPanel + 1], int jb) {
+#pragma unroll
+  for (int j = 1; j < kBPanel; ++j)
+#pragma unroll
+    for (int q = 0; q < j; ++q)
+      if (kFull || j < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+}
+
+template <typename T, bool kFull>
+__device__ __forceinline__ void trsv_upper(T (&x)[kBPanel], const T (*diag)[kBPanel + 1], const T *rdiag,
+                                           int jb) {
+#pragma unroll
+  for (int j = kBPanel - 1; j >= 0; --j) {
+    if (kFull || j < jb) {
+#pragma unroll
+      for (int q = j + 1; q < kBPanel; ++q)
+        if (kFull || q < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+      x[j] = mul(x[j], rdiag[j]);
+    }
+  }
+}
+
 template <typename T>
 __device__ void cta_update(T *__restrict__ D, int ldd, int r0, int mrows, int c0, int ncols,
                            const T *__restrict__ L, int ldl, int jb, const T (*__restrict__ blk)[kBlkLd],
@@ -497,6 +523,7 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
   auto Ls = reinterpret_cast<T(*)[64]>(b_smem + sizeof(T) * kBPanel * kBlkLd);
   auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (kBlkLd + 64));
   __shared__ T xrow[2][kBPanel];   // [0]: old row a, [1]: the pivot row
+  __shared__ __align__(16) T urow[kBPanel];  // the pivot row right of column j
   __shared__ T rdiag[kBPanel];     // reciprocals of U's diagonal block
   __shared__ int perm[kBThreads];  // P: row i of P q is row perm[i] of q
   __shared__ int pos[kBThreads];   // panel-local composite of the swaps
@@ -559,7 +586,10 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
       }
       if (t == p) {
 #pragma unroll
-        for (int c = 0; c < kBPanel; ++c) xrow[1][c] = r[c];
+        for (int c = 0; c < kBPanel; ++c) {
+          xrow[1][c] = r[c];
+          urow[c] = (c > j && c < jb) ? r[c] : elem<T>::zero();  // the update's row, masked
+        }
       }
       if (t == 0) {
         piv[j] = p;
@@ -590,11 +620,18 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         for (int c = 0; c < kBPanel; ++c)
           if (c == j) l = r[c];
         l = abs1(pv) >= sfmin ? mul(l, divide(elem<T>::one(), pv)) : divide(l, pv);
+        // unconditional rank-1 update against the masked row (zero at and left
+        // of column j; |l| <= 1 under partial pivoting), then column j = l
 #pragma unroll
-        for (int c = 0; c < kBPanel; ++c) {
-          if (c == j) r[c] = l;
-          else if (c > j && c < jb) r[c] = sub(r[c], mul(l, xrow[1][c]));
+        for (int c = 0; c < kBPanel; c += 4) {
+          T u[4];
+          lds4(&urow[c], u);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) r[c + i] = sub(r[c + i], mul(l, u[i]));
         }
+#pragma unroll
+        for (int c = 0; c < kBPanel; ++c)
+          if (c == j) r[c] = l;
       }
     }
     // panel back to memory; L11 to shared memory
@@ -635,11 +672,8 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         }
       }
       if (c >= k + jb) {
-#pragma unroll
-        for (int j = 0; j < kBPanel; ++j)
-#pragma unroll
-          for (int q = 0; q < kBPanel; ++q)
-            if (q < j && j < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+        if (jb == kBPanel) trsv_lower_unit<T, true>(x, diag, jb);
+        else trsv_lower_unit<T, false>(x, diag, jb);
       }
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
@@ -688,11 +722,8 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
       T x[kBPanel];
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? col[k + j] : elem<T>::zero();
-#pragma unroll
-      for (int j = 0; j < kBPanel; ++j)
-#pragma unroll
-        for (int q = 0; q < kBPanel; ++q)
-          if (q < j && j < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
+      if (jb == kBPanel) trsv_lower_unit<T, true>(x, diag, jb);
+      else trsv_lower_unit<T, false>(x, diag, jb);
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
         if (j < jb) {
@@ -718,15 +749,8 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
       T x[kBPanel];
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? col[k + j] : elem<T>::zero();
-#pragma unroll
-      for (int j = kBPanel - 1; j >= 0; --j) {
-        if (j < jb) {
-#pragma unroll
-          for (int q = 0; q < kBPanel; ++q)
-            if (q > j && q < jb) x[j] = sub(x[j], mul(diag[j][q], x[q]));
-          x[j] = mul(x[j], rdiag[j]);
-        }
-      }
+      if (jb == kBPanel) trsv_upper<T, true>(x, diag, rdiag, jb);
+      else trsv_upper<T, false>(x, diag, rdiag, jb);
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
         if (j < jb) {
