@@ -22,6 +22,7 @@
 #include <cfloat>
 #include <vector>
 
+#include "dmma.cuh"
 #include "expm_common.cuh"
 
 namespace clm {
@@ -363,6 +364,163 @@ __global__ void __launch_bounds__(256)
       o.C[(std::size_t)c * o.ldc + r] = v;
     }
   }
+}
+
+// ---- grouped FP64 GEMM on the tensor cores (DMMA m16n8k8): the same tile
+// numbering, operand policies and epilogue as g_gemm_kernel, with a 64 x 64
+// output tile per CTA of four warps (32 x 32 each), k-slices of 16 staged by
+// cp.async in a three-stage ring. A second product (A2 B2) continues the same
+// k loop into the same accumulators.
+constexpr int kDStages = 3;
+constexpr int kDSA = kGTile + 4, kDSB = 16 + 4;  // 4 mod 16 doubles: conflict-free fragments
+constexpr std::size_t kDSmem = sizeof(double) * kDStages * (16 * kDSA + kGTile * kDSB);
+
+template <typename Item, typename Ops, bool kSquare>
+__global__ void __launch_bounds__(128)
+    g_dgemm_kernel(const Item *__restrict__ items, const BPlan *__restrict__ plans,
+                   const int *__restrict__ tile_prefix, int batch, int phase, int ksq) {
+  constexpr int BK = 16, MI = 2, NI = 4;
+  const int tile = blockIdx.x;
+  int lo = 0, hi = batch - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_prefix[mid] <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const Item it = items[lo];
+  const BPlan pl = plans[lo];
+  GOps<double> o;
+  if constexpr (kSquare) {
+    if (!Ops::square(it, pl, blockIdx.y, ksq, o)) return;
+  } else {
+    if (!Ops::pade(it, pl, phase, blockIdx.y, o)) return;
+  }
+  const int n = it.n;
+  const int tn = (n + kGTile - 1) / kGTile;
+  const int local = tile - tile_prefix[lo];
+  const int m0 = (local % tn) * kGTile, n0 = (local / tn) * kGTile;
+
+  extern __shared__ __align__(16) double dsm[];
+  double *sA = dsm;                                 // [stage][k][m]
+  double *sB = dsm + kDStages * BK * kDSA;          // [stage][n][k]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp & 1) * 32, wn0 = (warp >> 1) * 32;
+  const int KT = (n + BK - 1) / BK;
+  const int total = (o.A2 ? 2 : 1) * KT;
+
+  auto load_tile = [&](int stage, int step) {
+    const bool second = step >= KT;
+    const double *Am = second ? o.A2 : o.A;
+    const double *Bm = second ? o.B2 : o.B;
+    const int lda = second ? o.lda2 : o.lda, ldb = second ? o.ldb2 : o.ldb;
+    const int k0 = (second ? step - KT : step) * BK;
+    double *a = sA + stage * BK * kDSA;
+    double *b = sB + stage * kGTile * kDSB;
+#pragma unroll
+    for (int c = tid; c < BK * kGTile; c += 128) {
+      const int kk = c / kGTile, mm = c % kGTile;
+      const int gm = m0 + mm, gk = k0 + kk;
+      const int bytes = (gk < n && gm < n) ? 8 : 0;
+      cp_async8(a + kk * kDSA + mm, bytes ? Am + (std::size_t)gk * lda + gm : Am, bytes);
+    }
+#pragma unroll
+    for (int c = tid; c < kGTile * BK; c += 128) {
+      const int nn = c / BK, kk = c % BK;
+      const int gn = n0 + nn, gk = k0 + kk;
+      const int bytes = (gn < n && gk < n) ? 8 : 0;
+      cp_async8(b + nn * kDSB + kk, bytes ? Bm + (std::size_t)gn * ldb + gk : Bm, bytes);
+    }
+  };
+
+  double acc[MI][NI][4];
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+#pragma unroll
+  for (int st = 0; st < kDStages - 1; ++st) {
+    if (st < total) load_tile(st, st);
+    cp_commit();
+  }
+  for (int step = 0; step < total; ++step) {
+    cp_wait<kDStages - 2>();
+    __syncthreads();
+    {
+      const int nx = step + kDStages - 1;
+      if (nx < total) load_tile(nx % kDStages, nx);
+      cp_commit();
+    }
+    const double *a = sA + (step % kDStages) * BK * kDSA;
+    const double *b = sB + (step % kDStages) * kGTile * kDSB;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      double af[MI][4], bf[NI][2];
+#pragma unroll
+      for (int i = 0; i < MI; ++i) {
+        const int m = wm0 + i * 16 + g;
+        af[i][0] = a[(kk + t) * kDSA + m];
+        af[i][1] = a[(kk + t) * kDSA + m + 8];
+        af[i][2] = a[(kk + t + 4) * kDSA + m];
+        af[i][3] = a[(kk + t + 4) * kDSA + m + 8];
+      }
+#pragma unroll
+      for (int j = 0; j < NI; ++j) {
+        const int nn = wn0 + j * 8 + g;
+        bf[j][0] = b[nn * kDSB + kk + t];
+        bf[j][1] = b[nn * kDSB + kk + t + 4];
+      }
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NI; ++j) dmma16x8x8(acc[i][j], af[i], bf[j]);
+    }
+  }
+  cp_wait<0>();
+  // epilogue: all old C values of a row block in flight before any store
+#pragma unroll
+  for (int i = 0; i < MI; ++i) {
+    double old[NI][4];
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
+        const int c = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        old[j][r] = (o.acc && m < n && c < n) ? o.C[(std::size_t)c * o.ldc + m] : 0.0;
+      }
+#pragma unroll
+    for (int j = 0; j < NI; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int m = m0 + wm0 + i * 16 + g + ((r & 2) ? 8 : 0);
+        const int c = n0 + wn0 + j * 8 + 2 * t + (r & 1);
+        if (m < n && c < n) o.C[(std::size_t)c * o.ldc + m] = o.neg ? old[j][r] - acc[i][j][r]
+                                                                    : old[j][r] + acc[i][j][r];
+      }
+  }
+}
+
+// Launch a grouped product phase on the engine of its element type: DMMA
+// tiles for double, the SIMT kernel otherwise.
+template <typename Item, typename U, typename Ops, bool kSquare>
+cudaError_t launch_group(cudaStream_t st, dim3 grid, const Item *items, const BPlan *plans,
+                         const int *prefix, int count, int phase, int k) {
+  if constexpr (std::is_same<U, double>::value) {
+    static bool configured = false;
+    auto kern = g_dgemm_kernel<Item, Ops, kSquare>;
+    if (!configured) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmem);
+      if (e != cudaSuccess) return e;
+      configured = true;
+    }
+    kern<<<grid, 128, kDSmem, st>>>(items, plans, prefix, count, phase, k);
+  } else {
+    g_gemm_kernel<Item, U, Ops, kSquare><<<grid, 256, 0, st>>>(items, plans, prefix, count, phase, k);
+  }
+  return launched();
 }
 
 // ---- LU with partial pivoting of q and the solve q R = p: one CTA per matrix
@@ -909,9 +1067,8 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
   const dim3 ew((unsigned)count, (unsigned)((max_n * max_n + kEwChunk - 1) / kEwChunk));
   auto gemm = [&](int phase, int ysub) -> cudaError_t {
     return timed_group(st, phase_flops(ns, pls, phase, 0), [&] {
-      g_gemm_kernel<BItem<C, W>, C, ExpmOps, false><<<dim3(tiles, ysub), 256, 0, st>>>(
-          d_items, d_plans, d_prefix, count, phase, 0);
-      return launched();
+      return launch_group<BItem<C, W>, C, ExpmOps, false>(st, dim3(tiles, ysub), d_items, d_plans, d_prefix,
+                                                           count, phase, 0);
     });
   };
   b_scale_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
@@ -937,9 +1094,8 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
     if ((e = launched()) != cudaSuccess) return e;
     for (int k = 1; k <= max_s; ++k) {
       e = timed_group(st, phase_flops(ns, pls, kPhSq, k), [&] {
-        g_gemm_kernel<BItem<C, W>, W, ExpmOps, true><<<tiles, 256, 0, st>>>(d_items, d_plans, d_prefix,
-                                                                            count, kPhSq, k);
-        return launched();
+        return launch_group<BItem<C, W>, W, ExpmOps, true>(st, dim3(tiles, 1), d_items, d_plans, d_prefix,
+                                                           count, kPhSq, k);
       });
       if (e != cudaSuccess) return e;
     }
@@ -1364,9 +1520,8 @@ cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::ty
   };
   auto gemm = [&](int phase, int ysub) -> cudaError_t {
     return timed_group(st, vflops(phase, 0), [&] {
-      g_gemm_kernel<Item, C, VjpOps, false><<<dim3(tiles, ysub), 256, 0, st>>>(d_items, d_plans, d_prefix,
-                                                                               count, phase, 0);
-      return launched();
+      return launch_group<Item, C, VjpOps, false>(st, dim3(tiles, ysub), d_items, d_plans, d_prefix, count,
+                                                  phase, 0);
     });
   };
   const std::size_t lu_smem = sizeof(C) * (kBPanel * (kBlkLd + 64) + kBPanel * (kBPanel + 1));
@@ -1397,9 +1552,8 @@ cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::ty
     if ((e = launched()) != cudaSuccess) return e;
     for (int k = 1; k <= max_s; ++k) {
       e = timed_group(st, vflops(kPhSq, k), [&] {
-        g_gemm_kernel<Item, W, VjpOps, true><<<dim3(tiles, 2), 256, 0, st>>>(d_items, d_plans, d_prefix,
-                                                                             count, kPhSq, k);
-        return launched();
+        return launch_group<Item, W, VjpOps, true>(st, dim3(tiles, 2), d_items, d_plans, d_prefix, count,
+                                                   kPhSq, k);
       });
       if (e != cudaSuccess) return e;
     }
