@@ -19,7 +19,9 @@
 // CTA of 256 threads in which thread i owns row i (pivot search, swaps,
 // rank-updates) or column i (swap gathers, triangular solves of the diagonal
 // blocks), with panels of 32 columns.
+#include <algorithm>
 #include <cfloat>
+#include <type_traits>
 #include <vector>
 
 #include "dmma.cuh"
@@ -528,16 +530,19 @@ cudaError_t launch_group(cudaStream_t st, dim3 grid, const Item *items, const BP
 // before the first store, so the L2 latency is paid once per eight elements.
 constexpr int kBU = 8;
 
-template <typename T> struct BLuOcc { static constexpr int kMinBlocks = 1; };
-template <> struct BLuOcc<float> { static constexpr int kMinBlocks = 2; };
+// CTAs per SM the LU kernel is compiled for: FP32 rows fit 128 registers
+// (two 256-thread CTAs), FP64 rows take up to 255 at 256 threads.
+template <typename T, int NT> struct BLuOcc {
+  static constexpr int kMinBlocks = (sizeof(T) == 4 ? 2 : 1) * (256 / NT);
+};
 
 // D(r0 + i, c) -= sum_{j < jb} L(i, j) blk[j][c] for i < mrows, c in [c0, c0 + ncols),
 // with L(i, j) = L[j * ldl + r0 + i] (column-major, global). All threads take
-// part: 64 x 64 output blocks, thread (tr, tc) = (t % 16, t / 16) owns rows
-// tr + 16 a and columns 4 tc + b (a, b < 4) of a block; L's 64 rows of a block
-// are staged in shared memory. c0 is a multiple of 4 and blk rows are padded
-// by 64 columns, so the 4-wide shared loads never leave their row.
-constexpr int kBlkLd = kBThreads + 64;
+// part: 64 x (NT / 4) output blocks, thread (tr, tc) = (t % 16, t / 16) owns
+// rows tr + 16 a and columns 4 tc + b (a, b < 4) of a block; L's 64 rows of a
+// block are staged in shared memory. c0 is a multiple of 4 and blk rows are
+// padded by 64 columns, so the 4-wide shared loads never leave their row.
+template <int NT> constexpr int blk_ld() { return NT + 64; }
 
 template <typename T>
 __device__ __forceinline__ void lds4(const T *src, T (&dst)[4]) {
@@ -583,25 +588,36 @@ __device__ __forceinline__ void trsv_upper(T (&x)[kBPanel], const T (*diag)[kBPa
   }
 }
 
-template <typename T>
+template <typename T, int NT>
 __device__ void cta_update(T *__restrict__ D, int ldd, int r0, int mrows, int c0, int ncols,
-                           const T *__restrict__ L, int ldl, int jb, const T (*__restrict__ blk)[kBlkLd],
-                           T (*__restrict__ Ls)[64]) {
+                           const T *__restrict__ L, int ldl, int jb,
+                           const T (*__restrict__ blk)[blk_ld<NT>()], T (*__restrict__ Ls)[64]) {
+  constexpr int CB = NT / 4;  // columns per block
   const int t = threadIdx.x, tr = t & 15, tc = t >> 4;
   for (int rb = 0; rb < mrows; rb += 64) {
     __syncthreads();  // Ls is rewritten
-    for (int e = t; e < 64 * kBPanel; e += kBThreads) {
+    for (int e = t; e < 64 * kBPanel; e += NT) {
       const int i = e & 63, j = e >> 6;
       Ls[j][i] = (j < jb && rb + i < mrows) ? L[(std::size_t)j * ldl + r0 + rb + i] : elem<T>::zero();
     }
     __syncthreads();
-    for (int cb = 0; cb < ncols; cb += 64) {
+    for (int cb = 0; cb < ncols; cb += CB) {
       T acc[4][4];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = elem<T>::zero();
       const int cc = c0 + cb + 4 * tc;
+      // the block's old values are requested before the k loop, so their
+      // latency overlaps the products
+      T old[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int i = rb + tr + 16 * a, c = cc + b;
+          old[a][b] = (i < mrows && c < c0 + ncols) ? D[(std::size_t)c * ldd + r0 + i] : elem<T>::zero();
+        }
 #pragma unroll 4
       for (int j = 0; j < jb; ++j) {
         T av[4], bv[4];
@@ -613,14 +629,6 @@ __device__ void cta_update(T *__restrict__ D, int ldd, int r0, int mrows, int c0
 #pragma unroll
           for (int b = 0; b < 4; ++b) acc[a][b] = fmac(av[a], bv[b], acc[a][b]);
       }
-      T old[4][4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int i = rb + tr + 16 * a, c = cc + b;
-          old[a][b] = (i < mrows && c < c0 + ncols) ? D[(std::size_t)c * ldd + r0 + i] : elem<T>::zero();
-        }
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -658,8 +666,8 @@ struct ExpmLu {
 
 // kFactor: LU with partial pivoting of Q, then the solve; otherwise the solve
 // alone with factors and permutation from an earlier kFactor launch.
-template <typename Item, typename T, typename Lu, bool kFactor>
-__global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
+template <typename Item, typename T, typename Lu, bool kFactor, int NT>
+__global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
     g_lu_kernel(const Item *__restrict__ items, const BPlan *__restrict__ plans, int *__restrict__ info,
                 int mode) {
   using R = typename elem<T>::real;
@@ -673,21 +681,22 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
   const int ldd = lo.ldd;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
 
-  // dynamic: blk[kBPanel][kBlkLd] (per-column staging, U12 rows, solved
+  // dynamic: blk[kBPanel][NT + 64] (per-column staging, U12 rows, solved
   // right-hand-side block rows), Ls[kBPanel][64] (staged L rows of the block
   // updates), then diag[kBPanel][kBPanel + 1]
   extern __shared__ __align__(16) unsigned char b_smem[];
-  auto blk = reinterpret_cast<T(*)[kBlkLd]>(b_smem);
-  auto Ls = reinterpret_cast<T(*)[64]>(b_smem + sizeof(T) * kBPanel * kBlkLd);
-  auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (kBlkLd + 64));
+  constexpr int LD = blk_ld<NT>();
+  auto blk = reinterpret_cast<T(*)[LD]>(b_smem);
+  auto Ls = reinterpret_cast<T(*)[64]>(b_smem + sizeof(T) * kBPanel * LD);
+  auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (LD + 64));
   __shared__ T xrow[2][kBPanel];   // [0]: old row a, [1]: the pivot row
   __shared__ __align__(16) T urow[kBPanel];  // the pivot row right of column j
   __shared__ T rdiag[kBPanel];     // reciprocals of U's diagonal block
-  __shared__ int perm[kBThreads];  // P: row i of P q is row perm[i] of q
-  __shared__ int pos[kBThreads];   // panel-local composite of the swaps
+  __shared__ int perm[NT];  // P: row i of P q is row perm[i] of q
+  __shared__ int pos[NT];   // panel-local composite of the swaps
   __shared__ int piv[kBPanel];
-  __shared__ double red_v[kBThreads / 32];
-  __shared__ int red_i[kBThreads / 32];
+  __shared__ double red_v[NT / 32];
+  __shared__ int red_i[NT / 32];
   __shared__ int first_zero;
 
   if (t < n) perm[t] = kFactor ? t : lo.perm[t];
@@ -730,7 +739,7 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
       double bv = red_v[0];
       int p = red_i[0];
 #pragma unroll
-      for (int w = 1; w < kBThreads / 32; ++w) {
+      for (int w = 1; w < NT / 32; ++w) {
         const double wv = red_v[w];
         const int wi = red_i[w];
         if (wv > bv || (wv == bv && wi < p)) {
@@ -842,7 +851,7 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
     }
     __syncthreads();
     // trailing update A22 -= L21 U12 by the whole CTA
-    cta_update(Q, n, k + jb, n - k - jb, k + jb, n - k - jb, Q + (std::size_t)k * n, n, jb, blk, Ls);
+    cta_update<T, NT>(Q, n, k + jb, n - k - jb, k + jb, n - k - jb, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
   if (kFactor) {
     if (t == 0) {
@@ -870,7 +879,7 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
   // forward, unit lower
   for (int k = 0; k < n; k += kBPanel) {
     const int jb = min(kBPanel, n - k);
-    for (int e = t; e < jb * jb; e += kBThreads) {
+    for (int e = t; e < jb * jb; e += NT) {
       const int j = e / jb, q = e - j * jb;  // row j, column q of the block
       diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
     }
@@ -890,12 +899,12 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         }
     }
     __syncthreads();
-    cta_update(D, ldd, k + jb, n - k - jb, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
+    cta_update<T, NT>(D, ldd, k + jb, n - k - jb, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
   // backward, non-unit upper
   for (int k = ((n - 1) / kBPanel) * kBPanel; k >= 0; k -= kBPanel) {
     const int jb = min(kBPanel, n - k);
-    for (int e = t; e < jb * jb; e += kBThreads) {
+    for (int e = t; e < jb * jb; e += NT) {
       const int j = e / jb, q = e - j * jb;
       diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
     }
@@ -917,8 +926,37 @@ __global__ void __launch_bounds__(kBThreads, BLuOcc<T>::kMinBlocks)
         }
     }
     __syncthreads();
-    cta_update(D, ldd, 0, k, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
+    cta_update<T, NT>(D, ldd, 0, k, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
+}
+
+template <typename T, int NT> constexpr std::size_t lu_smem_bytes() {
+  return sizeof(T) * (kBPanel * (blk_ld<NT>() + 64) + kBPanel * (kBPanel + 1));
+}
+
+// The LU kernel over a batch sorted by n (ascending), one launch per size
+// class: 64-thread CTAs for n <= 64, 128 for n <= 128, 256 above, so small
+// matrices pack more CTAs per SM.
+template <typename Item, typename T, typename Lu, bool kFactor>
+cudaError_t launch_lu(cudaStream_t st, const Item *items, const BPlan *plans, int *info, int mode,
+                      const std::vector<int> &ns) {
+  const int count = (int)ns.size();
+  const int b64 = (int)(std::upper_bound(ns.begin(), ns.end(), 64) - ns.begin());
+  const int b128 = (int)(std::upper_bound(ns.begin(), ns.end(), 128) - ns.begin());
+  auto one = [&](auto nt_tag, int from, int to) -> cudaError_t {
+    constexpr int NT = decltype(nt_tag)::value;
+    if (to <= from) return cudaSuccess;
+    auto kern = g_lu_kernel<Item, T, Lu, kFactor, NT>;
+    constexpr std::size_t smem = lu_smem_bytes<T, NT>();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<to - from, NT, smem, st>>>(items + from, plans + from, info, mode);
+    return launched();
+  };
+  cudaError_t e;
+  if ((e = one(std::integral_constant<int, 64>{}, 0, b64)) != cudaSuccess) return e;
+  if ((e = one(std::integral_constant<int, 128>{}, b64, b128)) != cudaSuccess) return e;
+  return one(std::integral_constant<int, 256>{}, b128, count);
 }
 
 // ---- precision conversion between the caller's buffers and FP64 copies ----
@@ -1081,14 +1119,8 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
   if ((e = gemm(kPhU, 1)) != cudaSuccess) return e;
   b_split_kernel<C, W><<<ew, 256, 0, st>>>(d_items);
   if ((e = launched()) != cudaSuccess) return e;
-  {
-    const std::size_t smem = sizeof(C) * (kBPanel * (kBlkLd + 64) + kBPanel * (kBPanel + 1));
-    auto kern = g_lu_kernel<BItem<C, W>, C, ExpmLu, true>;
-    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-      return e;
-    kern<<<count, kBThreads, smem, st>>>(d_items, d_plans, d_info, 0);
-    if ((e = launched()) != cudaSuccess) return e;
-  }
+  if ((e = launch_lu<BItem<C, W>, C, ExpmLu, true>(st, d_items, d_plans, d_info, 0, ns)) != cudaSuccess)
+    return e;
   if (max_s > 0) {
     b_widen_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
     if ((e = launched()) != cudaSuccess) return e;
@@ -1181,7 +1213,11 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
   std::vector<int> lo_prefix(1, 0), hi_prefix(1, 0), lo_n, hi_n;
   std::vector<BConv> cin, cout;
   int lo_max_n = 0, hi_max_n = 0, lo_max_s = 0, hi_max_s = 0;
-  for (int i = 0; i < batch; ++i) {
+  // matrices in ascending n: the LU runs one launch per size class
+  std::vector<int> order(batch);
+  for (int i = 0; i < batch; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return h_n[x] < h_n[y]; });
+  for (int i : order) {
     const calamanExpmPlan_t &p = plans[i];
     const BPlan bp{p.m, p.s, pade_num_powers(p.m), 0};
     const int n = h_n[i];
@@ -1524,13 +1560,6 @@ cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::ty
                                                   phase, 0);
     });
   };
-  const std::size_t lu_smem = sizeof(C) * (kBPanel * (kBlkLd + 64) + kBPanel * (kBPanel + 1));
-  auto lu_f = g_lu_kernel<Item, C, VjpLu, true>;
-  auto lu_s = g_lu_kernel<Item, C, VjpLu, false>;
-  if ((e = cudaFuncSetAttribute(lu_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem)) != cudaSuccess)
-    return e;
-  if ((e = cudaFuncSetAttribute(lu_s, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem)) != cudaSuccess)
-    return e;
 
   v_prep_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
   if ((e = launched()) != cudaSuccess) return e;
@@ -1542,11 +1571,9 @@ cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::ty
   if ((e = gemm(kPhU, 2)) != cudaSuccess) return e;
   v_split_kernel<C, W><<<ew, 256, 0, st>>>(d_items);
   if ((e = launched()) != cudaSuccess) return e;
-  lu_f<<<count, kBThreads, lu_smem, st>>>(d_items, d_plans, d_info, 0);
-  if ((e = launched()) != cudaSuccess) return e;
+  if ((e = launch_lu<Item, C, VjpLu, true>(st, d_items, d_plans, d_info, 0, ns)) != cudaSuccess) return e;
   if ((e = gemm(kPhRhs, 1)) != cudaSuccess) return e;
-  lu_s<<<count, kBThreads, lu_smem, st>>>(d_items, d_plans, d_info, 1);
-  if ((e = launched()) != cudaSuccess) return e;
+  if ((e = launch_lu<Item, C, VjpLu, false>(st, d_items, d_plans, d_info, 1, ns)) != cudaSuccess) return e;
   if (max_s > 0) {
     v_widen_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
     if ((e = launched()) != cudaSuccess) return e;
@@ -1673,7 +1700,11 @@ calamanStatus_t vjp_batched_api(calamanHandle_t blas, calamanStream_t stream, in
   std::vector<int> lo_prefix(1, 0), hi_prefix(1, 0), lo_n, hi_n;
   std::vector<BConv> cin, cout;
   int lo_max_n = 0, hi_max_n = 0, lo_max_s = 0, hi_max_s = 0;
-  for (int i = 0; i < batch; ++i) {
+  // matrices in ascending n: the LU runs one launch per size class
+  std::vector<int> order(batch);
+  for (int i = 0; i < batch; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return h_n[x] < h_n[y]; });
+  for (int i : order) {
     const calamanExpmPlan_t &p = plans[i];
     const BPlan bp{p.m, p.s, pade_num_powers(p.m), 0};
     const int n = h_n[i];

@@ -114,6 +114,70 @@ Status expm(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int n, co
     return calaman_expm_z(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
 }
 
+// ---- expm_vjp: the adjoint of expm (new entry, no reference counterpart) -------
+template <typename T> Status expm_vjp_bufferSize(SolverHandle h, int n, std::size_t *bytes) {
+  if constexpr (std::is_same_v<T, float>) return calaman_expm_vjp_bufferSize_s(h, n, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_expm_vjp_bufferSize_d(h, n, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_expm_vjp_bufferSize_c(h, n, bytes);
+  else return calaman_expm_vjp_bufferSize_z(h, n, bytes);
+}
+// d_gradA = L(A^H, G); d_expA may be nullptr
+template <typename T>
+Status expm_vjp(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int n, const T *d_A, int lda,
+                const T *d_G, int ldg, T *d_gradA, int ldga, T *d_expA, int lde, void *d_work,
+                std::size_t lwork_bytes, int *d_info, ExpmPlan *plan = nullptr) {
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_expm_vjp_s(blas, solver, stream, n, d_A, lda, d_G, ldg, d_gradA, ldga, d_expA, lde, d_work,
+                              lwork_bytes, d_info, plan);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_expm_vjp_d(blas, solver, stream, n, d_A, lda, d_G, ldg, d_gradA, ldga, d_expA, lde, d_work,
+                              lwork_bytes, d_info, plan);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_expm_vjp_c(blas, solver, stream, n, d_A, lda, d_G, ldg, d_gradA, ldga, d_expA, lde, d_work,
+                              lwork_bytes, d_info, plan);
+  else
+    return calaman_expm_vjp_z(blas, solver, stream, n, d_A, lda, d_G, ldg, d_gradA, ldga, d_expA, lde, d_work,
+                              lwork_bytes, d_info, plan);
+}
+
+// ---- expm_batched / expm_vjp_batched (new entries): float and double ----------
+template <typename T> Status expm_batched_bufferSize(SolverHandle h, int batch, const int *h_n, std::size_t *bytes) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "expm_batched: float or double");
+  if constexpr (std::is_same_v<T, float>) return calaman_expm_batched_bufferSize_s(h, batch, h_n, bytes);
+  else return calaman_expm_batched_bufferSize_d(h, batch, h_n, bytes);
+}
+template <typename T>
+Status expm_batched(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int batch, const int *h_n,
+                    const T *const *h_A, const int *h_lda, T *const *h_expA, const int *h_lde, void *d_work,
+                    std::size_t lwork_bytes, int *d_info, ExpmPlan *h_plans = nullptr) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "expm_batched: float or double");
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_expm_batched_s(blas, solver, stream, batch, h_n, h_A, h_lda, h_expA, h_lde, d_work,
+                                  lwork_bytes, d_info, h_plans);
+  else
+    return calaman_expm_batched_d(blas, solver, stream, batch, h_n, h_A, h_lda, h_expA, h_lde, d_work,
+                                  lwork_bytes, d_info, h_plans);
+}
+template <typename T>
+Status expm_vjp_batched_bufferSize(SolverHandle h, int batch, const int *h_n, std::size_t *bytes) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "expm_vjp_batched: float or double");
+  if constexpr (std::is_same_v<T, float>) return calaman_expm_vjp_batched_bufferSize_s(h, batch, h_n, bytes);
+  else return calaman_expm_vjp_batched_bufferSize_d(h, batch, h_n, bytes);
+}
+template <typename T>
+Status expm_vjp_batched(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int batch, const int *h_n,
+                        const T *const *h_A, const int *h_lda, const T *const *h_G, const int *h_ldg,
+                        T *const *h_gradA, const int *h_ldga, T *const *h_expA, const int *h_lde, void *d_work,
+                        std::size_t lwork_bytes, int *d_info, ExpmPlan *h_plans = nullptr) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "expm_vjp_batched: float or double");
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_expm_vjp_batched_s(blas, solver, stream, batch, h_n, h_A, h_lda, h_G, h_ldg, h_gradA, h_ldga,
+                                      h_expA, h_lde, d_work, lwork_bytes, d_info, h_plans);
+  else
+    return calaman_expm_vjp_batched_d(blas, solver, stream, batch, h_n, h_A, h_lda, h_G, h_ldg, h_gradA, h_ldga,
+                                      h_expA, h_lde, d_work, lwork_bytes, d_info, h_plans);
+}
+
 // ---- pade (src/expm/pade.cppm:77-191) ------------------------------------------
 template <typename T>
 Status pade(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int m, int n, const T *d_A,

@@ -58,6 +58,17 @@ int main() {
   const calaman::Status st = calaman::horner<double>(nullptr, 0, c.data(), 4, a.data(), n, p.data(), n,
                                                      work.data(), 4096);
   CHECK(st.code == CALAMAN_STATUS_NOT_INITIALIZED && std::string(st.name()) == "NOT_INITIALIZED");
+  // the new entries: size queries and argument rejection
+  CHECK(calaman::expm_vjp_bufferSize<double>(nullptr, 8, &bytes).ok() && bytes > 0);
+  std::vector<double> g(n * n, 0.5), d(n * n, 0.0);
+  CHECK(calaman::expm_vjp<double>(nullptr, nullptr, nullptr, 0, a.data(), n, g.data(), n, d.data(), n, nullptr,
+                                  n, work.data(), 4096, info) == invalid);
+  const int ns[3] = {4, 16, 300};
+  CHECK(calaman::expm_batched_bufferSize<float>(nullptr, 2, ns, &bytes).ok() && bytes > 0);
+  CHECK(calaman::expm_batched_bufferSize<float>(nullptr, 3, ns, &bytes).code == CALAMAN_STATUS_NOT_SUPPORTED);
+  CHECK(calaman::expm_vjp_batched_bufferSize<double>(nullptr, 2, ns, &bytes).ok() && bytes > 0);
+  CHECK(calaman::expm_batched<double>(nullptr, nullptr, nullptr, 0, ns, nullptr, nullptr, nullptr, nullptr,
+                                      nullptr, 0, nullptr).ok());  // an empty batch is a no-op
   std::printf("header_check ok\n");
   return 0;
 }
