@@ -1187,6 +1187,45 @@ std::size_t lu_scratch_bytes(int n) {
   return L.used;
 }
 
+// Look-ahead resources of the calling host thread on the current device: a
+// high-priority auxiliary stream on which the next panel is factored while the
+// caller's stream runs the wide trailing update, and the two events that order
+// them.
+struct LookAhead {
+  int device = -1;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ready = nullptr, done = nullptr;
+};
+thread_local LookAhead tl_lookahead;
+
+cudaError_t lookahead(LookAhead *&out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  LookAhead &la = tl_lookahead;
+  if (la.device != dev) {
+    if (la.aux) {  // a different device than last time: release the old set
+      cudaStreamDestroy(la.aux);
+      cudaEventDestroy(la.ready);
+      cudaEventDestroy(la.done);
+      la = LookAhead{};
+    }
+    int lo = 0, hi = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&lo, &hi)) != cudaSuccess) return e;
+    if ((e = cudaStreamCreateWithPriority(&la.aux, cudaStreamNonBlocking, hi)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&la.ready, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&la.done, cudaEventDisableTiming)) != cudaSuccess) return e;
+    la.device = dev;
+  }
+  out = &la;
+  return cudaSuccess;
+}
+
+// Blocked right-looking factorisation with a one-panel look-ahead: after the
+// swaps and U12 solve of panel k, the next panel's columns are updated first
+// (a narrow GEMM); panel k+1 is then factored on the auxiliary stream while
+// the caller's stream updates the columns beyond it, and panel k+1's swaps wait
+// for both.
 template <typename T>
 cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info_dev) {
   if (n < 1) return cudaSuccess;
@@ -1202,11 +1241,16 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
   if ((e = cudaFuncSetAttribute(swap_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)swap_smem)) !=
       cudaSuccess)
     return e;
+  LookAhead *la = nullptr;  // only matrices of more than one panel need it
+  if (n > kbn && (e = lookahead(la)) != cudaSuccess) return e;
+  auto panel = [&](cudaStream_t st, int k, int kb) {
+    return kb_cta > 0 ? launch_cta_panel<T>(st, n, A, lda, k, kb, sc, info_dev)
+                      : launch_panel<T>(st, n, A, lda, k, kb, sc, info_dev);
+  };
+  if ((e = panel(s, 0, kbn < n ? kbn : n)) != cudaSuccess) return e;
   for (int k = 0; k < n; k += kbn) {
     const int kb = (k + kbn < n) ? kbn : n - k;
-    e = kb_cta > 0 ? launch_cta_panel<T>(s, n, A, lda, k, kb, sc, info_dev)
-                   : launch_panel<T>(s, n, A, lda, k, kb, sc, info_dev);
-    if (e != cudaSuccess) return e;
+    if (k > 0 && (e = cudaStreamWaitEvent(s, la->done, 0)) != cudaSuccess) return e;  // panel k
     const int others = n - kb;
     if (others > 0) {
       const int warps = 8;
@@ -1216,10 +1260,22 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
     }
     const int rest = n - (k + kb);
     if (rest > 0) {
-      e = gemm_nn<T>(s, rest, rest, kb, -1.0, A + (std::size_t)k * lda + (k + kb), lda,
-                     A + (std::size_t)(k + kb) * lda + k, lda, 1.0,
+      const int kb2 = rest < kbn ? rest : kbn;  // the next panel's width
+      const T *L21 = A + (std::size_t)k * lda + (k + kb);
+      // next panel's columns first
+      e = gemm_nn<T>(s, rest, kb2, kb, -1.0, L21, lda, A + (std::size_t)(k + kb) * lda + k, lda, 1.0,
                      A + (std::size_t)(k + kb) * lda + (k + kb), lda);
       if (e != cudaSuccess) return e;
+      if ((e = cudaEventRecord(la->ready, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(la->aux, la->ready, 0)) != cudaSuccess) return e;
+      if ((e = panel(la->aux, k + kb, kb2)) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(la->done, la->aux)) != cudaSuccess) return e;
+      // the wide update, concurrent with that panel
+      if (rest > kb2) {
+        e = gemm_nn<T>(s, rest, rest - kb2, kb, -1.0, L21, lda, A + (std::size_t)(k + kb + kb2) * lda + k, lda,
+                       1.0, A + (std::size_t)(k + kb + kb2) * lda + (k + kb), lda);
+        if (e != cudaSuccess) return e;
+      }
     }
   }
   return cudaSuccess;
