@@ -695,8 +695,8 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
   __shared__ int perm[NT];  // P: row i of P q is row perm[i] of q
   __shared__ int pos[NT];   // panel-local composite of the swaps
   __shared__ int piv[kBPanel];
-  __shared__ double red_v[NT / 32];
-  __shared__ int red_i[NT / 32];
+  __shared__ unsigned long long red_key[NT / 32];
+  __shared__ int red_idx[NT / 32];
   __shared__ int first_zero;
 
   if (t < n) perm[t] = kFactor ? t : lo.perm[t];
@@ -720,33 +720,10 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
       for (int c = 0; c < kBPanel; ++c)
         if (c == j) rj = r[c];
       // pivot: largest |Re| + |Im| among rows >= a, first index on ties
-      double v = (mine && t >= a) ? abs1(rj) : -1.0;
-      int idx = t;
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        if (ov > v || (ov == v && oi < idx)) {
-          v = ov;
-          idx = oi;
-        }
-      }
-      if (lane == 0) {
-        red_v[warp] = v;
-        red_i[warp] = idx;
-      }
-      __syncthreads();
-      double bv = red_v[0];
-      int p = red_i[0];
-#pragma unroll
-      for (int w = 1; w < NT / 32; ++w) {
-        const double wv = red_v[w];
-        const int wi = red_i[w];
-        if (wv > bv || (wv == bv && wi < p)) {
-          bv = wv;
-          p = wi;
-        }
-      }
+      const ArgMax am = cta_argmax(argmax_key(abs1(rj), t, mine && t >= a), red_key, red_idx);
+      const double bv = __longlong_as_double((long long)am.key);
+      int p = am.idx;
+      if (p >= n) p = a;  // no comparable candidate (NaN column): keep row a
       if (t == a) {
 #pragma unroll
         for (int c = 0; c < kBPanel; ++c) xrow[0][c] = r[c];

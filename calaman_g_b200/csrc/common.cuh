@@ -234,6 +234,51 @@ struct GemmScratchScope {
 
 }  // namespace clm
 
+namespace clm {
+
+// ---- pivot search: CTA-wide argmax of |x| with the first index on ties ------
+// A candidate magnitude v >= 0 is keyed by its IEEE-754 bits, which order
+// non-negative doubles exactly as their values; rows that are not candidates
+// (and NaN magnitudes, which partial pivoting never selects) carry key 0 and
+// index INT_MAX. The warp stage is three redux.sync reductions (high word, low
+// word among the high word's winners, smallest index among the key's winners).
+struct ArgMax {
+  unsigned long long key;
+  int idx;
+};
+
+__device__ __forceinline__ ArgMax argmax_key(double v, int idx, bool candidate) {
+  if (!candidate || !(v >= 0.0)) return ArgMax{0ull, 0x7fffffff};
+  return ArgMax{(unsigned long long)__double_as_longlong(v), idx};
+}
+
+__device__ __forceinline__ ArgMax warp_argmax(ArgMax a) {
+  const unsigned full = 0xffffffffu;
+  const unsigned hi = (unsigned)(a.key >> 32), lo = (unsigned)a.key;
+  const unsigned mhi = __reduce_max_sync(full, hi);
+  const unsigned mlo = __reduce_max_sync(full, hi == mhi ? lo : 0u);
+  const bool win = hi == mhi && lo == mlo;
+  const unsigned midx = __reduce_min_sync(full, win ? (unsigned)a.idx : 0x7fffffffu);
+  return ArgMax{((unsigned long long)mhi << 32) | mlo, (int)midx};
+}
+
+// CTA-wide: every thread passes its own candidate and receives the winner.
+// red_key / red_idx: shared arrays of blockDim.x / 32 entries. Contains one
+// __syncthreads; the caller separates consecutive calls by another barrier.
+__device__ __forceinline__ ArgMax cta_argmax(ArgMax a, unsigned long long *red_key, int *red_idx) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  a = warp_argmax(a);
+  if (lane == 0) {
+    red_key[warp] = a.key;
+    red_idx[warp] = a.idx;
+  }
+  __syncthreads();
+  ArgMax b = lane < nwarps ? ArgMax{red_key[lane], red_idx[lane]} : ArgMax{0ull, 0x7fffffff};
+  return warp_argmax(b);
+}
+
+}  // namespace clm
+
 // The opaque handle behind calamanHandle_t.
 struct calamanContext {
   cudaStream_t stream = nullptr;

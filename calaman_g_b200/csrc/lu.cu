@@ -783,8 +783,8 @@ __global__ void __launch_bounds__(512, 1)
   __shared__ T xrow[2][KBS];            // [0]: old row a, [1]: the pivot row
   __shared__ T l11[KBS][KBS + 1];
   __shared__ __align__(16) T u12[KBS][kMaxKb];
-  __shared__ double red_v[16];
-  __shared__ int red_i[16];
+  __shared__ unsigned long long red_key[16];
+  __shared__ int red_idx[16];
   __shared__ int plist[kMaxKb];
   __shared__ int flags[1];
   __shared__ int mpos[2 * kMaxKb], morg[2 * kMaxKb];
@@ -813,27 +813,11 @@ __global__ void __launch_bounds__(512, 1)
         const int gi = tid + q * NT;
         if (gi >= a && gi < h) argmax_merge(bv, bi, abs1(r[q][j]), gi);
       }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-        argmax_merge(bv, bi, ov, oi);
-      }
-      if (lane == 0) {
-        red_v[warp] = bv;
-        red_i[warp] = bi;
-      }
-      __syncthreads();
-      double pv = lane < nwarps ? red_v[lane] : -1.0;
-      int p = lane < nwarps ? red_i[lane] : INT_MAX;
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, pv, off);
-        const int oi = __shfl_xor_sync(0xffffffffu, p, off);
-        argmax_merge(pv, p, ov, oi);
-      }
+      const ArgMax am = cta_argmax(argmax_key(bv, bi, bi != INT_MAX), red_key, red_idx);
+      double pv = __longlong_as_double((long long)am.key);
+      int p = am.idx;
       bool forced = false;
-      if (p == INT_MAX || p < a) {  // no comparable candidate (NaN column): keep row a
+      if (p >= h || p < a) {  // no comparable candidate (NaN column): keep row a
         p = a;
         pv = 0.0;
         forced = true;
