@@ -691,6 +691,7 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
   auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (LD + 64));
   __shared__ T xrow[2][kBPanel];   // [0]: old row a, [1]: the pivot row
   __shared__ __align__(16) T urow[kBPanel];  // the pivot row right of column j
+  __shared__ T xrcp[1];                       // the pivot's reciprocal
   __shared__ T rdiag[kBPanel];     // reciprocals of U's diagonal block
   __shared__ int perm[NT];  // P: row i of P q is row perm[i] of q
   __shared__ int pos[NT];   // panel-local composite of the swaps
@@ -720,7 +721,13 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
       for (int c = 0; c < kBPanel; ++c)
         if (c == j) rj = r[c];
       // pivot: largest |Re| + |Im| among rows >= a, first index on ties
-      const ArgMax am = cta_argmax(argmax_key(abs1(rj), t, mine && t >= a), red_key, red_idx);
+      // warp winners form their row's reciprocal while the warps exchange
+      const ArgMax wa = warp_argmax(argmax_key(abs1(rj), t, mine && t >= a));
+      cta_argmax_publish(wa, red_key, red_idx);
+      T wrcp = elem<T>::one();
+      if (t == wa.idx && !is_zero(rj)) wrcp = divide(elem<T>::one(), rj);
+      __syncthreads();
+      const ArgMax am = cta_argmax_collect(red_key, red_idx);
       const double bv = __longlong_as_double((long long)am.key);
       int p = am.idx;
       if (p >= n) p = a;  // no comparable candidate (NaN column): keep row a
@@ -734,6 +741,7 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
           xrow[1][c] = r[c];
           urow[c] = (c > j && c < jb) ? r[c] : elem<T>::zero();  // the update's row, masked
         }
+        xrcp[0] = wrcp;
       }
       if (t == 0) {
         piv[j] = p;
@@ -763,7 +771,7 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
 #pragma unroll
         for (int c = 0; c < kBPanel; ++c)
           if (c == j) l = r[c];
-        l = abs1(pv) >= sfmin ? mul(l, divide(elem<T>::one(), pv)) : divide(l, pv);
+        l = abs1(pv) >= sfmin ? mul(l, xrcp[0]) : divide(l, pv);
         // unconditional rank-1 update against the masked row (zero at and left
         // of column j; |l| <= 1 under partial pivoting), then column j = l
 #pragma unroll

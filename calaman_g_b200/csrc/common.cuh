@@ -262,6 +262,20 @@ __device__ __forceinline__ ArgMax warp_argmax(ArgMax a) {
   return ArgMax{((unsigned long long)mhi << 32) | mlo, (int)midx};
 }
 
+// The two stages of cta_argmax, for callers that overlap work with the
+// cross-warp exchange (the warp winner may start on its row meanwhile).
+__device__ __forceinline__ void cta_argmax_publish(const ArgMax &w, unsigned long long *red_key, int *red_idx) {
+  if ((threadIdx.x & 31) == 0) {
+    red_key[threadIdx.x >> 5] = w.key;
+    red_idx[threadIdx.x >> 5] = w.idx;
+  }
+}
+__device__ __forceinline__ ArgMax cta_argmax_collect(const unsigned long long *red_key, const int *red_idx) {
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const ArgMax b = lane < nwarps ? ArgMax{red_key[lane], red_idx[lane]} : ArgMax{0ull, 0x7fffffff};
+  return warp_argmax(b);
+}
+
 // CTA-wide: every thread passes its own candidate and receives the winner.
 // red_key / red_idx: shared arrays of blockDim.x / 32 entries. Contains one
 // __syncthreads; the caller separates consecutive calls by another barrier.
