@@ -52,6 +52,9 @@ CONFIGS = {
                           desc="float64 2048x2048, N(0,1) rescaled to ||A||_1=6"),
     "expm_f32_4096": dict(n=4096, suf="s", norm=8.0, gen="gauss",
                           desc="float32 4096x4096, N(0,1)/sqrt(n) rescaled to ||A||_1=8"),
+    "expm_balanced_f64_1024": dict(n=1024, suf="d", norm=1.0e4, gen="scaled", entry="expm_balanced",
+                                   desc="float64 1024x1024, N(0,1) under a random power-of-two "
+                                        "similarity (2^-12..2^12), ||A||_1=1e4, balanced expm"),
     "expm_batched_f32_8192": dict(kind="batched", count=8192, nmax=256, suf="s",
                                   desc="8192 float32 matrices, n uniform on {16,32,...,256}, "
                                        "N(0,1) rescaled to ||A||_1 log-uniform in [0.1,100]"),
@@ -74,6 +77,9 @@ def make_matrix(cfg, seed=20261203):
     if cfg["gen"] == "gue":
         x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
         a = -1j * (x + x.conj().T) / 2
+    elif cfg["gen"] == "scaled":
+        d = 2.0 ** rng.integers(-12, 13, n)
+        a = (rng.standard_normal((n, n)) * d[:, None]) / d[None, :]
     else:
         a = rng.standard_normal((n, n)) / np.sqrt(n)
     a = a * (cfg["norm"] / np.abs(a).sum(axis=0).max())
@@ -191,8 +197,11 @@ def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
     reps, t0 = 0, time.perf_counter()
     result = None
     while True:
-        result, plan, _ = O.expm(a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64),
-                                 single=cfg["suf"] in "sc")
+        x = a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
+        if cfg.get("entry") == "expm_balanced":
+            result, plan = O.expm_balanced(x, single=cfg["suf"] in "sc")
+        else:
+            result, plan, _ = O.expm(x, single=cfg["suf"] in "sc")
         reps += 1
         el = time.perf_counter() - t0
         if el >= min_seconds or reps >= max_reps:
@@ -241,8 +250,12 @@ def run_reference(args, cfg):
         per_step, unit = 1, "expm/s"
         holder = {}
 
-        def one():
-            holder["plan"] = O.expm(x, single=single)[1]
+        if cfg.get("entry") == "expm_balanced":
+            def one():
+                holder["plan"] = O.expm_balanced(x, single=single)[1]
+        else:
+            def one():
+                holder["plan"] = O.expm(x, single=single)[1]
         sample = "one full expm of the benchmark matrix per step"
         plan_info = holder
     for _ in range(args.warmup):
@@ -348,12 +361,13 @@ def run_ours(args, cfg):
     assert lib.calamanCreate(ctypes.byref(h)).ok
     assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
     nb = ctypes.c_size_t()
-    assert getattr(lib, f"calaman_expm_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
+    entry = cfg.get("entry", "expm")
+    assert getattr(lib, f"calaman_{entry}_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
     work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
     info = torch.zeros(2, dtype=torch.int32, device=dev)
     infop = ctypes.cast(info.data_ptr(), capi.c_int_p)
     plan = capi.ExpmPlan()
-    fn = getattr(lib, f"calaman_expm_{suf}")
+    fn = getattr(lib, f"calaman_{entry}_{suf}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step():

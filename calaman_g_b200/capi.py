@@ -152,6 +152,13 @@ for _suf in ("s", "d"):
     SIGNATURES[f"calaman_expm_batched_{_suf}"] = (Status, _BATCHED)
     SIGNATURES[f"calaman_expm_vjp_batched_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int_p, c_size_t_p])
     SIGNATURES[f"calaman_expm_vjp_batched_{_suf}"] = (Status, _VJPB)
+SIGNATURES["calaman_gebal_bufferSize"] = (Status, [c_int, c_int_p])
+for _suf in ("s", "d", "c", "z"):
+    # gebal: stream, job, n, A, lda, ilo, ihi, scale, work, max_sweeps, sweeps
+    SIGNATURES[f"calaman_gebal_{_suf}"] = (Status, [c_void_p, c_int, c_int, c_void_p, c_int, c_int_p,
+                                                   c_int_p, c_void_p, c_void_p, c_int, c_int_p])
+    SIGNATURES[f"calaman_expm_balanced_bufferSize_{_suf}"] = (Status, [_H, c_int, c_size_t_p])
+    SIGNATURES[f"calaman_expm_balanced_{_suf}"] = (Status, _EXPM)
 SIGNATURES["calamanSetFloatSplit"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetFloatSplit"] = (Status, [_H, c_int_p])
 

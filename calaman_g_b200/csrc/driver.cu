@@ -339,6 +339,27 @@ calamanStatus_t ps_api(calamanHandle_t h, int n, const T *c, int degree, const T
 
 }  // namespace
 
+// The expm driver and its workspace size for callers in other translation
+// units (the balanced composition in balance.cu).
+template <typename T>
+calamanStatus_t expm_entry(calamanHandle_t blas, calamanStream_t stream, int n, const T *A, int lda, T *E,
+                           int lde, void *work, std::size_t lwork, int *d_info, calamanExpmPlan_t *plan) {
+  return expm_api<T>(blas, stream, n, A, lda, E, lde, work, lwork, d_info, plan);
+}
+template <typename T>
+std::size_t expm_workspace_bytes(int n) {
+  return expm_bytes<T>(n);
+}
+#define CLM_INST_ENTRY(T)                                                                              \
+  template calamanStatus_t expm_entry<T>(calamanHandle_t, calamanStream_t, int, const T *, int, T *, int, \
+                                         void *, std::size_t, int *, calamanExpmPlan_t *);              \
+  template std::size_t expm_workspace_bytes<T>(int);
+CLM_INST_ENTRY(float)
+CLM_INST_ENTRY(double)
+CLM_INST_ENTRY(float2)
+CLM_INST_ENTRY(double2)
+#undef CLM_INST_ENTRY
+
 int sm_count() {
   int dev = 0, cnt = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 148;

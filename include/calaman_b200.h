@@ -223,6 +223,47 @@ calamanStatus_t calaman_expm_vjp_batched_d(
     const int *h_ldg, double *const *h_gradA, const int *h_ldga, double *const *h_expA,
     const int *h_lde, void *d_work, size_t lwork_bytes, int *d_info, calamanExpmPlan_t *h_plans);
 
+/* ---- balancing: the scaling half of gebal, and the balanced expm ---------
+ * calaman_gebal_*: src/lapack/gebal/interface.cppm:100-255 (calaman::gebal).
+ * job: 0 None, 1 Permute, 2 Scale, 3 Both (GebalJob order); only None and
+ * Scale are built (Permute/Both return NOT_SUPPORTED). Overwrites A with
+ * B = D^-1 A D (Parlett-Reinsch, powers of two, exact), d_scale (real, n) =
+ * diag(D); *ilo = 1, *ihi = n. d_work: calaman_gebal_bufferSize ints.
+ * max_sweeps <= 0 selects the default cap (1000); *sweeps (may be NULL)
+ * receives the sweeps run. Synchronises `stream` once per sweep.
+ * calaman_expm_balanced_*: new entry point composing the reference's
+ * documented recipe (src/expm/README.md:100-122): exp(A) = D exp(B) D^-1.
+ * Same arguments and results as calaman_expm_*; *plan is the plan of B. */
+calamanStatus_t calaman_gebal_bufferSize(int n, int *lwork_ints);
+calamanStatus_t calaman_gebal_s(calamanStream_t stream, int job, int n, float *d_A, int lda, int *ilo,
+                                int *ihi, float *d_scale, int *d_work, int max_sweeps, int *sweeps);
+calamanStatus_t calaman_gebal_d(calamanStream_t stream, int job, int n, double *d_A, int lda, int *ilo,
+                                int *ihi, double *d_scale, int *d_work, int max_sweeps, int *sweeps);
+calamanStatus_t calaman_gebal_c(calamanStream_t stream, int job, int n, void *d_A, int lda, int *ilo,
+                                int *ihi, float *d_scale, int *d_work, int max_sweeps, int *sweeps);
+calamanStatus_t calaman_gebal_z(calamanStream_t stream, int job, int n, void *d_A, int lda, int *ilo,
+                                int *ihi, double *d_scale, int *d_work, int max_sweeps, int *sweeps);
+calamanStatus_t calaman_expm_balanced_bufferSize_s(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_balanced_bufferSize_d(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_balanced_bufferSize_c(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_balanced_bufferSize_z(calamanSolverHandle_t h, int n, size_t *bytes);
+calamanStatus_t calaman_expm_balanced_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                        calamanStream_t stream, int n, const float *d_A, int lda,
+                                        float *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                        int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_balanced_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                        calamanStream_t stream, int n, const double *d_A, int lda,
+                                        double *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                        int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_balanced_c(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                        calamanStream_t stream, int n, const void *d_A, int lda,
+                                        void *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                        int *d_info, calamanExpmPlan_t *plan);
+calamanStatus_t calaman_expm_balanced_z(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                        calamanStream_t stream, int n, const void *d_A, int lda,
+                                        void *d_expA, int lde, void *d_work, size_t lwork_bytes,
+                                        int *d_info, calamanExpmPlan_t *plan);
+
 /* ---- expm without a caller workspace ----------------------------------
  * No counterpart in the reference: calaman_G's expm always takes a caller
  * workspace. For callers that cannot call cudaMalloc (code hosted by a

@@ -178,6 +178,47 @@ Status expm_vjp_batched(BlasHandle blas, SolverHandle solver, cudaStream_t strea
                                       h_expA, h_lde, d_work, lwork_bytes, d_info, h_plans);
 }
 
+// ---- gebal, scaling job (src/lapack/gebal/interface.cppm:100-255) ---------------
+enum class GebalJob { None = 0, Permute = 1, Scale = 2, Both = 3 };
+inline constexpr int gebal_default_max_sweeps = 1000;
+template <typename T> Status gebal_bufferSize(int n, int *lwork_ints) {
+  return calaman_gebal_bufferSize(n, lwork_ints);
+}
+template <typename T>
+Status gebal(cudaStream_t stream, GebalJob job, int n, T *d_A, int lda, int *ilo, int *ihi, real_t<T> *d_scale,
+             int *d_work, int max_sweeps = gebal_default_max_sweeps) {
+  const int j = static_cast<int>(job);
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_gebal_s(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_gebal_d(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_gebal_c(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
+  else
+    return calaman_gebal_z(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
+}
+
+// ---- expm_balanced: D exp(D^-1 A D) D^-1 (new entry) ----------------------------
+template <typename T> Status expm_balanced_bufferSize(SolverHandle h, int n, std::size_t *bytes) {
+  if constexpr (std::is_same_v<T, float>) return calaman_expm_balanced_bufferSize_s(h, n, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_expm_balanced_bufferSize_d(h, n, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_expm_balanced_bufferSize_c(h, n, bytes);
+  else return calaman_expm_balanced_bufferSize_z(h, n, bytes);
+}
+template <typename T>
+Status expm_balanced(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int n, const T *d_A, int lda,
+                     T *d_expA, int lde, void *d_work, std::size_t lwork_bytes, int *d_info,
+                     ExpmPlan *plan = nullptr) {
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_expm_balanced_s(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_expm_balanced_d(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_expm_balanced_c(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+  else
+    return calaman_expm_balanced_z(blas, solver, stream, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info, plan);
+}
+
 // ---- pade (src/expm/pade.cppm:77-191) ------------------------------------------
 template <typename T>
 Status pade(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int m, int n, const T *d_A,

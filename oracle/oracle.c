@@ -13,6 +13,7 @@
 #include "oracle.h"
 
 #include <complex.h>
+#include <float.h>
 #include <math.h>
 #include <pthread.h>
 #include <stdlib.h>

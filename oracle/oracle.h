@@ -85,6 +85,10 @@ double oracle_norm1_d(int n, const double *A, int lda);
 void oracle_gemm_d(int m, int n, int k, double alpha, const double *A, int lda,
                    const double *B, int ldb, double beta, double *C, int ldc);
 int oracle_getrf_d(int n, double *A, int lda, int *ipiv);
+/* scaling half of ?gebal (src/lapack/gebal/gebal.cu:175-310); A overwritten
+ * with D^-1 A D, scale = diag(D) */
+int oracle_gebal_scale_d(int n, double *A, int lda, double *scale, int max_sweeps, int *sweeps);
+int oracle_gebal_scale_z(int n, double *A, int lda, double *scale, int max_sweeps, int *sweeps);
 int oracle_getrs_d(int n, int nrhs, const double *LU, int lda, const int *ipiv,
                    double *B, int ldb);
 /* returns 0, or -1 for an invalid argument; *info gets the getrf info code */

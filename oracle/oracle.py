@@ -90,6 +90,7 @@ def lib():
                 c_int, dp, c_int, dp, c_int, c_int, ctypes.POINTER(_ExpmPlan), ip]
             getattr(L, f"oracle_getrf_{suf}").argtypes = [c_int, dp, c_int, ip]
             getattr(L, f"oracle_getrs_{suf}").argtypes = [c_int, c_int, dp, c_int, ip, dp, c_int]
+            getattr(L, f"oracle_gebal_scale_{suf}").argtypes = [c_int, dp, c_int, dp, c_int, ip]
         L.oracle_gemm_d.argtypes = [c_int, c_int, c_int, c_double, dp, c_int, dp, c_int,
                                     c_double, dp, c_int]
         L.oracle_gemm_z.argtypes = [c_int, c_int, c_int, dp, dp, c_int, dp, c_int, dp, dp, c_int]
@@ -319,3 +320,23 @@ def expm_vjp_frechet(a, g, single: bool = False):
         dr = r @ dr + dr @ r
         r = r @ r
     return np.asfortranarray(dr), np.asfortranarray(r.conj().T), plan
+
+
+def gebal_scale(a, max_sweeps: int = 1000):
+    """The scaling half of ?gebal (Parlett-Reinsch, powers of two): returns
+    (B = D^-1 A D, diag(D), sweeps). The norms are summed in the library's
+    sweep order, so FP64 results are bit-identical to it."""
+    b = np.array(_as_f64(a), order="F")
+    n = b.shape[0]
+    d = np.ones(n)
+    sweeps = ctypes.c_int(0)
+    getattr(lib(), f"oracle_gebal_scale_{_suffix(b)}")(n, _dp(b), max(n, 1), _dp(d), max_sweeps,
+                                                       ctypes.byref(sweeps))
+    return b, d, sweeps.value
+
+
+def expm_balanced(a, single: bool = False):
+    """D exp(D^-1 A D) D^-1 with D from gebal_scale; returns (E, ExpmPlan of B)."""
+    b, d, _ = gebal_scale(a)
+    e, plan, _ = expm(b, single)
+    return np.asfortranarray(e * d[:, None] / d[None, :]), plan

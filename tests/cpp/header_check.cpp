@@ -69,6 +69,11 @@ int main() {
   CHECK(calaman::expm_vjp_batched_bufferSize<double>(nullptr, 2, ns, &bytes).ok() && bytes > 0);
   CHECK(calaman::expm_batched<double>(nullptr, nullptr, nullptr, 0, ns, nullptr, nullptr, nullptr, nullptr,
                                       nullptr, 0, nullptr).ok());  // an empty batch is a no-op
+  int lw = 0, ilo = 0, ihi = 0;
+  CHECK(calaman::gebal_bufferSize<double>(8, &lw).ok() && lw >= 1);
+  CHECK(calaman::gebal<double>(nullptr, calaman::GebalJob::Permute, 4, a.data(), 4, &ilo, &ihi, work.data(),
+                               &lw).code == CALAMAN_STATUS_NOT_SUPPORTED);
+  CHECK(calaman::expm_balanced_bufferSize<std::complex<float>>(nullptr, 16, &bytes).ok() && bytes > 0);
   std::printf("header_check ok\n");
   return 0;
 }
