@@ -76,6 +76,16 @@ std::size_t lu_scratch_bytes(int n);
 template <typename T>
 cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info_dev);
 
+// While a NoLookAheadScope is open on a host thread, getrf on that thread
+// factors every panel on the caller's stream instead of overlapping the next
+// panel on the library's auxiliary stream, so it creates no stream or event.
+extern thread_local bool tl_no_lookahead;
+struct NoLookAheadScope {
+  bool saved;
+  NoLookAheadScope() : saved(tl_no_lookahead) { tl_no_lookahead = true; }
+  ~NoLookAheadScope() { tl_no_lookahead = saved; }
+};
+
 // Solve A X = B with the factors from getrf: B (n x nrhs, ldb) is read, X is
 // written to (ldx); B and X may not alias. info_dev[0] = 0.
 template <typename T>

@@ -1181,6 +1181,7 @@ struct LookAhead {
   cudaEvent_t ready = nullptr, done = nullptr;
 };
 thread_local LookAhead tl_lookahead;
+thread_local bool tl_no_lookahead = false;
 
 cudaError_t lookahead(LookAhead *&out) {
   int dev = 0;
@@ -1225,8 +1226,11 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
   if ((e = cudaFuncSetAttribute(swap_kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)swap_smem)) !=
       cudaSuccess)
     return e;
-  LookAhead *la = nullptr;  // only matrices of more than one panel need it
-  if (n > kbn && (e = lookahead(la)) != cudaSuccess) return e;
+  // only matrices of more than one panel use the look-ahead stream, and not
+  // while a NoLookAheadScope is open on this thread (then every panel runs on s)
+  const bool ahead = n > kbn && !tl_no_lookahead;
+  LookAhead *la = nullptr;
+  if (ahead && (e = lookahead(la)) != cudaSuccess) return e;
   auto panel = [&](cudaStream_t st, int k, int kb) {
     return kb_cta > 0 ? launch_cta_panel<T>(st, n, A, lda, k, kb, sc, info_dev)
                       : launch_panel<T>(st, n, A, lda, k, kb, sc, info_dev);
@@ -1234,7 +1238,7 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
   if ((e = panel(s, 0, kbn < n ? kbn : n)) != cudaSuccess) return e;
   for (int k = 0; k < n; k += kbn) {
     const int kb = (k + kbn < n) ? kbn : n - k;
-    if (k > 0 && (e = cudaStreamWaitEvent(s, la->done, 0)) != cudaSuccess) return e;  // panel k
+    if (ahead && k > 0 && (e = cudaStreamWaitEvent(s, la->done, 0)) != cudaSuccess) return e;  // panel k
     const int others = n - kb;
     if (others > 0) {
       const int warps = 8;
@@ -1250,10 +1254,14 @@ cudaError_t getrf(cudaStream_t s, int n, T *A, int lda, void *scratch, int *info
       e = gemm_nn<T>(s, rest, kb2, kb, -1.0, L21, lda, A + (std::size_t)(k + kb) * lda + k, lda, 1.0,
                      A + (std::size_t)(k + kb) * lda + (k + kb), lda);
       if (e != cudaSuccess) return e;
-      if ((e = cudaEventRecord(la->ready, s)) != cudaSuccess) return e;
-      if ((e = cudaStreamWaitEvent(la->aux, la->ready, 0)) != cudaSuccess) return e;
-      if ((e = panel(la->aux, k + kb, kb2)) != cudaSuccess) return e;
-      if ((e = cudaEventRecord(la->done, la->aux)) != cudaSuccess) return e;
+      if (ahead) {
+        if ((e = cudaEventRecord(la->ready, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(la->aux, la->ready, 0)) != cudaSuccess) return e;
+        if ((e = panel(la->aux, k + kb, kb2)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(la->done, la->aux)) != cudaSuccess) return e;
+      } else if ((e = panel(s, k + kb, kb2)) != cudaSuccess) {  // disjoint from the wide update
+        return e;
+      }
       // the wide update, concurrent with that panel
       if (rest > kb2) {
         e = gemm_nn<T>(s, rest, rest - kb2, kb, -1.0, L21, lda, A + (std::size_t)(k + kb + kb2) * lda + k, lda,

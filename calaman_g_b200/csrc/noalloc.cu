@@ -4,7 +4,8 @@
 // Some callers cannot call cudaMalloc: code hosted by a framework that owns
 // every device allocation and hands out none, loops that must not allocate
 // once they are running, and small FFI or plugin callers with no device
-// allocator at hand. This entry point serves them by running the ordinary
+// allocator at hand. The call also creates no stream or event: its LU runs
+// every panel on the caller's stream. This entry point serves them by running the ordinary
 // calaman_expm_d on a workspace that lives in a file-scope device array of
 // this library, so the caller passes only the input, the output and d_info.
 //
@@ -61,6 +62,8 @@ extern "C" calamanStatus_t calaman_expm_noalloc_d(calamanBlasHandle_t blas, cala
   if (need > kNoAllocScratchBytes) return clm::blas_status(CALAMAN_STATUS_NOT_SUPPORTED);
   void *scratch = nullptr;
   CLM_TRY(scratch_for_current_device(&scratch));
+  // no look-ahead stream either: this path creates no CUDA resources
+  clm::NoLookAheadScope serial;
   return calaman_expm_d(blas, blas, stream, n, d_A, lda, d_expA, lde, scratch, kNoAllocScratchBytes,
                         d_info, plan);
 }
