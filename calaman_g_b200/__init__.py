@@ -26,6 +26,7 @@ __all__ = [
     "horner_bufferSize", "paterson_stockmeyer", "paterson_stockmeyer_plan",
     "paterson_stockmeyer_bufferSize", "paterson_stockmeyer_cost",
     "paterson_stockmeyer_block_size", "to_colmajor", "from_colmajor", "lib",
+    "lacn2_bufferSize", "lacn2_estimate",
 ]
 
 
@@ -262,6 +263,40 @@ def matrix_norm1(a, handle: Handle | None = None) -> float:
     cs = torch.empty(n, dtype=real, device=a.device)
     return getattr(lib(), f"calaman_matrix_norm1_{_suffix(a.dtype)}")(
         ctypes.c_void_p(h.stream), n, _vp(A), n, _vp(cs))
+
+
+def lacn2_bufferSize(n: int, dtype) -> int:
+    return getattr(lib(), f"calaman_lacn2_bufferSize_{_suffix(dtype)}")(n)
+
+
+def lacn2_estimate(apply, apply_t, n: int, dtype=None, handle: Handle | None = None,
+                   device=None):
+    """Estimate ||A||_1 of an operator given only its products, by driving the
+    reverse-communication estimator (calaman_lacn2_*, LAPACK xLACN2) to
+    completion. ``apply(x)`` / ``apply_t(x)`` return A x / A^T x for a CUDA
+    vector x of ``dtype`` (float32 or float64), on the handle's stream.
+    Returns (est, v) with est <= ||A||_1 and v = A w, est = ||v||_1 / ||w||_1."""
+    torch = _torch()
+    dtype = dtype or torch.float64
+    if dtype not in (torch.float32, torch.float64):
+        raise TypeError("lacn2 is real only (float32 or float64)")
+    suf = _suffix(dtype)
+    ct = ctypes.c_float if dtype == torch.float32 else ctypes.c_double
+    h = handle or default_handle()
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    nbytes = lacn2_bufferSize(n, dtype)
+    work = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+    v = torch.zeros(n, dtype=dtype, device=dev)
+    x = torch.zeros(n, dtype=dtype, device=dev)
+    est, kase = ct(0), ctypes.c_int(0)
+    isave = (ctypes.c_int * 3)()
+    fn = getattr(lib(), f"calaman_lacn2_{suf}")
+    while True:
+        _check("lacn2", fn(h.ptr, n, _vp(v), _vp(x), _vp(work), nbytes, ctypes.byref(est),
+                           ctypes.byref(kase), isave))
+        if kase.value == 0:
+            return float(est.value), v
+        x.copy_(apply(x) if kase.value == 1 else apply_t(x))
 
 
 def horner_bufferSize(n: int, dtype) -> int:

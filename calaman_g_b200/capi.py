@@ -159,6 +159,11 @@ for _suf in ("s", "d", "c", "z"):
                                                    c_int_p, c_void_p, c_void_p, c_int, c_int_p])
     SIGNATURES[f"calaman_expm_balanced_bufferSize_{_suf}"] = (Status, [_H, c_int, c_size_t_p])
     SIGNATURES[f"calaman_expm_balanced_{_suf}"] = (Status, _EXPM)
+for _suf, _real in (("s", c_float), ("d", c_double)):
+    # lacn2: blas, n, v, x, work, bytes, est (host), kase (host), isave[3] (host)
+    SIGNATURES[f"calaman_lacn2_bufferSize_{_suf}"] = (c_size_t, [c_int])
+    SIGNATURES[f"calaman_lacn2_{_suf}"] = (Status, [_H, c_int, c_void_p, c_void_p, c_void_p, c_size_t,
+                                                   ctypes.POINTER(_real), c_int_p, c_int_p])
 SIGNATURES["calamanSetFloatSplit"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetFloatSplit"] = (Status, [_H, c_int_p])
 

@@ -264,6 +264,24 @@ calamanStatus_t calaman_expm_balanced_z(calamanBlasHandle_t blas, calamanSolverH
                                         void *d_expA, int lde, void *d_work, size_t lwork_bytes,
                                         int *d_info, calamanExpmPlan_t *plan);
 
+/* ---- lacn2: 1-norm estimate by reverse communication (LAPACK xLACN2) ----
+ * src/lapack/lacn2/interface.cppm:85-200 (calaman::lacn2_bufferSize,
+ * calaman::lacn2). Real only (s/d), as the reference. Start with *kase = 0;
+ * on a return with *kase 1 (2) overwrite d_x with A x (A^T x), ordered on
+ * the handle's stream, and call again with everything else unchanged; *kase
+ * 0 on return: *est <= ||A||_1 and d_v = A w with est = ||v||_1 / ||w||_1.
+ * est, kase and isave[3] are host state (isave 1-based, as the reference's
+ * std::array<int, 3>); d_work holds ISGN and must be the same buffer, of at
+ * least calaman_lacn2_bufferSize_*(n) bytes, on every call of one run.
+ * Synchronises the handle's stream at most once per call. INVALID_VALUE for
+ * n < 1, a null pointer, a bad state or a short workspace. */
+size_t calaman_lacn2_bufferSize_s(int n);
+size_t calaman_lacn2_bufferSize_d(int n);
+calamanStatus_t calaman_lacn2_s(calamanBlasHandle_t blas, int n, float *d_v, float *d_x, void *d_work,
+                                size_t work_bytes, float *est, int *kase, int *isave);
+calamanStatus_t calaman_lacn2_d(calamanBlasHandle_t blas, int n, double *d_v, double *d_x, void *d_work,
+                                size_t work_bytes, double *est, int *kase, int *isave);
+
 /* ---- expm without a caller workspace ----------------------------------
  * No counterpart in the reference: calaman_G's expm always takes a caller
  * workspace. For callers that cannot call cudaMalloc (code hosted by a

@@ -17,6 +17,7 @@
 // wwrDoubleComplex); horner and paterson_stockmeyer exist for float and double.
 #pragma once
 
+#include <array>
 #include <complex>
 #include <cstddef>
 #include <type_traits>
@@ -196,6 +197,22 @@ Status gebal(cudaStream_t stream, GebalJob job, int n, T *d_A, int lda, int *ilo
     return calaman_gebal_c(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
   else
     return calaman_gebal_z(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
+}
+
+// ---- lacn2 (src/lapack/lacn2/interface.cppm:85-200) -------------------------------
+template <typename T> std::size_t lacn2_bufferSize(int n) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "lacn2 is real only");
+  if constexpr (std::is_same_v<T, float>) return calaman_lacn2_bufferSize_s(n);
+  else return calaman_lacn2_bufferSize_d(n);
+}
+template <typename T>
+Status lacn2(BlasHandle handle, int n, T *d_v, T *d_x, void *d_work, std::size_t work_bytes, T &est,
+             int &kase, std::array<int, 3> &isave) {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "lacn2 is real only");
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_lacn2_s(handle, n, d_v, d_x, d_work, work_bytes, &est, &kase, isave.data());
+  else
+    return calaman_lacn2_d(handle, n, d_v, d_x, d_work, work_bytes, &est, &kase, isave.data());
 }
 
 // ---- expm_balanced: D exp(D^-1 A D) D^-1 (new entry) ----------------------------

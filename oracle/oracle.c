@@ -215,6 +215,18 @@ oracle_ps_plan_t oracle_ps_plan(int degree, int s_requested) {
 #undef SUF
 #undef IS_CPLX
 
+#define R float
+#define SUF s
+#include "oracle_lacn2.inc"
+#undef R
+#undef SUF
+
+#define R double
+#define SUF d
+#include "oracle_lacn2.inc"
+#undef R
+#undef SUF
+
 void oracle_gemm_d(int m, int n, int k, double alpha, const double *A, int lda, const double *B,
                    int ldb, double beta, double *C, int ldc) {
   gemm_impl_d(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);

@@ -25,6 +25,8 @@
  *                                         src/paterson_stockmeyer/paterson_stockmeyer.cu:51-85
  *   oracle_horner_d                       src/horner/interface.cppm:156-194,
  *                                         src/horner/horner.cu:39-67
+ *   oracle_lacn2_{s,d}                    src/lapack/lacn2/interface.cppm:104-200
+ *                                         (LAPACK xLACN2, 3.10+ sign test)
  *   oracle_getrf/getrs_{d,z}              LAPACK xGETRF/xGETRS semantics (the
  *                                         reference reaches cuSOLVER through
  *                                         WarpWraps, src/expm/pade.cppm:186-188):
@@ -114,6 +116,14 @@ int oracle_paterson_stockmeyer_d(int n, const double *coeffs, int degree, const 
                                  int lda, double *P, int ldp, int s_requested);
 int oracle_horner_d(int n, const double *coeffs, int degree, const double *A, int lda,
                     double *P, int ldp);
+
+/* ---- 1-norm estimator by reverse communication (LAPACK xLACN2) --------
+ * Start with *kase = 0; on a return with kase 1 (2) overwrite x with A x
+ * (A^T x) and call again. kase 0 on return: *est <= ||A||_1, v = A w with
+ * est = ||v||_1 / ||w||_1. isgn: n ints kept across calls; isave: 3 ints,
+ * 1-based. Returns 0, or -1 for a bad argument or state. */
+int oracle_lacn2_s(int n, float *v, float *x, int *isgn, float *est, int *kase, int *isave);
+int oracle_lacn2_d(int n, double *v, double *x, int *isgn, double *est, int *kase, int *isave);
 
 #ifdef __cplusplus
 }

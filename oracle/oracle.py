@@ -96,6 +96,9 @@ def lib():
         L.oracle_gemm_z.argtypes = [c_int, c_int, c_int, dp, dp, c_int, dp, c_int, dp, dp, c_int]
         L.oracle_paterson_stockmeyer_d.argtypes = [c_int, dp, c_int, dp, c_int, dp, c_int, c_int]
         L.oracle_horner_d.argtypes = [c_int, dp, c_int, dp, c_int, dp, c_int]
+        for suf, ct in (("s", ctypes.c_float), ("d", c_double)):
+            rp = ctypes.POINTER(ct)
+            getattr(L, f"oracle_lacn2_{suf}").argtypes = [c_int, rp, rp, ip, rp, ip, ip]
         _lib = L
     return _lib
 
@@ -340,3 +343,40 @@ def expm_balanced(a, single: bool = False):
     b, d, _ = gebal_scale(a)
     e, plan, _ = expm(b, single)
     return np.asfortranarray(e * d[:, None] / d[None, :]), plan
+
+
+class Lacn2Trace:
+    """One run of the 1-norm estimator: the kase returned by every call, the
+    isave state after it, the final estimate and v (= A w)."""
+
+    def __init__(self, kases, isaves, est, v):
+        self.kases, self.isaves, self.est, self.v = kases, isaves, est, v
+
+
+def lacn2(apply, apply_t, n: int, single: bool = False, max_calls: int = 64) -> Lacn2Trace:
+    """Drive the reverse-communication estimator (xLACN2, oracle_lacn2_{s,d})
+    to completion. ``apply(x)`` / ``apply_t(x)`` return A x / A^T x as numpy
+    vectors; they are evaluated in float64 and rounded to the working
+    precision."""
+    dt = np.float32 if single else np.float64
+    ct = ctypes.c_float if single else ctypes.c_double
+    fn = getattr(lib(), "oracle_lacn2_" + ("s" if single else "d"))
+    v = np.zeros(n, dtype=dt)
+    x = np.zeros(n, dtype=dt)
+    isgn = np.zeros(max(n, 1), dtype=np.int32)
+    est, kase = ct(0), ctypes.c_int(0)
+    isave = (ctypes.c_int * 3)()
+    rp = ctypes.POINTER(ct)
+    kases, isaves = [], []
+    for _ in range(max_calls):
+        rc = fn(n, v.ctypes.data_as(rp), x.ctypes.data_as(rp), _ip(isgn), ctypes.byref(est),
+                ctypes.byref(kase), isave)
+        if rc != 0:
+            raise ValueError("oracle_lacn2: invalid argument or state")
+        kases.append(kase.value)
+        isaves.append(tuple(isave))
+        if kase.value == 0:
+            return Lacn2Trace(kases, isaves, float(est.value), v.copy())
+        y = apply(x.astype(np.float64)) if kase.value == 1 else apply_t(x.astype(np.float64))
+        x[:] = np.asarray(y, dtype=np.float64).astype(dt)
+    raise RuntimeError("oracle_lacn2 did not finish")

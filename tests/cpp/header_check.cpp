@@ -74,6 +74,12 @@ int main() {
   CHECK(calaman::gebal<double>(nullptr, calaman::GebalJob::Permute, 4, a.data(), 4, &ilo, &ihi, work.data(),
                                &lw).code == CALAMAN_STATUS_NOT_SUPPORTED);
   CHECK(calaman::expm_balanced_bufferSize<std::complex<float>>(nullptr, 16, &bytes).ok() && bytes > 0);
+  // lacn2: size query and host-side rejection (no device work)
+  CHECK(calaman::lacn2_bufferSize<double>(100) >= 100 * sizeof(int));
+  double est = 0;
+  int kase = 1;
+  std::array<int, 3> isave{9, 0, 0};
+  CHECK(calaman::lacn2<double>(nullptr, 4, d.data(), g.data(), work.data(), 1 << 20, est, kase, isave) == invalid);
   std::printf("header_check ok\n");
   return 0;
 }

@@ -214,3 +214,29 @@ def test_handle_calls_reject_null(lib):
 def test_norm1_rejects_bad_arguments(lib):
     assert np.isnan(lib.calaman_matrix_norm1_d(None, 0, None, 1, None))
     assert np.isnan(lib.calaman_matrix_norm1_s(None, 4, None, 4, None))
+
+
+def test_lacn2_size_and_rejections(lib):
+    """calaman::lacn2's argument contract (src/lapack/lacn2/interface.cppm:119-126):
+    INVALID_VALUE for n < 1, null vectors or workspace, a state outside 1..5
+    with kase != 0, and a short workspace -- all before device work."""
+    for suf, ct in (("s", ctypes.c_float), ("d", ctypes.c_double)):
+        size = getattr(lib, f"calaman_lacn2_bufferSize_{suf}")
+        assert size(1000) >= 1000 * 4 and size(1000) % 256 == 0
+        fn = getattr(lib, f"calaman_lacn2_{suf}")
+        est, kase = ct(0), ctypes.c_int(0)
+        isave = (ctypes.c_int * 3)()
+        buf = ctypes.c_void_p(1 << 20)  # never dereferenced: every call below is rejected
+        iv = capi.INVALID_VALUE
+
+        def call(n, v, x, w, nbytes, k=0, s0=0):
+            kase.value, isave[0] = k, s0
+            return fn(None, n, v, x, w, nbytes, ctypes.byref(est), ctypes.byref(kase), isave).code
+
+        assert call(0, buf, buf, buf, size(4)) == iv
+        assert call(4, None, buf, buf, size(4)) == iv
+        assert call(4, buf, None, buf, size(4)) == iv
+        assert call(4, buf, buf, None, size(4)) == iv
+        assert call(4, buf, buf, buf, size(4) - 1) == iv
+        assert call(4, buf, buf, buf, size(4), k=1, s0=0) == iv
+        assert call(4, buf, buf, buf, size(4), k=2, s0=6) == iv
