@@ -55,6 +55,9 @@ CONFIGS = {
     "expm_balanced_f64_1024": dict(n=1024, suf="d", norm=1.0e4, gen="scaled", entry="expm_balanced",
                                    desc="float64 1024x1024, N(0,1) under a random power-of-two "
                                         "similarity (2^-12..2^12), ||A||_1=1e4, balanced expm"),
+    "expm_herm_c128_1024": dict(n=1024, suf="z", norm=50.0, gen="herm", entry="expm_herm",
+                                desc="complex128 1024x1024 Hermitian H=(X+X^H)/2 (GUE), ||H||_1=50, "
+                                     "expm_herm (eigendecomposition route)"),
     "expm_batched_f32_8192": dict(kind="batched", count=8192, nmax=256, suf="s",
                                   desc="8192 float32 matrices, n uniform on {16,32,...,256}, "
                                        "N(0,1) rescaled to ||A||_1 log-uniform in [0.1,100]"),
@@ -74,9 +77,11 @@ ELEM_BYTES = {"s": 4, "d": 8, "c": 8, "z": 16}
 def make_matrix(cfg, seed=20261203):
     rng = np.random.default_rng(seed)
     n = cfg["n"]
-    if cfg["gen"] == "gue":
+    if cfg["gen"] in ("gue", "herm"):
         x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
-        a = -1j * (x + x.conj().T) / 2
+        a = (x + x.conj().T) / 2
+        if cfg["gen"] == "gue":
+            a = -1j * a
     elif cfg["gen"] == "scaled":
         d = 2.0 ** rng.integers(-12, 13, n)
         a = (rng.standard_normal((n, n)) * d[:, None]) / d[None, :]
@@ -123,6 +128,14 @@ def vjp_flops(n, m, s):
     pim = {3: 1, 5: 2, 7: 3, 9: 4, 13: 3}[m]
     gemms = 3 * pim + (6 if m == 13 else 0) + 4 + 3 * s
     return gemms * 2.0 * n ** 3 + (2.0 / 3.0) * n ** 3 + 2 * 2.0 * n ** 3
+
+
+def herm_flops(n, cplx):
+    """Algorithmic flops of the eigendecomposition route: Householder
+    tridiagonalisation (4/3 n^3), back-transformation of the eigenvectors
+    (2 n^3) and the product M U^H (2 n^3), x4 for complex, plus the
+    divide-and-conquer merges' real products (8/3 n^3 summed over levels)."""
+    return (4.0 if cplx else 1.0) * (4.0 / 3.0 + 4.0) * n ** 3 + (8.0 / 3.0) * n ** 3
 
 
 def expm_flops(n, m, s, cplx):
@@ -200,6 +213,8 @@ def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
         x = a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
         if cfg.get("entry") == "expm_balanced":
             result, plan = O.expm_balanced(x, single=cfg["suf"] in "sc")
+        elif cfg.get("entry") == "expm_herm":
+            result = O.expm_herm(x)
         else:
             result, plan, _ = O.expm(x, single=cfg["suf"] in "sc")
         reps += 1
@@ -253,11 +268,16 @@ def run_reference(args, cfg):
         if cfg.get("entry") == "expm_balanced":
             def one():
                 holder["plan"] = O.expm_balanced(x, single=single)[1]
+        elif cfg.get("entry") == "expm_herm":
+            def one():
+                O.expm_herm(x)
         else:
             def one():
                 holder["plan"] = O.expm(x, single=single)[1]
         sample = "one full expm of the benchmark matrix per step"
-        plan_info = holder
+        if cfg.get("entry") == "expm_herm":
+            sample += " (eigendecomposition route: LAPACK zheevd through numpy, threaded BLAS)"
+        plan_info = holder if cfg.get("entry") != "expm_herm" else None
     for _ in range(args.warmup):
         one()
     t0 = time.perf_counter()
@@ -279,9 +299,11 @@ def run_reference(args, cfg):
                                    f"algorithm), {cores} threads"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    if kind == "single":
+    if kind == "single" and plan_info:
         line["tflops"] = expm_flops(cfg["n"], plan_info["plan"].m, plan_info["plan"].s,
                                     cfg["suf"] in "cz") * value / 1e12
+    elif kind == "single":
+        line["tflops"] = herm_flops(cfg["n"], cfg["suf"] in "cz") * value / 1e12
     print(json.dumps(line), flush=True)
 
 
@@ -362,7 +384,11 @@ def run_ours(args, cfg):
     assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
     nb = ctypes.c_size_t()
     entry = cfg.get("entry", "expm")
-    assert getattr(lib, f"calaman_{entry}_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
+    herm = entry == "expm_herm"
+    if herm:
+        assert getattr(lib, f"calaman_{entry}_bufferSize_{suf}")(h, capi.FILL_LOWER, n, ctypes.byref(nb)).ok
+    else:
+        assert getattr(lib, f"calaman_{entry}_bufferSize_{suf}")(h, n, ctypes.byref(nb)).ok
     work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
     info = torch.zeros(2, dtype=torch.int32, device=dev)
     infop = ctypes.cast(info.data_ptr(), capi.c_int_p)
@@ -371,11 +397,16 @@ def run_ours(args, cfg):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def step():
-        st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), n, ctypes.c_void_p(dA.data_ptr()), n,
-                ctypes.c_void_p(dE.data_ptr()), n, ctypes.c_void_p(work.data_ptr()), nb.value,
-                infop, ctypes.byref(plan))
+        if herm:
+            st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), capi.FILL_LOWER, n,
+                    ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(dE.data_ptr()), n,
+                    ctypes.c_void_p(work.data_ptr()), nb.value, infop)
+        else:
+            st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), n, ctypes.c_void_p(dA.data_ptr()), n,
+                    ctypes.c_void_p(dE.data_ptr()), n, ctypes.c_void_p(work.data_ptr()), nb.value,
+                    infop, ctypes.byref(plan))
         if not st.ok:
-            raise RuntimeError(f"expm failed: {st!r}")
+            raise RuntimeError(f"{entry} failed: {st!r}")
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -428,7 +459,7 @@ def run_ours(args, cfg):
     e2e_value = world * args.steps / (e2e_ms * 1e-3)
 
     if rank == 0:
-        flops = expm_flops(n, plan.m, plan.s, cplx)
+        flops = herm_flops(n, cplx) if herm else expm_flops(n, plan.m, plan.s, cplx)
         achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
         executed = None
         if suf == "s":
@@ -454,7 +485,8 @@ def run_ours(args, cfg):
             "dtype": {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[suf],
             "data": "synthetic (seeded)",
             "config": {"workload": args.config, "desc": cfg["desc"],
-                       "plan": {"m": plan.m, "s": plan.s, "num_gemms": plan.num_gemms},
+                       "plan": None if herm else {"m": plan.m, "s": plan.s,
+                                                   "num_gemms": plan.num_gemms},
                        "l2": "flushed before every timed step (256 MiB write, untimed)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "tflops": flops * value / 1e12,

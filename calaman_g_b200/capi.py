@@ -25,6 +25,7 @@ INVALID_VALUE = 7
 NOT_SUPPORTED = 15
 DOMAIN_BLAS, DOMAIN_SOLVER, DOMAIN_RUNTIME = 0, 1, 2
 POINTER_MODE_HOST, POINTER_MODE_DEVICE = 0, 1
+FILL_LOWER, FILL_UPPER = 0, 1
 
 _NAMES = {0: "SUCCESS", 1: "NOT_INITIALIZED", 3: "ALLOC_FAILED", 7: "INVALID_VALUE",
           8: "ARCH_MISMATCH", 13: "EXECUTION_FAILED", 14: "INTERNAL_ERROR", 15: "NOT_SUPPORTED"}
@@ -159,6 +160,15 @@ for _suf in ("s", "d", "c", "z"):
                                                    c_int_p, c_void_p, c_void_p, c_int, c_int_p])
     SIGNATURES[f"calaman_expm_balanced_bufferSize_{_suf}"] = (Status, [_H, c_int, c_size_t_p])
     SIGNATURES[f"calaman_expm_balanced_{_suf}"] = (Status, _EXPM)
+for _suf in ("s", "d", "c", "z"):
+    # expm_herm: blas, solver, stream, uplo, n, A, lda, E, lde, work, bytes, info
+    SIGNATURES[f"calaman_expm_herm_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int, c_size_t_p])
+    SIGNATURES[f"calaman_expm_herm_{_suf}"] = (Status, [_H, _H, c_void_p, c_int, c_int, c_void_p, c_int,
+                                                       c_void_p, c_int, c_void_p, c_size_t, c_int_p])
+    # heevd: stream, uplo, n, A, lda, w, work, bytes, info
+    SIGNATURES[f"calaman_heevd_bufferSize_{_suf}"] = (Status, [c_int, c_int, c_size_t_p])
+    SIGNATURES[f"calaman_heevd_{_suf}"] = (Status, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                                   c_void_p, c_size_t, c_int_p])
 for _suf, _real in (("s", c_float), ("d", c_double)):
     # lacn2: blas, n, v, x, work, bytes, est (host), kase (host), isave[3] (host)
     SIGNATURES[f"calaman_lacn2_bufferSize_{_suf}"] = (c_size_t, [c_int])

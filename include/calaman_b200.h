@@ -72,6 +72,10 @@ typedef void *calamanStream_t; /* a cudaStream_t */
 
 enum { CALAMAN_POINTER_MODE_HOST = 0, CALAMAN_POINTER_MODE_DEVICE = 1 };
 
+/* wwrblasFillMode_t: which triangle of a symmetric / Hermitian matrix is read
+ * (numerically the CUDA backend's values). */
+enum { CALAMAN_FILL_MODE_LOWER = 0, CALAMAN_FILL_MODE_UPPER = 1 };
+
 /* wwrblasCreate / wwrsolverDnCreate: binds the current device, stream 0. */
 calamanStatus_t calamanCreate(calamanHandle_t *handle);
 calamanStatus_t calamanDestroy(calamanHandle_t handle);
@@ -263,6 +267,51 @@ calamanStatus_t calaman_expm_balanced_z(calamanBlasHandle_t blas, calamanSolverH
                                         calamanStream_t stream, int n, const void *d_A, int lda,
                                         void *d_expA, int lde, void *d_work, size_t lwork_bytes,
                                         int *d_info, calamanExpmPlan_t *plan);
+
+/* ---- expm_herm: exp(A) for symmetric / Hermitian A by eigendecomposition --
+ * src/expm/expm_herm.cppm:70-199 (calaman::expm_herm_bufferSize, expm_herm).
+ * Reads only the `uplo` triangle of A (CALAMAN_FILL_MODE_*); exp(A) =
+ * U diag(exp(w)) U^H from the library's own eigensolver. Never synchronises.
+ * d_info: ONE device int, 0 on success (n + 1 if the eigensolver could not
+ * complete). INVALID_VALUE for n < 1, n > 46340, lda/lde < n, a null
+ * workspace or a bad uplo; ALLOC_FAILED for a short workspace. The single
+ * tiers are solved in FP64 and rounded. */
+calamanStatus_t calaman_expm_herm_bufferSize_s(calamanSolverHandle_t h, int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_expm_herm_bufferSize_d(calamanSolverHandle_t h, int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_expm_herm_bufferSize_c(calamanSolverHandle_t h, int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_expm_herm_bufferSize_z(calamanSolverHandle_t h, int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_expm_herm_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                    calamanStream_t stream, int uplo, int n, const float *d_A, int lda,
+                                    float *d_expA, int lde, void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_expm_herm_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                    calamanStream_t stream, int uplo, int n, const double *d_A, int lda,
+                                    double *d_expA, int lde, void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_expm_herm_c(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                    calamanStream_t stream, int uplo, int n, const void *d_A, int lda,
+                                    void *d_expA, int lde, void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_expm_herm_z(calamanBlasHandle_t blas, calamanSolverHandle_t solver,
+                                    calamanStream_t stream, int uplo, int n, const void *d_A, int lda,
+                                    void *d_expA, int lde, void *d_work, size_t lwork_bytes, int *d_info);
+
+/* ---- heevd: the symmetric / Hermitian eigensolver behind expm_herm -------
+ * The reference's expm_herm calls the vendor syevd / heevd through WarpWraps
+ * (src/expm/expm_herm.cppm:176-182); this is the library's own, with that
+ * call's meaning: eigenvalues ascending into d_w (real, n), eigenvectors
+ * overwrite A (columns, lda), only the `uplo` triangle is read. Tridiagonal
+ * reduction, divide and conquer, compact-WY back-transformation, all on the
+ * device; never synchronises. d_info: one device int as for expm_herm. */
+calamanStatus_t calaman_heevd_bufferSize_s(int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_heevd_bufferSize_d(int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_heevd_bufferSize_c(int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_heevd_bufferSize_z(int uplo, int n, size_t *bytes);
+calamanStatus_t calaman_heevd_s(calamanStream_t stream, int uplo, int n, float *d_A, int lda, float *d_w,
+                                void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_heevd_d(calamanStream_t stream, int uplo, int n, double *d_A, int lda, double *d_w,
+                                void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_heevd_c(calamanStream_t stream, int uplo, int n, void *d_A, int lda, float *d_w,
+                                void *d_work, size_t lwork_bytes, int *d_info);
+calamanStatus_t calaman_heevd_z(calamanStream_t stream, int uplo, int n, void *d_A, int lda, double *d_w,
+                                void *d_work, size_t lwork_bytes, int *d_info);
 
 /* ---- lacn2: 1-norm estimate by reverse communication (LAPACK xLACN2) ----
  * src/lapack/lacn2/interface.cppm:85-200 (calaman::lacn2_bufferSize,

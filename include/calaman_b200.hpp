@@ -199,6 +199,49 @@ Status gebal(cudaStream_t stream, GebalJob job, int n, T *d_A, int lda, int *ilo
     return calaman_gebal_z(stream, j, n, d_A, lda, ilo, ihi, d_scale, d_work, max_sweeps, nullptr);
 }
 
+// ---- expm_herm (src/expm/expm_herm.cppm:70-199) and its eigensolver ---------------
+enum class FillMode : int { Lower = CALAMAN_FILL_MODE_LOWER, Upper = CALAMAN_FILL_MODE_UPPER };
+template <typename T> Status expm_herm_bufferSize(SolverHandle h, FillMode uplo, int n, std::size_t *bytes) {
+  const int u = static_cast<int>(uplo);
+  if constexpr (std::is_same_v<T, float>) return calaman_expm_herm_bufferSize_s(h, u, n, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_expm_herm_bufferSize_d(h, u, n, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_expm_herm_bufferSize_c(h, u, n, bytes);
+  else return calaman_expm_herm_bufferSize_z(h, u, n, bytes);
+}
+template <typename T>
+Status expm_herm(BlasHandle blas, SolverHandle solver, cudaStream_t stream, FillMode uplo, int n, const T *d_A,
+                 int lda, T *d_expA, int lde, void *d_work, std::size_t lwork_bytes, int *d_info) {
+  const int u = static_cast<int>(uplo);
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_expm_herm_s(blas, solver, stream, u, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_expm_herm_d(blas, solver, stream, u, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_expm_herm_c(blas, solver, stream, u, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info);
+  else
+    return calaman_expm_herm_z(blas, solver, stream, u, n, d_A, lda, d_expA, lde, d_work, lwork_bytes, d_info);
+}
+template <typename T> Status heevd_bufferSize(FillMode uplo, int n, std::size_t *bytes) {
+  const int u = static_cast<int>(uplo);
+  if constexpr (std::is_same_v<T, float>) return calaman_heevd_bufferSize_s(u, n, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_heevd_bufferSize_d(u, n, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>) return calaman_heevd_bufferSize_c(u, n, bytes);
+  else return calaman_heevd_bufferSize_z(u, n, bytes);
+}
+template <typename T>
+Status heevd(cudaStream_t stream, FillMode uplo, int n, T *d_A, int lda, real_t<T> *d_w, void *d_work,
+             std::size_t lwork_bytes, int *d_info) {
+  const int u = static_cast<int>(uplo);
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_heevd_s(stream, u, n, d_A, lda, d_w, d_work, lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_heevd_d(stream, u, n, d_A, lda, d_w, d_work, lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_heevd_c(stream, u, n, d_A, lda, d_w, d_work, lwork_bytes, d_info);
+  else
+    return calaman_heevd_z(stream, u, n, d_A, lda, d_w, d_work, lwork_bytes, d_info);
+}
+
 // ---- lacn2 (src/lapack/lacn2/interface.cppm:85-200) -------------------------------
 template <typename T> std::size_t lacn2_bufferSize(int n) {
   static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "lacn2 is real only");

@@ -380,3 +380,31 @@ def lacn2(apply, apply_t, n: int, single: bool = False, max_calls: int = 64) -> 
         y = apply(x.astype(np.float64)) if kase.value == 1 else apply_t(x.astype(np.float64))
         x[:] = np.asarray(y, dtype=np.float64).astype(dt)
     raise RuntimeError("oracle_lacn2 did not finish")
+
+
+def hermitian_from_triangle(a, upper: bool) -> np.ndarray:
+    """The symmetric / Hermitian matrix whose `upper` (else lower) triangle is
+    a's, diagonal real: what an eigensolver reading one triangle sees."""
+    a = _as_f64(a)
+    t = np.triu(a) if upper else np.tril(a)
+    h = t + (np.triu(a, 1) if upper else np.tril(a, -1)).conj().T
+    np.fill_diagonal(h, np.real(np.diag(a)))
+    return np.asfortranarray(h)
+
+
+def heevd(a, upper: bool = False):
+    """Eigenvalues (ascending) and eigenvectors of the Hermitian matrix read
+    from one triangle: LAPACK xSYEVD / xHEEVD through numpy.linalg.eigh (the
+    routine the reference reaches through WarpWraps as the vendor's syevd /
+    heevd, src/expm/expm_herm.cppm:176-182)."""
+    h = hermitian_from_triangle(a, upper)
+    w, u = np.linalg.eigh(h)
+    return w, np.asfortranarray(u)
+
+
+def expm_herm(a, upper: bool = False) -> np.ndarray:
+    """exp(A) = U diag(exp(w)) U^H for symmetric / Hermitian A read from one
+    triangle (calaman::expm_herm, src/expm/expm_herm.cppm:163-196: eigensolve,
+    column scale by exp(w_j), one product with U^H)."""
+    w, u = heevd(a, upper)
+    return np.asfortranarray((u * np.exp(w)[None, :]) @ u.conj().T)

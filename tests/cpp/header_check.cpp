@@ -74,6 +74,12 @@ int main() {
   CHECK(calaman::gebal<double>(nullptr, calaman::GebalJob::Permute, 4, a.data(), 4, &ilo, &ihi, work.data(),
                                &lw).code == CALAMAN_STATUS_NOT_SUPPORTED);
   CHECK(calaman::expm_balanced_bufferSize<std::complex<float>>(nullptr, 16, &bytes).ok() && bytes > 0);
+  // expm_herm / heevd: size queries and host-side rejection
+  CHECK(calaman::expm_herm_bufferSize<std::complex<double>>(nullptr, calaman::FillMode::Upper, 16, &bytes).ok() &&
+        bytes > 0);
+  CHECK(calaman::heevd_bufferSize<float>(calaman::FillMode::Lower, 16, &bytes).ok() && bytes > 0);
+  CHECK(calaman::expm_herm<double>(nullptr, nullptr, nullptr, calaman::FillMode::Lower, 0, a.data(), n, d.data(), n,
+                                   work.data(), 4096, info) == invalid);
   // lacn2: size query and host-side rejection (no device work)
   CHECK(calaman::lacn2_bufferSize<double>(100) >= 100 * sizeof(int));
   double est = 0;

@@ -103,6 +103,46 @@ class Runner:
     def workspace(self, nbytes: int):
         return self.torch.empty(max(nbytes, 256), dtype=self.torch.uint8, device="cuda")
 
+    def expm_herm(self, a: np.ndarray, suf: str, upper: bool = False, lda: int | None = None,
+                  lde: int | None = None, out_fill=-123.5, lwork: int | None = None):
+        """calaman_expm_herm_<suf>: returns (status, E (n x n), full E buffer, info)."""
+        n = a.shape[0]
+        lda = lda or n
+        lde = lde or n
+        dA = _dev(colmajor_buffer(a, lda, suf))
+        dE = _dev(np.full(n * lde, out_fill, dtype=NP_DTYPE[suf]))
+        b = ctypes.c_size_t()
+        uplo = self.capi.FILL_UPPER if upper else self.capi.FILL_LOWER
+        assert getattr(self.lib, f"calaman_expm_herm_bufferSize_{suf}")(self.h, uplo, n, ctypes.byref(b)).ok
+        w = self.workspace(b.value)
+        info = self.torch.full((1,), -99, dtype=self.torch.int32, device="cuda")
+        st = getattr(self.lib, f"calaman_expm_herm_{suf}")(
+            self.h, self.h, ctypes.c_void_p(self.stream), uplo, n, vp(dA), lda, vp(dE), lde, vp(w),
+            b.value if lwork is None else lwork, ctypes.cast(info.data_ptr(), self.capi.c_int_p))
+        self.torch.cuda.synchronize()
+        full = dE.cpu().numpy()
+        e = full.reshape(n, lde)[:, :n].T
+        return st, e, full, int(info.cpu()[0])
+
+    def heevd(self, a: np.ndarray, suf: str, upper: bool = False, lda: int | None = None):
+        """calaman_heevd_<suf>: returns (status, w, U (n x n), info)."""
+        n = a.shape[0]
+        lda = lda or n
+        dA = _dev(colmajor_buffer(a, lda, suf))
+        real = self.torch.float32 if suf in ("s", "c") else self.torch.float64
+        dw = self.torch.full((n,), float("nan"), dtype=real, device="cuda")
+        b = ctypes.c_size_t()
+        uplo = self.capi.FILL_UPPER if upper else self.capi.FILL_LOWER
+        assert getattr(self.lib, f"calaman_heevd_bufferSize_{suf}")(uplo, n, ctypes.byref(b)).ok
+        w = self.workspace(b.value)
+        info = self.torch.full((1,), -99, dtype=self.torch.int32, device="cuda")
+        st = getattr(self.lib, f"calaman_heevd_{suf}")(
+            ctypes.c_void_p(self.stream), uplo, n, vp(dA), lda, vp(dw), vp(w), b.value,
+            ctypes.cast(info.data_ptr(), self.capi.c_int_p))
+        self.torch.cuda.synchronize()
+        u = dA.cpu().numpy().reshape(n, lda)[:, :n].T
+        return st, dw.cpu().numpy(), u, int(info.cpu()[0])
+
     def expm(self, a: np.ndarray, suf: str, lda: int | None = None, lde: int | None = None,
              out_fill=-123.5, lwork: int | None = None):
         n = a.shape[0]
