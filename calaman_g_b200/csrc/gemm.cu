@@ -11,6 +11,7 @@
 // Operands are staged global -> shared by cp.async in a multi-stage ring; all
 // edges (M, N, K not multiples of the tile) are zero-filled by the copy's
 // src-size operand, so any shape and any leading dimension is legal.
+#include <algorithm>
 #include "dmma.cuh"
 
 namespace clm {
@@ -27,7 +28,15 @@ template <int BM, int BN, int WM, int WN, int STAGES, bool V16>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     dgemm_nn_kernel(int M, int N, int K, double alpha, const double *__restrict__ A, int lda,
                     const double *__restrict__ B, int ldb, double beta, double *__restrict__ C,
-                    int ldc) {
+                    int ldc, int kslice, long long cstride) {
+  // split K: slice blockIdx.z takes K rows [z kslice, (z+1) kslice) into C + z cstride
+  {
+    const int kz0 = blockIdx.z * kslice;
+    K = min(K - kz0, kslice);
+    A += (std::size_t)kz0 * lda;
+    B += kz0;
+    C += (std::size_t)blockIdx.z * cstride;
+  }
   constexpr int BK = 16;
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int SA = BM + 4;
@@ -179,7 +188,14 @@ template <int BM, int BN, int WM, int WN, int STAGES>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     zgemm_nn_kernel(int M, int N, int K, double alpha, const double2 *__restrict__ A, int lda,
                     const double2 *__restrict__ B, int ldb, double beta, double2 *__restrict__ C,
-                    int ldc) {
+                    int ldc, int kslice, long long cstride) {
+  {
+    const int kz0 = blockIdx.z * kslice;
+    K = min(K - kz0, kslice);
+    A += (std::size_t)kz0 * lda;
+    B += kz0;
+    C += (std::size_t)blockIdx.z * cstride;
+  }
   constexpr int BK = 16;
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int SA = BM + 2;
@@ -389,7 +405,8 @@ __global__ void __launch_bounds__(256)
 
 template <int BM, int BN, int WM, int WN, int STAGES, bool V16>
 cudaError_t run_dgemm(cudaStream_t s, int M, int N, int K, double alpha, const double *A, int lda,
-                      const double *B, int ldb, double beta, double *C, int ldc) {
+                      const double *B, int ldb, double beta, double *C, int ldc, int splits = 1,
+                      int kslice = 0, long long cstride = 0) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int smem = STAGES * (16 * (BM + 4) + BN * 20) * (int)sizeof(double);
   auto kern = dgemm_nn_kernel<BM, BN, WM, WN, STAGES, V16>;
@@ -399,14 +416,16 @@ cudaError_t run_dgemm(cudaStream_t s, int M, int N, int K, double alpha, const d
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-  kern<<<grid, NT, smem, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
+  kern<<<grid, NT, smem, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, splits > 1 ? kslice : K,
+                              cstride);
   return cudaGetLastError();
 }
 
 template <int BM, int BN, int WM, int WN, int STAGES>
 cudaError_t run_zgemm(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A, int lda,
-                      const double2 *B, int ldb, double beta, double2 *C, int ldc) {
+                      const double2 *B, int ldb, double beta, double2 *C, int ldc, int splits = 1,
+                      int kslice = 0, long long cstride = 0) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int smem = STAGES * (16 * (BM + 2) + BN * 20) * (int)sizeof(double2);
   auto kern = zgemm_nn_kernel<BM, BN, WM, WN, STAGES>;
@@ -416,8 +435,9 @@ cudaError_t run_zgemm(cudaStream_t s, int M, int N, int K, double alpha, const d
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN);
-  kern<<<grid, NT, smem, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
+  kern<<<grid, NT, smem, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, splits > 1 ? kslice : K,
+                              cstride);
   return cudaGetLastError();
 }
 
@@ -496,6 +516,75 @@ cudaError_t gemm_nn<float2>(cudaStream_t s, int M, int N, int K, double alpha, c
     simt_gemm_nn_kernel<float2><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     return cudaGetLastError();
   });
+}
+
+// ---- split-K: the skinny products (few output tiles, long K) ----------------
+namespace {
+template <typename T>
+__global__ void splitk_reduce_kernel(int M, int N, int splits, const T *__restrict__ part, double alpha,
+                                     double beta, T *__restrict__ C, int ldc) {
+  const long long total = (long long)M * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    T acc = part[idx];
+    for (int z = 1; z < splits; ++z) acc = add(acc, part[(std::size_t)z * total + idx]);  // slice order
+    const int i = (int)(idx % M), j = (int)(idx / M);
+    T &c = C[(std::size_t)j * ldc + i];
+    c = beta == 0.0 ? scale(acc, alpha) : rfma(alpha, acc, scale(c, beta));
+  }
+}
+
+// Slices of 64-multiple K so that tiles x slices fills two waves of SMs.
+int splitk_slices(int M, int N, int K, int max_splits, int *kslice) {
+  const long long tiles = (long long)((M + 63) / 64) * ((N + 63) / 64);
+  long long want = (2LL * sm_count() + tiles - 1) / tiles;
+  want = std::min<long long>(want, max_splits);
+  want = std::min<long long>(want, std::max(1, K / 64));
+  if (want < 1) want = 1;
+  int ks = (int)((K + want - 1) / want);
+  ks = (ks + 63) / 64 * 64;
+  *kslice = ks;
+  return (K + ks - 1) / ks;
+}
+}  // namespace
+
+template <>
+cudaError_t gemm_nn_splitk<double>(cudaStream_t s, int M, int N, int K, double alpha, const double *A, int lda,
+                                   const double *B, int ldb, double beta, double *C, int ldc, double *partial,
+                                   int max_splits) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  int ks = 0;
+  const int sp = splitk_slices(M, N, K, max_splits, &ks);
+  if (sp <= 1) return gemm_nn<double>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  const bool v16 = aligned16(A) && aligned16(B) && (lda % 2 == 0) && (ldb % 2 == 0);
+  cudaError_t e = timed_launch(s, real_flops(M, N, K), [&] {
+    return v16 ? run_dgemm<64, 64, 32, 32, 4, true>(s, M, N, K, 1.0, A, lda, B, ldb, 0.0, partial, M, sp, ks,
+                                                     (long long)M * N)
+               : run_dgemm<64, 64, 32, 32, 4, false>(s, M, N, K, 1.0, A, lda, B, ldb, 0.0, partial, M, sp, ks,
+                                                      (long long)M * N);
+  });
+  if (e != cudaSuccess) return e;
+  splitk_reduce_kernel<double><<<std::min(((long long)M * N + 255) / 256, 4LL * 148), 256, 0, s>>>(
+      M, N, sp, partial, alpha, beta, C, ldc);
+  return launched();
+}
+
+template <>
+cudaError_t gemm_nn_splitk<double2>(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A,
+                                    int lda, const double2 *B, int ldb, double beta, double2 *C, int ldc,
+                                    double2 *partial, int max_splits) {
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  int ks = 0;
+  const int sp = splitk_slices(M, N, K, max_splits, &ks);
+  if (sp <= 1) return gemm_nn<double2>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  cudaError_t e = timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
+    return run_zgemm<64, 64, 32, 16, 3>(s, M, N, K, 1.0, A, lda, B, ldb, 0.0, partial, M, sp, ks,
+                                         (long long)M * N);
+  });
+  if (e != cudaSuccess) return e;
+  splitk_reduce_kernel<double2><<<std::min(((long long)M * N + 255) / 256, 4LL * 148), 256, 0, s>>>(
+      M, N, sp, partial, alpha, beta, C, ldc);
+  return launched();
 }
 
 }  // namespace clm

@@ -58,6 +58,8 @@ __device__ __forceinline__ double re(double x) { return x; }
 __device__ __forceinline__ double re(double2 x) { return x.x; }
 __device__ __forceinline__ double abs2(double x) { return x * x; }
 __device__ __forceinline__ double abs2(double2 x) { return x.x * x.x + x.y * x.y; }
+__device__ __forceinline__ double sub_(double a, double b) { return a - b; }
+__device__ __forceinline__ double2 sub_(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 template <typename C> __device__ __forceinline__ C from_re(double r);
 template <> __device__ __forceinline__ double from_re<double>(double r) { return r; }
 template <> __device__ __forceinline__ double2 from_re<double2>(double r) { return make_double2(r, 0.0); }
@@ -85,14 +87,14 @@ __device__ __forceinline__ V warp_sum(V v) {
 // Sum over the block, returned to every thread (same order everywhere).
 template <typename V, int kWarps>
 __device__ __forceinline__ V block_sum(V v, V *red) {
+  static_assert(kWarps <= 32, "one partial per lane");
   v = warp_sum(v);
   __syncthreads();
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
-  V t = red[0];
-#pragma unroll
-  for (int w = 1; w < kWarps; ++w) t = add(t, red[w]);
-  return t;
+  V t{};
+  if ((threadIdx.x & 31) < kWarps) t = red[threadIdx.x & 31];
+  return warp_sum(t);  // every warp forms the same total from the same partials
 }
 
 // ---- bounded grid barrier ---------------------------------------------------
@@ -108,13 +110,19 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 // counter only grows: barrier e is passed when it reaches e * gridDim.x.
 // Returns false (for every thread of the CTA) when the wait ran out or another
 // CTA reported a failure; the caller then returns.
+__device__ __forceinline__ void red_add_release(unsigned *p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// The arrival is a release (it publishes every write the CTA made before the
+// block barrier), the polls are acquires (later reads of the CTA see every
+// CTA's published writes).
 __device__ bool grid_sync(unsigned *count, int *err, unsigned &epoch, int *s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
     ++epoch;
     const unsigned target = epoch * gridDim.x;
-    __threadfence();
-    atomicAdd(count, 1u);
+    red_add_release(count, 1u);
     int ok = 1;
     unsigned spins = 0;
     while (ld_acquire(count) < target) {
@@ -122,10 +130,9 @@ __device__ bool grid_sync(unsigned *count, int *err, unsigned &epoch, int *s_ok)
         ok = 0;
         break;
       }
-      __nanosleep(64);
+      __nanosleep(20);
     }
     if (!ok) atomicExch(err, 1);
-    __threadfence();
     *s_ok = ok;
   }
   __syncthreads();
@@ -183,9 +190,10 @@ __global__ void herm_fill_kernel(int n, const T *__restrict__ A, int lda, int up
 }
 
 // ---- stage 1: tridiagonal reduction, one cooperative launch ----------------
-constexpr int kTrdThreads = 512;
+constexpr int kTrdThreads = 1024;
 constexpr int kTrdWarps = kTrdThreads / 32;
-constexpr int kTrdChunk = 1024;  // rows staged in shared memory per pass
+constexpr int kTrdMaxGrid = 160;  // CTAs of the reduction: one per SM at most
+constexpr int kTrdVecs = 5;       // pivot, v, next v, p, w (n each)
 
 template <typename C>
 struct TrdArgs {
@@ -193,6 +201,7 @@ struct TrdArgs {
   C *W;
   double *d, *e;
   C *tau, *vsc, *p;
+  C *vec;  // per-CTA vectors (4 n each) when they do not stay in shared memory
   unsigned *bar;
   int *err;
 };
@@ -221,97 +230,197 @@ __device__ __forceinline__ void reflector(double2 alpha, double xnorm2, double2 
     return;
   }
   beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2), alpha.x);
-  tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-  scl = divide(make_double2(1.0, 0.0), make_double2(alpha.x - beta, alpha.y));
+  // two independent reciprocals instead of a chain of divisions:
+  // tau = (beta - alpha) / beta, scl = 1 / (alpha - beta) = conj(d) / |d|^2
+  const double rb = 1.0 / beta;
+  const double dr = alpha.x - beta, di = alpha.y;
+  const double rd = 1.0 / (dr * dr + di * di);
+  tau = make_double2((beta - alpha.x) * rb, -alpha.y * rb);
+  scl = make_double2(dr * rd, -di * rd);
 }
 
-template <typename C>
+// One grid barrier per column, and one pass over the CTA's own columns per
+// column. After the barrier of step k every CTA holds, identically, the pivot
+// column k+1 brought up to date (the value its owner published, minus step
+// k's rank-2 correction), forms reflector k+1 itself, and then sweeps its own
+// columns once: each element gets step k's update and, still in registers,
+// enters the dot product with v_{k+1} that is its share of step k+1's
+// Hermitian product. Only that product p has to cross CTAs (double-buffered,
+// so a CTA one step ahead never overwrites what a slower one still reads).
+//   prologue: reflector 0, p^(0) = tau_0 A v_0 over the own columns;
+//   step k: barrier; gather p^(k) and the published column k+1;
+//     alpha_h = -1/2 tau_k p^H v_k, w = p + alpha_h v_k;
+//     pivot k+1 = old column k+1 - v_k conj(w_{k+1}) - w conj(v_{k+1});
+//     reflector k+1; own columns c >= k+2 -= v_k conj(w_c) + w conj(v_k,c)
+//     fused with p^(k+1)_c = tau_{k+1} conj(col_c) . v_{k+1};
+//     the owner of column k+2 publishes it.
+// Column k+1 is never updated in place at step k (every CTA derives it), so
+// reading its published value races with nothing. kRes keeps the CTA's own
+// columns and the five vectors in shared memory; otherwise the columns stay
+// in W (L2) and the vectors in a per-CTA global scratch.
+template <typename C, bool kRes>
+__device__ __forceinline__ C trd_ld(const C *p) {
+  if constexpr (kRes) return *p;
+  else return ldcg(p);
+}
+
+template <typename C, bool kRes>
 __global__ void __launch_bounds__(kTrdThreads, 1) hetrd_kernel(TrdArgs<C> a) {
   extern __shared__ __align__(16) unsigned char trd_smem[];
-  C *xs = reinterpret_cast<C *>(trd_smem);
-  C *ys = xs + kTrdChunk;
-  C *acc = ys + kTrdChunk;  // one slot per owned column
   __shared__ C red_c[kTrdWarps];
   __shared__ double red_d[kTrdWarps];
   __shared__ int s_ok;
   const int n = a.n, G = gridDim.x, b = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ncmax = (n + G - 1) / G;
+  C *acc = reinterpret_cast<C *>(trd_smem);  // max(ncmax, kTrdWarps) partial dots
+  C *xv, *res = nullptr;
+  if constexpr (kRes) {
+    xv = acc + (ncmax > kTrdWarps ? ncmax : kTrdWarps);
+    res = xv + kTrdVecs * (std::size_t)n;  // own column j at res + j n
+  } else {
+    xv = a.vec + (std::size_t)b * kTrdVecs * n;
+  }
+  C *vv = xv + n, *vn = vv + n, *pv = vn + n, *wv = pv + n;
   const C zero = from_re<C>(0.0), one = from_re<C>(1.0);
+  if constexpr (kRes) {
+    for (int j = 0; j < ncmax; ++j) {
+      const int c = b + j * G;
+      if (c >= n) break;
+      for (int r = tid; r < n; r += kTrdThreads) res[(std::size_t)j * n + r] = ldcg(a.W + (std::size_t)c * n + r);
+    }
+  }
+  for (int i = tid; i < n; i += kTrdThreads) xv[i] = ldcg(a.W + i);  // the first pivot, column 0
+  __syncthreads();
+  // own columns c >= first, as (index of the first, count, warps per column)
+  auto own = [&](int first, int &c0, int &nc, int &j0, int &wpc) {
+    c0 = first + ((b - first) % G + G) % G;
+    nc = c0 < n ? (n - 1 - c0) / G + 1 : 0;
+    j0 = (c0 - b) / G;
+    wpc = nc > 0 && nc < kTrdWarps ? kTrdWarps / nc : 1;
+  };
+  auto column = [&](int c0, int j0, int j) -> C * {
+    if constexpr (kRes) return res + (std::size_t)(j0 + j) * n;
+    else return a.W + (std::size_t)(c0 + j * G) * n;
+  };
+  C tau = zero, scl = zero;
+  if (n > 1) {
+    // prologue: reflector 0 and p^(0) = tau_0 conj(col_c) . v_0, own c >= 1
+    double nrm = 0.0;
+    for (int i = 2 + tid; i < n; i += kTrdThreads) nrm += abs2(xv[i]);
+    double beta;
+    reflector(xv[1], block_sum<double, kTrdWarps>(nrm, red_d), tau, scl, beta);
+    for (int i = 1 + tid; i < n; i += kTrdThreads) vv[i] = (i == 1) ? one : mul(scl, xv[i]);
+    if (b == 0 && tid == 0) {
+      a.d[0] = re(xv[0]);
+      a.e[0] = beta;
+      a.tau[0] = tau;
+      a.vsc[0] = scl;
+    }
+    __syncthreads();
+    int c0, nc, j0, wpc;
+    own(1, c0, nc, j0, wpc);
+    for (int jw = warp; jw < nc * wpc; jw += kTrdWarps) {
+      const int j = jw / wpc, sub = jw - j * wpc;
+      const C *col = column(c0, j0, j);
+      C sacc = zero;
+#pragma unroll 4
+      for (int i = 1 + lane + 32 * sub; i < n; i += 32 * wpc) sacc = fmac(cj(trd_ld<C, kRes>(col + i)), vv[i], sacc);
+      sacc = warp_sum(sacc);
+      if (lane == 0) acc[jw] = sacc;
+    }
+    __syncthreads();
+    for (int j = tid; j < nc; j += kTrdThreads) {
+      C dot = acc[j * wpc];
+      for (int sub = 1; sub < wpc; ++sub) dot = add(dot, acc[j * wpc + sub]);
+      a.p[c0 + j * G] = mul(tau, dot);
+    }
+  }
   unsigned epoch = 0;
   for (int k = 0; k + 1 < n; ++k) {
     if (!grid_sync(a.bar, a.err, epoch, &s_ok)) return;
-    const C *colk = a.W + (std::size_t)k * n;
-    const int c0 = k + 1 + ((b - (k + 1)) % G + G) % G;  // first owned column > k
-    const int nc = c0 < n ? (n - 1 - c0) / G + 1 : 0;
-    for (int j = tid; j < nc; j += kTrdThreads) acc[j] = zero;
-    // (a) |x|^2 for x = column k below row k+1, and conj(col_c) . x per owned c
-    double nrm = 0.0;
-    for (int r0 = k + 2; r0 < n; r0 += kTrdChunk) {
-      const int len = min(kTrdChunk, n - r0);
-      __syncthreads();
-      for (int t = tid; t < len; t += kTrdThreads) {
-        const C x = ldcg(colk + r0 + t);
-        xs[t] = x;
-        nrm += abs2(x);
-      }
-      __syncthreads();
-      for (int j = warp; j < nc; j += kTrdWarps) {
-        const C *col = a.W + (std::size_t)(c0 + j * G) * n + r0;
-        C s = zero;
-        for (int t = lane; t < len; t += 32) s = fmac(cj(ldcg(col + t)), xs[t], s);
-        s = warp_sum(s);
-        if (lane == 0) acc[j] = add(acc[j], s);
-      }
-    }
-    const double xnorm2 = block_sum<double, kTrdWarps>(nrm, red_d);
-    const C alpha = ldcg(colk + k + 1);
-    C tau, scl;
-    double beta;
-    reflector(alpha, xnorm2, tau, scl, beta);
-    // p_c = tau (A22 v)_c = tau (conj(W[k+1][c]) + scl conj(col_c) . x)
-    for (int j = tid; j < nc; j += kTrdThreads) {
-      const int c = c0 + j * G;
-      const C w1 = cj(ldcg(a.W + (std::size_t)c * n + k + 1));
-      a.p[c] = mul(tau, fmac(scl, acc[j], w1));
-    }
-    if (b == 0 && tid == 0) {
-      a.d[k] = re(ldcg(colk + k));
-      a.e[k] = beta;
-      a.tau[k] = tau;
-      a.vsc[k] = scl;
-    }
-    if (!grid_sync(a.bar, a.err, epoch, &s_ok)) return;
-    // (b) alpha_h = -1/2 tau p^H v; w = p + alpha_h v; A22 -= v w^H + w v^H
+    const C *pk = a.p + (std::size_t)(k & 1) * n;
+    C *pn = a.p + (std::size_t)((k + 1) & 1) * n;
+    // the pivot column k is read by nobody else now: store it for the back-transform
+    if (b == 0)
+      for (int i = k + 1 + tid; i < n; i += kTrdThreads) a.W[(std::size_t)k * n + i] = xv[i];
+    // gather p^(k) and the published column k+1
     C part = zero;
-    for (int i = k + 2 + tid; i < n; i += kTrdThreads) part = fmac(cj(ldcg(a.p + i)), ldcg(colk + i), part);
-    const C phx = block_sum<C, kTrdWarps>(part, red_c);
-    const C phv = fmac(scl, phx, cj(ldcg(a.p + k + 1)));
+    for (int i = k + 1 + tid; i < n; i += kTrdThreads) {
+      const C pi = ldcg(pk + i);
+      pv[i] = pi;
+      wv[i] = ldcg(a.W + (std::size_t)(k + 1) * n + i);
+      part = fmac(cj(pi), vv[i], part);
+    }
+    const C phv = block_sum<C, kTrdWarps>(part, red_c);  // also orders the CTA-0 store above
     const C ah = scale(mul(tau, phv), -0.5);
-    for (int r0 = k + 1; r0 < n; r0 += kTrdChunk) {
-      const int len = min(kTrdChunk, n - r0);
-      __syncthreads();
-      for (int t = tid; t < len; t += kTrdThreads) {
-        const int i = r0 + t;
-        const C v = (i == k + 1) ? one : mul(scl, ldcg(colk + i));
-        xs[t] = v;
-        ys[t] = fmac(ah, v, ldcg(a.p + i));
-      }
-      __syncthreads();
-      for (int j = warp; j < nc; j += kTrdWarps) {
-        const int c = c0 + j * G;
-        const C vc = (c == k + 1) ? one : mul(scl, ldcg(colk + c));
-        const C cvc = cj(vc), cwc = cj(fmac(ah, vc, ldcg(a.p + c)));
-        C *col = a.W + (std::size_t)c * n + r0;
-        for (int t = lane; t < len; t += 32) {
-          C x = sub(ldcg(col + t), add(mul(xs[t], cwc), mul(ys[t], cvc)));
-          if (r0 + t == c) x = from_re<C>(re(x));
-          col[t] = x;
-        }
+    const C cw1 = cj(add(pv[k + 1], ah));  // conj(w_{k+1}); v_{k+1} = 1
+    double nrm = 0.0;
+    for (int i = k + 1 + tid; i < n; i += kTrdThreads) {
+      const C wi = fmac(ah, vv[i], pv[i]);
+      C x = sub_(wv[i], add(mul(vv[i], cw1), wi));
+      if (i == k + 1) x = from_re<C>(re(x));
+      xv[i] = x;
+      wv[i] = wi;
+      if (i >= k + 3) nrm += abs2(x);
+    }
+    const double xnorm2 = block_sum<double, kTrdWarps>(nrm, red_d);  // xv, wv complete
+    const bool more = k + 2 < n;  // a reflector k+1 exists
+    C taun = zero, scln = zero;
+    if (more) {
+      double beta;
+      reflector(xv[k + 2], xnorm2, taun, scln, beta);
+      for (int i = k + 2 + tid; i < n; i += kTrdThreads) vn[i] = (i == k + 2) ? one : mul(scln, xv[i]);
+      if (b == 0 && tid == 0) {
+        a.d[k + 1] = re(xv[k + 1]);
+        a.e[k + 1] = beta;
+        a.tau[k + 1] = taun;
+        a.vsc[k + 1] = scln;
       }
     }
+    __syncthreads();
+    // own columns c >= k+2: update (rows k+1..) fused with the next dot (rows k+2..)
+    {
+      int c0, nc, j0, wpc;
+      own(k + 2, c0, nc, j0, wpc);
+      for (int jw = warp; jw < nc * wpc; jw += kTrdWarps) {
+        const int j = jw / wpc, sub = jw - j * wpc;
+        const int c = c0 + j * G;
+        C *col = column(c0, j0, j);
+        const C cvc = cj(vv[c]), cwc = cj(wv[c]);
+        C sacc = zero;
+#pragma unroll 4
+        for (int i = k + 1 + lane + 32 * sub; i < n; i += 32 * wpc) {
+          C y = sub_(trd_ld<C, kRes>(col + i), add(mul(vv[i], cwc), mul(wv[i], cvc)));
+          if (i == c) y = from_re<C>(re(y));
+          col[i] = y;
+          if (i >= k + 2) sacc = fmac(cj(y), vn[i], sacc);
+        }
+        sacc = warp_sum(sacc);
+        if (lane == 0) acc[jw] = sacc;
+      }
+      __syncthreads();
+      if (more)
+        for (int j = tid; j < nc; j += kTrdThreads) {
+          C dot = acc[j * wpc];
+          for (int sub = 1; sub < wpc; ++sub) dot = add(dot, acc[j * wpc + sub]);
+          pn[c0 + j * G] = mul(taun, dot);
+        }
+    }
+    if constexpr (kRes) {
+      // the owner of column k+2 publishes it (rows k+2..) for the next step
+      if (more && (k + 2) % G == b) {
+        const C *src = res + (std::size_t)((k + 2 - b) / G) * n;
+        for (int r = k + 2 + tid; r < n; r += kTrdThreads) a.W[(std::size_t)(k + 2) * n + r] = src[r];
+      }
+    }
+    C *t = vv;
+    vv = vn;
+    vn = t;
+    tau = taun;
+    scl = scln;
   }
-  if (!grid_sync(a.bar, a.err, epoch, &s_ok)) return;
-  if (b == 0 && tid == 0) a.d[n - 1] = re(ldcg(a.W + (std::size_t)(n - 1) * n + (n - 1)));
+  if (b == 0 && tid == 0) a.d[n - 1] = re(xv[n - 1]);
 }
 
 // ---- stage 2: divide and conquer on the tridiagonal (FP64) -----------------
@@ -464,11 +573,12 @@ __global__ void __launch_bounds__(kDcThreads) dc_deflate_kernel(DcLevel L, DcWs 
         continue;
       }
       const double zp = sz[prev];
-      const double tau = hypot(zj, zp);
-      const double c = zj / tau, s = -zp / tau;
       const double t = sd[j] - sd[prev];
-      if (fabs(t * c * s) <= tol) {
+      const double tt = zj * zj + zp * zp;  // |t c s| <= tol with c = zj/tau, s = -zp/tau
+      if (fabs(t * zj * zp) <= tol * tt) {
         // close poles: rotate columns (prev, j) so z_prev = 0 and deflate prev
+        const double tau = sqrt(tt);
+        const double c = zj / tau, s = -zp / tau;
         sz[j] = tau;
         sz[prev] = 0.0;
         w.rot_a[b0 + nr] = sc_[prev];
@@ -524,12 +634,16 @@ __global__ void __launch_bounds__(kDcThreads) dc_rotate_kernel(DcLevel L, DcWs w
 // difference d_i - lambda = (d_i - d_K) - tau keeps full relative accuracy.
 // Each step fits psi (poles i <= j) and phi (poles i > j) by c + s/(d - x)
 // through value and slope and takes the root of the fitted two-pole
-// equation, falling back to bisection of the bracket.
-__global__ void __launch_bounds__(128) dc_secular_kernel(DcLevel L, DcWs w) {
+// equation, falling back to bisection of the bracket. One warp per root: the
+// lanes share the sums (every lane ends with the same totals, so the
+// iteration is warp-uniform).
+constexpr int kSecWarps = 4;
+__global__ void __launch_bounds__(32 * kSecWarps) dc_secular_kernel(DcLevel L, DcWs w) {
   const int q = blockIdx.y;
   int b0, n1, m;
   merge_dims(L, q, b0, n1, m);
-  const int j = blockIdx.x * 128 + threadIdx.x;
+  const int j = blockIdx.x * kSecWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const int k = w.cnt[3 * q];
   if (j >= k) return;
   const double *dv = w.nd_d + b0, *zv = w.nd_z + b0;
@@ -541,31 +655,31 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(DcLevel L, DcWs w) {
   if (j + 1 < k) {
     const double gap = dv[j + 1] - dv[j];
     const double mid = 0.5 * gap;
-    double g = rinv;
-    for (int i = 0; i < k; ++i) g += zv[i] * zv[i] / ((dv[i] - dv[j]) - mid);
+    double g = 0.0;
+    for (int i = lane; i < k; i += 32) g += zv[i] * zv[i] / ((dv[i] - dv[j]) - mid);
+    g = rinv + warp_sum(g);
     if (g >= 0.0) {
       K = j;
       lo = 0.0;
       hi = mid;
     } else {
-      K = j + 1;
+      K = j + 1;  // tau relative to d_{j+1}: (d_j - d_{j+1}) + mid = -mid
       lo = -mid;
       hi = 0.0;
-      // bracket in tau relative to d_{j+1}: (d_j - d_{j+1}) + mid = -mid
     }
   } else {
     double zz = 0.0;
-    for (int i = 0; i < k; ++i) zz += zv[i] * zv[i];
+    for (int i = lane; i < k; i += 32) zz += zv[i] * zv[i];
     lo = 0.0;
-    hi = rho * zz;
+    hi = rho * warp_sum(zz);
   }
   const double dK = dv[K];
-  const double dj = dv[j] - dK;                             // pole j relative to the origin
-  const double dj1 = (j + 1 < k) ? dv[j + 1] - dK : 0.0;    // pole j+1 (unused for the last root)
+  const double dj = dv[j] - dK;                           // pole j relative to the origin
+  const double dj1 = (j + 1 < k) ? dv[j + 1] - dK : 0.0;  // pole j+1 (unused for the last root)
   double tau = 0.5 * (lo + hi);
   for (int it = 0; it < 100; ++it) {
     double psi = 0.0, phi = 0.0, dpsi = 0.0, dphi = 0.0;
-    for (int i = 0; i < k; ++i) {
+    for (int i = lane; i < k; i += 32) {
       const double dl = (dv[i] - dK) - tau;
       const double t = zv[i] / dl;
       if (i <= j) {
@@ -576,6 +690,10 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(DcLevel L, DcWs w) {
         dphi += t * t;
       }
     }
+    psi = warp_sum(psi);
+    phi = warp_sum(phi);
+    dpsi = warp_sum(dpsi);
+    dphi = warp_sum(dphi);
     const double g = rinv + psi + phi;
     if (g == 0.0) break;
     if (g < 0.0) lo = tau;
@@ -588,11 +706,11 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(DcLevel L, DcWs w) {
     double next;
     if (j + 1 < k) {
       const double Dj1 = dj1 - tau;
-      const double s = dpsi * Dj * Dj, S = dphi * Dj1 * Dj1;
-      const double C = rinv + (psi - dpsi * Dj) + (phi - dphi * Dj1);
-      // C + s/(dj - x) + S/(dj1 - x) = 0; with u = x - tau:
-      // C (Dj - u)(Dj1 - u) + s (Dj1 - u) + S (Dj - u) = 0
-      const double qa = C, qb = -(C * (Dj + Dj1) + s + S), qc = C * Dj * Dj1 + s * Dj1 + S * Dj;
+      const double sj = dpsi * Dj * Dj, sj1 = dphi * Dj1 * Dj1;
+      const double Cm = rinv + (psi - dpsi * Dj) + (phi - dphi * Dj1);
+      // Cm + sj/(dj - x) + sj1/(dj1 - x) = 0; with u = x - tau:
+      // Cm (Dj - u)(Dj1 - u) + sj (Dj1 - u) + sj1 (Dj - u) = 0
+      const double qa = Cm, qb = -(Cm * (Dj + Dj1) + sj + sj1), qc = Cm * Dj * Dj1 + sj * Dj1 + sj1 * Dj;
       double u = NAN;
       if (qa == 0.0) {
         if (qb != 0.0) u = -qc / qb;
@@ -606,34 +724,36 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(DcLevel L, DcWs w) {
       }
       next = tau + u;
     } else {
-      const double s = dpsi * Dj * Dj;
-      const double C = rinv + (psi - dpsi * Dj) + phi;
-      next = C > 0.0 ? dj + s / C : NAN;  // C + s/(dj - x) = 0
+      const double sj = dpsi * Dj * Dj;
+      const double Cm = rinv + (psi - dpsi * Dj) + phi;
+      next = Cm > 0.0 ? dj + sj / Cm : NAN;  // Cm + sj/(dj - x) = 0
     }
     tau = (next > lo && next < hi) ? next : 0.5 * (lo + hi);
   }
-  for (int i = 0; i < k; ++i) del[i] = (dv[i] - dK) - tau;
-  w.nd_lam[b0 + j] = dK + tau;
+  for (int i = lane; i < k; i += 32) del[i] = (dv[i] - dK) - tau;
+  if (lane == 0) w.nd_lam[b0 + j] = dK + tau;
 }
 
 // Gu-Eisenstat: zhat_i^2 = (lambda_i - d_i)/rho * prod_{j != i} (lambda_j - d_i)/(d_j - d_i),
-// the z for which the computed roots are exact; sign from z.
-__global__ void __launch_bounds__(128) dc_zhat_kernel(DcLevel L, DcWs w) {
+// the z for which the computed roots are exact; sign from z. One warp per i
+// (lane partial products, then a xor-butterfly product).
+__global__ void __launch_bounds__(32 * kSecWarps) dc_zhat_kernel(DcLevel L, DcWs w) {
   const int q = blockIdx.y;
   int b0, n1, m;
   merge_dims(L, q, b0, n1, m);
-  const int i = blockIdx.x * 128 + threadIdx.x;
+  const int i = blockIdx.x * kSecWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   const int k = w.cnt[3 * q];
   if (i >= k) return;
   const double *dv = w.nd_d + b0;
   const double rho = 2.0 * fabs(w.ee[b0 + n1 - 1]);
   const double *del = w.DEL + merge_off(L, b0);
-  double prod = -del[(std::size_t)i * m + i] / rho;
-  for (int j = 0; j < k; ++j) {
-    if (j == i) continue;
-    prod *= -del[(std::size_t)j * m + i] / (dv[j] - dv[i]);
-  }
-  w.zh[b0 + i] = copysign(sqrt(fmax(prod, 0.0)), w.nd_z[b0 + i]);
+  double prod = 1.0;
+  for (int j = lane; j < k; j += 32)
+    prod *= (j == i) ? -del[(std::size_t)i * m + i] / rho : -del[(std::size_t)j * m + i] / (dv[j] - dv[i]);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) prod *= __shfl_xor_sync(0xffffffffu, prod, o);
+  if (lane == 0) w.zh[b0 + i] = copysign(sqrt(fmax(prod, 0.0)), w.nd_z[b0 + i]);
 }
 
 // Place every eigenpair of the merge at its eigenvalue's rank: the
@@ -750,9 +870,9 @@ cudaError_t stedc_run(cudaStream_t s, int n, const double *d, const double *e, D
     if ((err = launched()) != cudaSuccess) return err;
     dc_rotate_kernel<<<dim3((mmax + kDcThreads - 1) / kDcThreads, nm), kDcThreads, 0, s>>>(L, w);
     if ((err = launched()) != cudaSuccess) return err;
-    dc_secular_kernel<<<dim3((mmax + 127) / 128, nm), 128, 0, s>>>(L, w);
+    dc_secular_kernel<<<dim3((mmax + kSecWarps - 1) / kSecWarps, nm), 32 * kSecWarps, 0, s>>>(L, w);
     if ((err = launched()) != cudaSuccess) return err;
-    dc_zhat_kernel<<<dim3((mmax + 127) / 128, nm), 128, 0, s>>>(L, w);
+    dc_zhat_kernel<<<dim3((mmax + kSecWarps - 1) / kSecWarps, nm), 32 * kSecWarps, 0, s>>>(L, w);
     if ((err = launched()) != cudaSuccess) return err;
     dc_vectors_kernel<<<dim3((mmax + kDcThreads / 32 - 1) / (kDcThreads / 32), nm), kDcThreads, 0, s>>>(L, w);
     if ((err = launched()) != cudaSuccess) return err;
@@ -791,13 +911,22 @@ cudaError_t stedc_run(cudaStream_t s, int n, const double *d, const double *e, D
 // ---- stage 3: back-transformation U = Q Z (compact WY blocks) --------------
 constexpr int kWyBlock = 64;
 
+// All blocks' V (mrows x kb, ld mrows) and V^H (kb x mrows, ld kb), packed
+// block after block: block bi starts at 64 (bi (n-1) - 64 bi (bi-1) / 2).
+__host__ __device__ __forceinline__ std::size_t wy_off(int n, int bi) {
+  return (std::size_t)kWyBlock * ((std::size_t)bi * (n - 1) - (std::size_t)kWyBlock * bi * (bi - 1) / 2);
+}
+
 template <typename C>
-__global__ void wy_build_kernel(int n, int j0, int kb, const C *__restrict__ W, const C *__restrict__ tau,
-                                const C *__restrict__ vsc, C *__restrict__ V, C *__restrict__ VH) {
-  const int mrows = n - j0 - 1;
+__global__ void wy_build_kernel(int n, const C *__restrict__ W, const C *__restrict__ tau, const C *__restrict__ vsc,
+                                C *__restrict__ Vall, C *__restrict__ VHall) {
+  const int bi = blockIdx.z, j0 = bi * kWyBlock;
+  const int kb = min(kWyBlock, n - 1 - j0), mrows = n - j0 - 1;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y;
-  if (r >= mrows) return;
+  if (r >= mrows || jj >= kb) return;
+  C *V = Vall + wy_off(n, bi);
+  C *VH = VHall + wy_off(n, bi);
   const int j = j0 + jj, row = j0 + 1 + r;
   C v = from_re<C>(0.0);
   if (!is_zero(tau[j])) {
@@ -808,24 +937,44 @@ __global__ void wy_build_kernel(int n, int j0, int kb, const C *__restrict__ W, 
   VH[(std::size_t)r * kb + jj] = cj(v);
 }
 
-// T (kb x kb, upper triangular) with H_j0 ... H_{j0+kb-1} = I - V T V^H:
-// T(i,i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i), G = V^H V.
+// T (kb x kb, upper triangular) of every block (one CTA each) with
+// H_j0 ... H_{j0+kb-1} = I - V T V^H: T(i,i) = tau_i,
+// T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i), G = V^H V. G and T live in
+// shared memory (2 kb^2 elements); thread r owns row r.
 template <typename C>
-__global__ void wy_t_kernel(int kb, const C *__restrict__ tau, const C *__restrict__ G, C *__restrict__ T) {
+__global__ void wy_t_kernel(int n, const C *__restrict__ tau, const C *__restrict__ Gall, C *__restrict__ Tall) {
+  extern __shared__ __align__(16) unsigned char wy_smem[];
+  const int bi = blockIdx.x, j0 = bi * kWyBlock;
+  const int kb = min(kWyBlock, n - 1 - j0);
+  const C *G = Gall + (std::size_t)bi * kWyBlock * kWyBlock;
+  C *T = Tall + (std::size_t)bi * kWyBlock * kWyBlock;
+  C *Gs = reinterpret_cast<C *>(wy_smem);
+  C *Ts = Gs + kb * kb;
   const int r = threadIdx.x;
+  for (int idx = r; idx < kb * kb; idx += blockDim.x) {
+    Gs[idx] = G[idx];
+    Ts[idx] = from_re<C>(0.0);
+  }
+  __syncthreads();
   for (int i = 0; i < kb; ++i) {
-    C s = from_re<C>(0.0);
-    if (r < i)
-      for (int l = r; l < i; ++l) s = fmac(T[(std::size_t)l * kb + r], G[(std::size_t)i * kb + l], s);
-    __syncthreads();
-    if (r < kb) T[(std::size_t)i * kb + r] = r < i ? neg(mul(tau[i], s)) : (r == i ? tau[i] : from_re<C>(0.0));
+    if (r < i) {
+      C sacc = from_re<C>(0.0);
+      for (int l = r; l < i; ++l) sacc = fmac(Ts[l * kb + r], Gs[i * kb + l], sacc);
+      Ts[i * kb + r] = neg(mul(tau[j0 + i], sacc));  // column i: no thread reads it this round
+    } else if (r == i) {
+      Ts[i * kb + i] = tau[j0 + i];
+    }
     __syncthreads();
   }
+  for (int idx = r; idx < kb * kb; idx += blockDim.x) T[idx] = Ts[idx];
 }
+
+constexpr int kSplitMax = 16;  // K slices of the skinny back-transform products
 
 template <typename C>
 struct BtWs {
-  C *V, *VH, *G, *T, *Wm, *Wm2;
+  C *Vall, *VHall;  // aliases of the divide-and-conquer scratch (free by then)
+  C *G, *T, *Wm, *Wm2, *part;
 };
 
 __global__ void real_to_c_kernel(std::size_t count, const double *__restrict__ Z, double *__restrict__ U) {
@@ -847,17 +996,34 @@ cudaError_t back_transform(cudaStream_t s, int n, const C *W, const C *tau, cons
   real_to_c_kernel<<<(int)std::min<std::size_t>((nn + 255) / 256, 8 * 148), 256, 0, s>>>(nn, Z, U);
   if ((err = launched()) != cudaSuccess) return err;
   if (n < 2) return cudaSuccess;
-  for (int j0 = ((n - 2) / kWyBlock) * kWyBlock; j0 >= 0; j0 -= kWyBlock) {
-    const int j1 = std::min(j0 + kWyBlock, n - 1), kb = j1 - j0, mrows = n - j0 - 1;
-    wy_build_kernel<C><<<dim3((mrows + 127) / 128, kb), 128, 0, s>>>(n, j0, kb, W, tau, vsc, bt.V, bt.VH);
-    if ((err = launched()) != cudaSuccess) return err;
-    if ((err = gemm_nn<C>(s, kb, kb, mrows, 1.0, bt.VH, kb, bt.V, mrows, 0.0, bt.G, kb)) != cudaSuccess) return err;
-    wy_t_kernel<C><<<1, kWyBlock, 0, s>>>(kb, tau + j0, bt.G, bt.T);
-    if ((err = launched()) != cudaSuccess) return err;
+  const int nblk = (n - 1 + kWyBlock - 1) / kWyBlock;
+  // every block's V, V^H, Gram matrix and T first: none depends on U
+  wy_build_kernel<C><<<dim3((n + 126) / 128, kWyBlock, nblk), 128, 0, s>>>(n, W, tau, vsc, bt.Vall, bt.VHall);
+  if ((err = launched()) != cudaSuccess) return err;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int j0 = bi * kWyBlock, kb = std::min(kWyBlock, n - 1 - j0), mrows = n - j0 - 1;
+    const C *V = bt.Vall + wy_off(n, bi), *VH = bt.VHall + wy_off(n, bi);
+    if ((err = gemm_nn_splitk<C>(s, kb, kb, mrows, 1.0, VH, kb, V, mrows, 0.0,
+                                 bt.G + (std::size_t)bi * kWyBlock * kWyBlock, kb, bt.part, kSplitMax)) !=
+        cudaSuccess)
+      return err;
+  }
+  if ((err = cudaFuncSetAttribute(wy_t_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  2 * kWyBlock * kWyBlock * (int)sizeof(C))) != cudaSuccess)
+    return err;
+  wy_t_kernel<C><<<nblk, kWyBlock, 2 * (std::size_t)kWyBlock * kWyBlock * sizeof(C), s>>>(n, tau, bt.G, bt.T);
+  if ((err = launched()) != cudaSuccess) return err;
+  // U = (I - V_0 T_0 V_0^H) ... (I - V_last T_last V_last^H) Z, the last block first
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int j0 = bi * kWyBlock, kb = std::min(kWyBlock, n - 1 - j0), mrows = n - j0 - 1;
+    const C *V = bt.Vall + wy_off(n, bi), *VH = bt.VHall + wy_off(n, bi);
+    const C *T = bt.T + (std::size_t)bi * kWyBlock * kWyBlock;
     C *Us = U + j0 + 1;
-    if ((err = gemm_nn<C>(s, kb, n, mrows, 1.0, bt.VH, kb, Us, n, 0.0, bt.Wm, kb)) != cudaSuccess) return err;
-    if ((err = gemm_nn<C>(s, kb, n, kb, 1.0, bt.T, kb, bt.Wm, kb, 0.0, bt.Wm2, kb)) != cudaSuccess) return err;
-    if ((err = gemm_nn<C>(s, mrows, n, kb, -1.0, bt.V, mrows, bt.Wm2, kb, 1.0, Us, n)) != cudaSuccess) return err;
+    if ((err = gemm_nn_splitk<C>(s, kb, n, mrows, 1.0, VH, kb, Us, n, 0.0, bt.Wm, kb, bt.part, kSplitMax)) !=
+        cudaSuccess)
+      return err;
+    if ((err = gemm_nn<C>(s, kb, n, kb, 1.0, T, kb, bt.Wm, kb, 0.0, bt.Wm2, kb)) != cudaSuccess) return err;
+    if ((err = gemm_nn<C>(s, mrows, n, kb, -1.0, V, mrows, bt.Wm2, kb, 1.0, Us, n)) != cudaSuccess) return err;
   }
   return cudaSuccess;
 }
@@ -865,7 +1031,7 @@ cudaError_t back_transform(cudaStream_t s, int n, const C *W, const C *tau, cons
 // ---- workspace ---------------------------------------------------------------
 template <typename C>
 struct HermWs {
-  C *W, *U, *M, *tau, *vsc, *p;
+  C *W, *U, *M, *tau, *vsc, *p, *vec;
   double *d, *e, *lam;
   DcWs dc;
   BtWs<C> bt;
@@ -884,7 +1050,8 @@ HermWs<C> carve_herm(void *base, int n, bool want_expm, std::size_t *bytes) {
   w.M = want_expm ? L.take<C>(nn) : nullptr;
   w.tau = L.take<C>(nv);
   w.vsc = L.take<C>(nv);
-  w.p = L.take<C>(nv);
+  w.p = L.take<C>(2 * nv);
+  w.vec = L.take<C>(kTrdVecs * nv * kTrdMaxGrid);
   w.d = L.take<double>(nv);
   w.e = L.take<double>(nv);
   w.lam = L.take<double>(nv);
@@ -900,13 +1067,16 @@ HermWs<C> carve_herm(void *base, int n, bool want_expm, std::size_t *bytes) {
   for (int **p : iv) *p = L.take<int>(nv);
   c.cnt = L.take<int>(3 * nv);
   c.sc = L.take<double>(1);
-  const std::size_t nb = kWyBlock;
-  w.bt.V = L.take<C>(nv * nb);
-  w.bt.VH = L.take<C>(nv * nb);
-  w.bt.G = L.take<C>(nb * nb);
-  w.bt.T = L.take<C>(nb * nb);
+  const std::size_t nb = kWyBlock, nblk = (nv + nb - 1) / nb;
+  // V and V^H of all blocks (about n^2 / 2 elements each) reuse Za|Zb and
+  // DEL|UF: the back-transform starts by copying Z out of them
+  w.bt.Vall = reinterpret_cast<C *>(c.Za);
+  w.bt.VHall = reinterpret_cast<C *>(c.DEL);
+  w.bt.G = L.take<C>(nblk * nb * nb);
+  w.bt.T = L.take<C>(nblk * nb * nb);
   w.bt.Wm = L.take<C>(nv * nb);
   w.bt.Wm2 = L.take<C>(nv * nb);
+  w.bt.part = L.take<C>(kSplitMax * nv * nb);
   w.bar = L.take<unsigned>(1);
   w.err = L.take<int>(1);
   w.amax = L.take<unsigned long long>(1);
@@ -916,6 +1086,27 @@ HermWs<C> carve_herm(void *base, int n, bool want_expm, std::size_t *bytes) {
 
 __global__ void herm_status_kernel(int n, const int *__restrict__ err, int *__restrict__ info) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *info = *err ? n + 1 : 0;
+}
+
+constexpr std::size_t kTrdResidentBytes = 220 * 1024;
+
+template <typename C, bool kRes>
+cudaError_t launch_hetrd(cudaStream_t s, int G, std::size_t smem, int n, HermWs<C> &w) {
+  cudaError_t err;
+  int per_sm = 0;
+  if ((err = cudaFuncSetAttribute(hetrd_kernel<C, kRes>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+      cudaSuccess)
+    return err;
+  if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel<C, kRes>, kTrdThreads, smem)) !=
+      cudaSuccess)
+    return err;
+  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+  TrdArgs<C> ta{n, w.W, w.d, w.e, w.tau, w.vsc, w.p, w.vec, w.bar, w.err};
+  void *args[] = {&ta};
+  if ((err = cudaLaunchCooperativeKernel((const void *)hetrd_kernel<C, kRes>, dim3(G), dim3(kTrdThreads), args, smem,
+                                         s)) != cudaSuccess)
+    return err;
+  return launched();
 }
 
 // Eigenvalues (FP64, ascending, of the scaled matrix) into w.lam and
@@ -933,22 +1124,14 @@ cudaError_t heev_run(cudaStream_t s, int upper, int n, const T *A, int lda, Herm
   herm_fill_kernel<T, C><<<dim3((n + 127) / 128, std::min(n, 1024)), 128, 0, s>>>(n, A, lda, upper, w.amax, w.W);
   if ((err = launched()) != cudaSuccess) return err;
   // tridiagonal reduction: one cooperative launch
-  int per_sm = 0;
-  const int G = std::max(1, std::min(sm_count(), (n + 7) / 8));
-  std::size_t smem = (2 * kTrdChunk + (std::size_t)((n + G - 1) / G)) * sizeof(C);
-  if ((err = cudaFuncSetAttribute(hetrd_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+  const int G = std::max(1, std::min(std::min(sm_count(), kTrdMaxGrid), (n + 7) / 8));
+  const std::size_t ncmax = (std::size_t)((n + G - 1) / G);
+  const std::size_t base = std::max<std::size_t>(ncmax, kTrdWarps) * sizeof(C);
+  const std::size_t resident = base + (ncmax + kTrdVecs) * (std::size_t)n * sizeof(C);
+  const bool use_res = resident <= kTrdResidentBytes;
+  if ((err = use_res ? launch_hetrd<C, true>(s, G, resident, n, w) : launch_hetrd<C, false>(s, G, base, n, w)) !=
       cudaSuccess)
     return err;
-  if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hetrd_kernel<C>, kTrdThreads, smem)) !=
-      cudaSuccess)
-    return err;
-  if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
-  TrdArgs<C> ta{n, w.W, w.d, w.e, w.tau, w.vsc, w.p, w.bar, w.err};
-  void *args[] = {&ta};
-  if ((err = cudaLaunchCooperativeKernel((const void *)hetrd_kernel<C>, dim3(G), dim3(kTrdThreads), args, smem, s)) !=
-      cudaSuccess)
-    return err;
-  if ((err = launched()) != cudaSuccess) return err;
   double *Z = nullptr;
   if ((err = stedc_run(s, n, w.d, w.e, w.dc, w.lam, &Z)) != cudaSuccess) return err;
   return back_transform<C>(s, n, w.W, w.tau, w.vsc, Z, w.U, w.bt);

@@ -59,6 +59,14 @@ template <typename T>
 cudaError_t gemm_nn(cudaStream_t s, int M, int N, int K, double alpha, const T *A, int lda,
                     const T *B, int ldb, double beta, T *C, int ldc);
 
+// The same product with K split into slices computed in parallel (blockIdx.z)
+// into `partial` (slices * M * N elements, ld M) and summed in slice order:
+// for skinny products whose few output tiles would leave most SMs idle.
+// At most max_splits slices of a 64-multiple of K; FP64 types only.
+template <typename T>
+cudaError_t gemm_nn_splitk(cudaStream_t s, int M, int N, int K, double alpha, const T *A, int lda, const T *B,
+                           int ldb, double beta, T *C, int ldc, T *partial, int max_splits);
+
 // FP32 GEMM on the tcgen05 tensor cores as split-BF16 part products (terms =
 // 3 or 6), accumulated in FP32 TMEM; needs tc_gemm_workspace_bytes of scratch.
 std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms);
