@@ -58,6 +58,14 @@ CONFIGS = {
     "expm_herm_c128_1024": dict(n=1024, suf="z", norm=50.0, gen="herm", entry="expm_herm",
                                 desc="complex128 1024x1024 Hermitian H=(X+X^H)/2 (GUE), ||H||_1=50, "
                                      "expm_herm (eigendecomposition route)"),
+    "geodesic_c128_1024_p6": dict(kind="geodesic", n=1024, suf="z", samples=6, scale=10.0, step=0.1,
+                                  desc="cg_unitary geodesic trial points W_j = exp(j mu H) W, j = 1..5 "
+                                       "(Table 1 search, P + 1 = 6 samples), complex128 1024x1024, W "
+                                       "unitary (QR of complex N(0,1)), H skew-Hermitian with ||H||_2 = 10, "
+                                       "mu = 0.1"),
+    "geodesic_c128_1024_dft31": dict(kind="geodesic", n=1024, suf="z", samples=31, scale=10.0, step=0.02,
+                                     desc="the same with the Table 2 (DFT) sample count, 31 samples, "
+                                          "mu = 0.02"),
     "expm_batched_f32_8192": dict(kind="batched", count=8192, nmax=256, suf="s",
                                   desc="8192 float32 matrices, n uniform on {16,32,...,256}, "
                                        "N(0,1) rescaled to ||A||_1 log-uniform in [0.1,100]"),
@@ -120,6 +128,17 @@ def vjp_pair(n, norm, seed):
     a = a * (norm / np.abs(a).sum(axis=0).max())
     g = rng.standard_normal((n, n))
     return a, g
+
+
+def geodesic_inputs(cfg, seed=20261205):
+    """W unitary (QR of complex N(0,1)), H skew-Hermitian rescaled to spectral norm `scale`."""
+    rng = np.random.default_rng(seed)
+    n = cfg["n"]
+    w, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    y = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    h = (y - y.conj().T) / 2
+    h = h * (cfg["scale"] / np.linalg.norm(h, 2))
+    return np.asfortranarray(w), np.asfortranarray(h)
 
 
 def vjp_flops(n, m, s):
@@ -249,6 +268,15 @@ def run_reference(args, cfg):
             for m in mats:
                 O.expm(m, single=single)
         sample = "the first 32 matrices of the batch per step"
+        plan_info = None
+    elif kind == "geodesic":
+        w, hmat = geodesic_inputs(cfg)
+        per_step, unit = 1, "search/s"
+
+        def one():
+            O.geodesic_points(w, hmat, cfg["step"], cfg["samples"])
+        sample = ("the trial points of one search per step (general expm, then the power chain and "
+                  "products with numpy's threaded BLAS)")
         plan_info = None
     elif kind == "vjp":
         k = 1 if cfg["n"] > 512 else 8
@@ -896,6 +924,133 @@ def run_vjp(args, cfg):
         dist.destroy_process_group()
 
 
+def run_geodesic(args, cfg):
+    """One step = the trial points of one line search through
+    calaman_geodesic_points_z (one Hermitian eigensolve, one wide product).
+    Replicas under torchrun."""
+    torch, world, rank, local, dev, dist = _init_dist()
+    from calaman_g_b200 import capi
+
+    lib = capi.load()
+    n, num = cfg["n"], cfg["samples"]
+    w, hmat = geodesic_inputs(cfg)
+    host_w = torch.from_numpy(np.ascontiguousarray(w.T).reshape(-1)).pin_memory()
+    host_h = torch.from_numpy(np.ascontiguousarray(hmat.T).reshape(-1)).pin_memory()
+    host_o = torch.empty((num - 1) * n * n, dtype=torch.complex128).pin_memory()
+    dW, dH = host_w.to(dev), host_h.to(dev)
+    dO = torch.empty((num - 1) * n * n, dtype=torch.complex128, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    h = ctypes.c_void_p()
+    assert lib.calamanCreate(ctypes.byref(h)).ok
+    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
+    nb = ctypes.c_size_t()
+    assert lib.calaman_geodesic_points_bufferSize_z(h, n, num, ctypes.byref(nb)).ok
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    info = torch.zeros(1, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        st = lib.calaman_geodesic_points_z(h, h, ctypes.c_void_p(stream.cuda_stream), n,
+                                           ctypes.c_void_p(dW.data_ptr()), n, ctypes.c_void_p(dH.data_ptr()), n,
+                                           float(cfg["step"]), num, ctypes.c_void_p(dO.data_ptr()),
+                                           ctypes.c_void_p(work.data_ptr()), nb.value,
+                                           ctypes.cast(info.data_ptr(), capi.c_int_p))
+        if not st.ok:
+            raise RuntimeError(f"geodesic_points failed: {st!r}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.calamanGetLaunchCount()
+    assert lib.calamanSetKernelTiming(h, 1).ok
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                starts[i].record(stream)
+                step()
+                ends[i].record(stream)
+        torch.cuda.synchronize()
+        launches = lib.calamanGetLaunchCount() - launches0
+        kt = capi.KernelTiming()
+        assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
+        lib.calamanSetKernelTiming(h, 0)
+        total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+        e2e_ms = 0.0
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a_ev.record(stream)
+                dW.copy_(host_w, non_blocking=True)
+                dH.copy_(host_h, non_blocking=True)
+                step()
+                host_o.copy_(dO, non_blocking=True)
+                b_ev.record(stream)
+                b_ev.synchronize()
+                e2e_ms += a_ev.elapsed_time(b_ev)
+    torch.cuda.synchronize()
+    if info.item() != 0:
+        raise RuntimeError(f"geodesic_points reported info {info.item()}")
+    total_ms, e2e_ms = _max_over_ranks(torch, dist, dev, [total_ms, e2e_ms])
+    value = world * args.steps / (total_ms * 1e-3)
+    e2e_value = world * args.steps / (e2e_ms * 1e-3)
+    if rank == 0:
+        peak = measure_fp64_peak(torch, dev, True)
+        achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
+        baseline, acc = None, {}
+        if world == 1 and not args.no_cpu:
+            from oracle import oracle as O
+
+            cores = os.cpu_count() or 1
+            O.set_threads(cores)
+            t0 = time.perf_counter()
+            ref = O.geodesic_points(w, hmat, cfg["step"], num)
+            el = time.perf_counter() - t0
+            baseline = {"value": 1.0 / el, "unit": "search/s", "cores": cores, "kind": "port",
+                        "sample": f"one search's trial points in the reference's order (general expm, "
+                                  f"power chain, products), {el:.1f} s, {cores} threads"}
+            got = host_o.numpy()
+            worst = 0.0
+            for j, r in enumerate(ref):
+                g = got[j * n * n:(j + 1) * n * n].reshape(n, n).T
+                worst = max(worst, float(np.linalg.norm(g - r) / np.linalg.norm(r)))
+            acc["max_rel_frob_vs_oracle"] = worst
+        flops = herm_flops(n, True) - 8.0 * n ** 3 + 8.0 * n ** 3 * (1 + (num - 1))
+        line = {
+            "metric": METRIC, "value": value, "unit": "search/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.config, "desc": cfg["desc"], "samples": num,
+                       "l2": "flushed before every timed step (256 MiB write, untimed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "tflops": flops * value / world / 1e12,
+            "algorithmic_flops_per_search": flops,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if achieved else None, "traffic": None,
+                         "kernel": "dense products (every GEMM launch in the timed steps)",
+                         "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
+                         "peak_source": "cuBLAS complex128 GEMM 4096^3 measured in this run"},
+            "cpu_baseline": baseline,
+            "e2e": {"value": e2e_value, "unit": "search/s", "h2d_bytes_per_step": 2 * n * n * 16,
+                    "d2h_bytes_per_step": (num - 1) * n * n * 16},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "accuracy": acc,
+        }
+        print(json.dumps(line), flush=True)
+    lib.calamanDestroy(h)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -913,6 +1068,8 @@ def main():
         run_batched(args, cfg)
     elif kind == "vjp":
         run_vjp(args, cfg)
+    elif kind == "geodesic":
+        run_geodesic(args, cfg)
     else:
         run_ours(args, cfg)
 

@@ -169,6 +169,12 @@ for _suf in ("s", "d", "c", "z"):
     SIGNATURES[f"calaman_heevd_bufferSize_{_suf}"] = (Status, [c_int, c_int, c_size_t_p])
     SIGNATURES[f"calaman_heevd_{_suf}"] = (Status, [c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
                                                    c_void_p, c_size_t, c_int_p])
+for _suf in ("s", "d", "c", "z"):
+    # geodesic points: blas, solver, stream, n, W, ldw, H, ldh, step, num_samples, Wout, work, bytes, info
+    SIGNATURES[f"calaman_geodesic_points_bufferSize_{_suf}"] = (Status, [_H, c_int, c_int, c_size_t_p])
+    SIGNATURES[f"calaman_geodesic_points_{_suf}"] = (Status, [_H, _H, c_void_p, c_int, c_void_p, c_int,
+                                                             c_void_p, c_int, c_double, c_int, c_void_p,
+                                                             c_void_p, c_size_t, c_int_p])
 for _suf, _real in (("s", c_float), ("d", c_double)):
     # lacn2: blas, n, v, x, work, bytes, est (host), kase (host), isave[3] (host)
     SIGNATURES[f"calaman_lacn2_bufferSize_{_suf}"] = (c_size_t, [c_int])

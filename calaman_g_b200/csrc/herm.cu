@@ -168,6 +168,10 @@ __device__ __forceinline__ double herm_sigma(const unsigned long long *amax) {
   return 1.0;
 }
 
+__device__ __forceinline__ double2 to_c2(float x) { return make_double2((double)x, 0.0); }
+__device__ __forceinline__ double2 to_c2(double x) { return make_double2(x, 0.0); }
+__device__ __forceinline__ double2 to_c2(float2 x) { return make_double2(x.x, x.y); }
+__device__ __forceinline__ double2 to_c2(double2 x) { return x; }
 __device__ __forceinline__ double to_c(float x) { return (double)x; }
 __device__ __forceinline__ double to_c(double x) { return x; }
 __device__ __forceinline__ double2 to_c(float2 x) { return make_double2(x.x, x.y); }
@@ -1227,6 +1231,147 @@ calamanStatus_t heevd_api(calamanStream_t stream, int uplo, int n, T *A, int lda
   return ok_status();
 }
 
+// ---- geodesic trial points: W_j = exp(j step H) W ---------------------------
+// The sampling sweep of the cg_unitary line searches
+// (src/cg_unitary/geodesic_search.cppm:338-420) evaluates the cost gradient at
+// W_j = exp(j mu H) W, j = 1 .. N-1, H in u(n) (skew-Hermitian), and forms the
+// rotations as R_1 = expm(mu H), R_j = R_{j-1} R_1 -- N-2 dependent products,
+// then N-1 more for R_j W. Here H = -i Hh with Hh = i H Hermitian, so
+// exp(t H) = U diag(exp(-i t w)) U^H from ONE Hermitian eigensolve, and all
+// trial points come out of one wide product:
+//   [W_1 | ... | W_{N-1}] = U [D_1 Y | ... | D_{N-1} Y],  Y = U^H W,
+// D_j = diag(exp(-i j mu w)): no error accumulates along j, and the N-1
+// products become one GEMM with N-1 times the columns. Real tiers (H skew-
+// symmetric, W orthogonal) run through the complex path and keep real parts.
+
+// Wt = i H, Hermitian, from H's lower triangle (its strictly upper part is not
+// read); the diagonal keeps i H_jj's real part.
+template <typename T>
+__global__ void geo_fill_kernel(int n, const T *__restrict__ H, int ldh, double2 *__restrict__ Wt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const double2 h = i >= j ? to_c2(H[(std::size_t)j * ldh + i]) : cj(to_c2(H[(std::size_t)i * ldh + j]));
+    // lower entry i H_ij; the mirrored upper entry is conj(i H_ji) = -i conj(H_ji)
+    double2 v = i >= j ? make_double2(-h.y, h.x) : make_double2(h.y, -h.x);
+    if (i == j) v.y = 0.0;
+    Wt[(std::size_t)j * n + i] = v;
+  }
+}
+
+template <typename T>
+__global__ void geo_load_kernel(int n, const T *__restrict__ W, int ldw, double2 *__restrict__ Wc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = blockIdx.y; j < n; j += gridDim.y) Wc[(std::size_t)j * n + i] = to_c2(W[(std::size_t)j * ldw + i]);
+}
+
+// B (n x (N-1) n): block j-1 = D_j Y, D_j = diag(exp(-i j mu w_r)), w = lam / sigma
+__global__ void geo_phase_kernel(int n, int nsteps, double mu, const double *__restrict__ lam,
+                                 const unsigned long long *__restrict__ amax, const double2 *__restrict__ Y,
+                                 double2 *__restrict__ B) {
+  const double sg = herm_sigma(amax);
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const double wr = lam[r] / sg;
+  for (int col = blockIdx.y; col < nsteps * n; col += gridDim.y) {
+    const int j = col / n + 1, c = col - (j - 1) * n;
+    double sn, cs;
+    sincos(-(double)j * mu * wr, &sn, &cs);
+    B[(std::size_t)col * n + r] = mul(make_double2(cs, sn), Y[(std::size_t)c * n + r]);
+  }
+}
+
+template <typename T>
+__global__ void geo_real_out_kernel(std::size_t count, const double2 *__restrict__ Z, T *__restrict__ out) {
+  for (std::size_t i = blockIdx.x * (std::size_t)blockDim.x + threadIdx.x; i < count;
+       i += (std::size_t)gridDim.x * blockDim.x)
+    out[i] = (T)Z[i].x;
+}
+template <typename T>
+__global__ void geo_cplx_out_kernel(std::size_t count, const double2 *__restrict__ Z, T *__restrict__ out) {
+  for (std::size_t i = blockIdx.x * (std::size_t)blockDim.x + threadIdx.x; i < count;
+       i += (std::size_t)gridDim.x * blockDim.x) {
+    T v;
+    v.x = Z[i].x;
+    v.y = Z[i].y;
+    out[i] = v;
+  }
+}
+
+constexpr int kGeoMaxSamples = 64;
+
+struct GeoWs {
+  HermWs<double2> h;
+  double2 *Hh, *Wc, *Y, *B, *Out;
+};
+
+GeoWs carve_geo(void *base, int n, int num_samples, bool direct_out, std::size_t *bytes) {
+  Layout L(base);
+  GeoWs g;
+  const std::size_t nn = (std::size_t)n * n, ns = (std::size_t)(num_samples > 1 ? num_samples - 1 : 1);
+  g.Hh = L.take<double2>(nn);
+  g.Wc = L.take<double2>(nn);
+  g.Y = L.take<double2>(nn);
+  g.B = L.take<double2>(ns * nn);
+  g.Out = direct_out ? nullptr : L.take<double2>(ns * nn);
+  std::size_t hb = 0;
+  g.h = carve_herm<double2>(L.cursor(), n, false, &hb);
+  if (bytes) *bytes = L.used + hb;
+  return g;
+}
+
+template <typename T>
+calamanStatus_t geodesic_api(calamanHandle_t blas, calamanStream_t stream, int n, const T *W, int ldw, const T *H,
+                             int ldh, double mu, int num_samples, T *Wout, void *work, std::size_t lwork,
+                             int *d_info) {
+  constexpr bool kDirect = std::is_same<T, double2>::value;
+  if (n < 1 || n > kMaxDim || ldw < n || ldh < n || W == nullptr || H == nullptr || work == nullptr ||
+      d_info == nullptr || num_samples < 1 || num_samples > kGeoMaxSamples || !std::isfinite(mu) ||
+      (num_samples > 1 && Wout == nullptr))
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  std::size_t need = 0;
+  carve_geo(nullptr, n, num_samples, kDirect, &need);
+  if (lwork < need) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CLM_CUDA(cudaMemsetAsync(d_info, 0, sizeof(int), s));
+  if (num_samples == 1) return ok_status();  // sample 0 is W itself
+  GeoWs g = carve_geo(work, n, num_samples, kDirect, nullptr);
+  TimerScope timing(timer_of(blas));
+  const dim3 grid2((n + 127) / 128, std::min(n, 1024));
+  geo_fill_kernel<T><<<grid2, 128, 0, s>>>(n, H, ldh, g.Hh);
+  CLM_CUDA(launched());
+  geo_load_kernel<T><<<grid2, 128, 0, s>>>(n, W, ldw, g.Wc);
+  CLM_CUDA(launched());
+  CLM_CUDA((heev_run<double2, double2>(s, 0, n, g.Hh, n, g.h)));  // Hh = U diag(lam / sigma) U^H
+  double2 *UH = g.h.W;                                              // the reflectors are spent
+  CLM_CUDA(launch_transpose<double2>(s, n, n, 1.0, g.h.U, n, UH, n, true));
+  CLM_CUDA(gemm_nn<double2>(s, n, n, n, 1.0, UH, n, g.Wc, n, 0.0, g.Y, n));
+  const int steps = num_samples - 1;
+  geo_phase_kernel<<<dim3((n + 127) / 128, std::min(steps * n, 4096)), 128, 0, s>>>(n, steps, mu, g.h.lam, g.h.amax,
+                                                                                   g.Y, g.B);
+  CLM_CUDA(launched());
+  double2 *out = kDirect ? reinterpret_cast<double2 *>(Wout) : g.Out;
+  CLM_CUDA(gemm_nn<double2>(s, n, steps * n, n, 1.0, g.h.U, n, g.B, n, 0.0, out, n));
+  if constexpr (!kDirect) {
+    const std::size_t count = (std::size_t)steps * n * n;
+    const int blocks = (int)std::min<std::size_t>((count + 255) / 256, 8 * 148);
+    if constexpr (elem<T>::complex) geo_cplx_out_kernel<T><<<blocks, 256, 0, s>>>(count, out, Wout);
+    else geo_real_out_kernel<T><<<blocks, 256, 0, s>>>(count, out, Wout);
+    CLM_CUDA(launched());
+  }
+  herm_status_kernel<<<1, 32, 0, s>>>(n, g.h.err, d_info);
+  CLM_CUDA(launched());
+  return ok_status();
+}
+
+template <typename T>
+std::size_t geodesic_bytes(int n, int num_samples) {
+  std::size_t b = 0;
+  carve_geo(nullptr, n, num_samples, std::is_same<T, double2>::value, &b);
+  return b;
+}
+
 }  // namespace
 }  // namespace clm
 
@@ -1259,6 +1404,27 @@ extern "C" {
                                       void *work, size_t lwork, int *d_info) {                              \
     return heevd_api<T>(stream, uplo, n, reinterpret_cast<T *>(A), lda, d_w, work, lwork, d_info);          \
   }
+#define CLM_GEO_API(SUF, T, PT, CPT)                                                                         \
+  calamanStatus_t calaman_geodesic_points_bufferSize_##SUF(calamanSolverHandle_t, int n, int num_samples,      \
+                                                           size_t *bytes) {                                    \
+    if (n < 1 || n > kMaxDim || num_samples < 1 || num_samples > kGeoMaxSamples || bytes == nullptr)            \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                                        \
+    *bytes = geodesic_bytes<T>(n, num_samples);                                                                \
+    return ok_status();                                                                                        \
+  }                                                                                                            \
+  calamanStatus_t calaman_geodesic_points_##SUF(calamanBlasHandle_t blas, calamanSolverHandle_t,               \
+                                                calamanStream_t stream, int n, CPT W, int ldw, CPT H, int ldh,  \
+                                                double step, int num_samples, PT Wout, void *work,             \
+                                                size_t lwork, int *d_info) {                                   \
+    return geodesic_api<T>(blas, stream, n, reinterpret_cast<const T *>(W), ldw, reinterpret_cast<const T *>(H), \
+                           ldh, step, num_samples, reinterpret_cast<T *>(Wout), work, lwork, d_info);          \
+  }
+CLM_GEO_API(s, float, float *, const float *)
+CLM_GEO_API(d, double, double *, const double *)
+CLM_GEO_API(c, float2, void *, const void *)
+CLM_GEO_API(z, double2, void *, const void *)
+#undef CLM_GEO_API
+
 CLM_HERM_API(s, float, float, float *, const float *)
 CLM_HERM_API(d, double, double, double *, const double *)
 CLM_HERM_API(c, float2, float, void *, const void *)

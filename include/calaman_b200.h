@@ -313,6 +313,38 @@ calamanStatus_t calaman_heevd_c(calamanStream_t stream, int uplo, int n, void *d
 calamanStatus_t calaman_heevd_z(calamanStream_t stream, int uplo, int n, void *d_A, int lda, double *d_w,
                                 void *d_work, size_t lwork_bytes, int *d_info);
 
+/* ---- geodesic trial points of the cg_unitary line searches ---------------
+ * The rotation half of calaman::cg_detail::sample_derivative
+ * (src/cg_unitary/geodesic_search.cppm:338-420): for j = 1 .. num_samples-1,
+ * d_Wout block j-1 (n x n, packed, ld n) = exp(j * step * H) * W, with H in
+ * u(n) (skew-Hermitian; skew-symmetric for the real tiers) and W n x n (ldw).
+ * Sample 0 is W itself and is not written. Only H's lower triangle (and the
+ * imaginary part of its diagonal) is read. The reference forms R_1 =
+ * expm(step H) and R_j = R_{j-1} R_1; here exp(t H) comes from one Hermitian
+ * eigensolve of i H and every trial point from one wide product, no error
+ * growing along j. 1 <= num_samples <= 64. Never synchronises; d_info: ONE
+ * device int as for expm_herm. INVALID_VALUE / ALLOC_FAILED as expm. */
+calamanStatus_t calaman_geodesic_points_bufferSize_s(calamanSolverHandle_t h, int n, int num_samples, size_t *bytes);
+calamanStatus_t calaman_geodesic_points_bufferSize_d(calamanSolverHandle_t h, int n, int num_samples, size_t *bytes);
+calamanStatus_t calaman_geodesic_points_bufferSize_c(calamanSolverHandle_t h, int n, int num_samples, size_t *bytes);
+calamanStatus_t calaman_geodesic_points_bufferSize_z(calamanSolverHandle_t h, int n, int num_samples, size_t *bytes);
+calamanStatus_t calaman_geodesic_points_s(calamanBlasHandle_t blas, calamanSolverHandle_t solver, calamanStream_t stream,
+                                          int n, const float *d_W, int ldw, const float *d_H, int ldh, double step,
+                                          int num_samples, float *d_Wout, void *d_work, size_t lwork_bytes,
+                                          int *d_info);
+calamanStatus_t calaman_geodesic_points_d(calamanBlasHandle_t blas, calamanSolverHandle_t solver, calamanStream_t stream,
+                                          int n, const double *d_W, int ldw, const double *d_H, int ldh, double step,
+                                          int num_samples, double *d_Wout, void *d_work, size_t lwork_bytes,
+                                          int *d_info);
+calamanStatus_t calaman_geodesic_points_c(calamanBlasHandle_t blas, calamanSolverHandle_t solver, calamanStream_t stream,
+                                          int n, const void *d_W, int ldw, const void *d_H, int ldh, double step,
+                                          int num_samples, void *d_Wout, void *d_work, size_t lwork_bytes,
+                                          int *d_info);
+calamanStatus_t calaman_geodesic_points_z(calamanBlasHandle_t blas, calamanSolverHandle_t solver, calamanStream_t stream,
+                                          int n, const void *d_W, int ldw, const void *d_H, int ldh, double step,
+                                          int num_samples, void *d_Wout, void *d_work, size_t lwork_bytes,
+                                          int *d_info);
+
 /* ---- lacn2: 1-norm estimate by reverse communication (LAPACK xLACN2) ----
  * src/lapack/lacn2/interface.cppm:85-200 (calaman::lacn2_bufferSize,
  * calaman::lacn2). Real only (s/d), as the reference. Start with *kase = 0;

@@ -242,6 +242,33 @@ Status heevd(cudaStream_t stream, FillMode uplo, int n, T *d_A, int lda, real_t<
     return calaman_heevd_z(stream, u, n, d_A, lda, d_w, d_work, lwork_bytes, d_info);
 }
 
+// ---- geodesic trial points (src/cg_unitary/geodesic_search.cppm:338-420) ----------
+template <typename T> Status geodesic_points_bufferSize(SolverHandle h, int n, int num_samples, std::size_t *bytes) {
+  if constexpr (std::is_same_v<T, float>) return calaman_geodesic_points_bufferSize_s(h, n, num_samples, bytes);
+  else if constexpr (std::is_same_v<T, double>) return calaman_geodesic_points_bufferSize_d(h, n, num_samples, bytes);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_geodesic_points_bufferSize_c(h, n, num_samples, bytes);
+  else return calaman_geodesic_points_bufferSize_z(h, n, num_samples, bytes);
+}
+template <typename T>
+Status geodesic_points(BlasHandle blas, SolverHandle solver, cudaStream_t stream, int n, const T *d_W, int ldw,
+                       const T *d_H, int ldh, real_t<T> step, int num_samples, T *d_Wout, void *d_work,
+                       std::size_t lwork_bytes, int *d_info) {
+  const double mu = static_cast<double>(step);
+  if constexpr (std::is_same_v<T, float>)
+    return calaman_geodesic_points_s(blas, solver, stream, n, d_W, ldw, d_H, ldh, mu, num_samples, d_Wout, d_work,
+                                     lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, double>)
+    return calaman_geodesic_points_d(blas, solver, stream, n, d_W, ldw, d_H, ldh, mu, num_samples, d_Wout, d_work,
+                                     lwork_bytes, d_info);
+  else if constexpr (std::is_same_v<T, std::complex<float>>)
+    return calaman_geodesic_points_c(blas, solver, stream, n, d_W, ldw, d_H, ldh, mu, num_samples, d_Wout, d_work,
+                                     lwork_bytes, d_info);
+  else
+    return calaman_geodesic_points_z(blas, solver, stream, n, d_W, ldw, d_H, ldh, mu, num_samples, d_Wout, d_work,
+                                     lwork_bytes, d_info);
+}
+
 // ---- lacn2 (src/lapack/lacn2/interface.cppm:85-200) -------------------------------
 template <typename T> std::size_t lacn2_bufferSize(int n) {
   static_assert(std::is_same_v<T, float> || std::is_same_v<T, double>, "lacn2 is real only");

@@ -408,3 +408,17 @@ def expm_herm(a, upper: bool = False) -> np.ndarray:
     column scale by exp(w_j), one product with U^H)."""
     w, u = heevd(a, upper)
     return np.asfortranarray((u * np.exp(w)[None, :]) @ u.conj().T)
+
+
+def geodesic_points(w, h, step: float, num_samples: int):
+    """The rotation half of the cg_unitary sampling sweep in the reference's
+    order (src/cg_unitary/geodesic_search.cppm:354-410): R_1 = expm(step H)
+    with the general expm, R_j = R_{j-1} R_1, W_j = R_j W, j = 1..N-1."""
+    w = _as_f64(w)
+    h = _as_f64(h)
+    r1, _, _ = expm(step * h)
+    out, r = [], None
+    for j in range(1, num_samples):
+        r = r1 if j == 1 else r @ r1
+        out.append(np.asfortranarray(r @ w))
+    return out

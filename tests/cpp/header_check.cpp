@@ -80,6 +80,9 @@ int main() {
   CHECK(calaman::heevd_bufferSize<float>(calaman::FillMode::Lower, 16, &bytes).ok() && bytes > 0);
   CHECK(calaman::expm_herm<double>(nullptr, nullptr, nullptr, calaman::FillMode::Lower, 0, a.data(), n, d.data(), n,
                                    work.data(), 4096, info) == invalid);
+  // geodesic trial points: size query and rejection
+  CHECK(calaman::geodesic_points_bufferSize<std::complex<double>>(nullptr, 32, 6, &bytes).ok() && bytes > 0);
+  CHECK(calaman::geodesic_points_bufferSize<double>(nullptr, 32, 65, &bytes) == invalid);
   // lacn2: size query and host-side rejection (no device work)
   CHECK(calaman::lacn2_bufferSize<double>(100) >= 100 * sizeof(int));
   double est = 0;
