@@ -184,7 +184,12 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
 // (complex units) are 2 and 4 mod 8, so a quarter-warp's 16-byte loads hit
 // 8 distinct bank quads.
 // ---------------------------------------------------------------------------
-template <int BM, int BN, int WM, int WN, int STAGES>
+// kGauss: three real products per complex product instead of four (Gauss /
+// "3M": t1 = Ar Br, t2 = Ai Bi, t3 = (Ar + Ai)(Br + Bi); Re = t1 - t2,
+// Im = t3 - t1 - t2). The kernel is bound by the FP64 tensor pipe, so a quarter
+// of its DMMAs go; the imaginary part's rounding error grows to
+// ~eps (|Ar| + |Ai|)(|Br| + |Bi|) per term, the same order as the real part's.
+template <int BM, int BN, int WM, int WN, int STAGES, bool kGauss = false>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     zgemm_nn_kernel(int M, int N, int K, double alpha, const double2 *__restrict__ A, int lda,
                     const double2 *__restrict__ B, int ldb, double beta, double2 *__restrict__ C,
@@ -236,13 +241,22 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     }
   };
 
-  double re[MI][NI][4], im[MI][NI][4];
+  // 4M: re, im accumulate Re and Im directly; 3M (kGauss): re = t1, im = t2, t3
+  double re[MI][NI][4], im[MI][NI][4], t3[kGauss ? MI : 1][kGauss ? NI : 1][4];
 #pragma unroll
   for (int i = 0; i < MI; ++i)
 #pragma unroll
     for (int j = 0; j < NI; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) re[i][j][r] = im[i][j][r] = 0.0;
+  if constexpr (kGauss) {
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+      for (int j = 0; j < NI; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) t3[i][j][r] = 0.0;
+  }
 
   const int KT = (K + BK - 1) / BK;
 #pragma unroll
@@ -285,18 +299,50 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
         br[j][0] = y0.x; bi[j][0] = y0.y;
         br[j][1] = y1.x; bi[j][1] = y1.y;
       }
+      if constexpr (kGauss) {
+        double as[MI][4], bs[NI][2];
 #pragma unroll
-      for (int i = 0; i < MI; ++i)
+        for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < NI; ++j) {
-          dmma16x8x8(re[i][j], ar[i], br[j]);
-          dmma16x8x8(re[i][j], an[i], bi[j]);
-          dmma16x8x8(im[i][j], ar[i], bi[j]);
-          dmma16x8x8(im[i][j], ai[i], br[j]);
-        }
+          for (int r = 0; r < 4; ++r) as[i][r] = ar[i][r] + ai[i][r];
+#pragma unroll
+        for (int j = 0; j < NI; ++j)
+#pragma unroll
+          for (int r = 0; r < 2; ++r) bs[j][r] = br[j][r] + bi[j][r];
+#pragma unroll
+        for (int i = 0; i < MI; ++i)
+#pragma unroll
+          for (int j = 0; j < NI; ++j) {
+            dmma16x8x8(re[i][j], ar[i], br[j]);
+            dmma16x8x8(im[i][j], ai[i], bi[j]);
+            dmma16x8x8(t3[i][j], as[i], bs[j]);
+          }
+      } else {
+#pragma unroll
+        for (int i = 0; i < MI; ++i)
+#pragma unroll
+          for (int j = 0; j < NI; ++j) {
+            dmma16x8x8(re[i][j], ar[i], br[j]);
+            dmma16x8x8(re[i][j], an[i], bi[j]);
+            dmma16x8x8(im[i][j], ar[i], bi[j]);
+            dmma16x8x8(im[i][j], ai[i], br[j]);
+          }
+      }
     }
   }
   cp_wait<0>();
+  if constexpr (kGauss) {
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+      for (int j = 0; j < NI; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const double t1 = re[i][j][r], t2 = im[i][j][r];
+          re[i][j][r] = t1 - t2;
+          im[i][j][r] = t3[i][j][r] - t1 - t2;
+        }
+  }
 
   // epilogue: all old C values of a row block are loaded before any store
 #pragma unroll
@@ -422,13 +468,13 @@ cudaError_t run_dgemm(cudaStream_t s, int M, int N, int K, double alpha, const d
   return cudaGetLastError();
 }
 
-template <int BM, int BN, int WM, int WN, int STAGES>
+template <int BM, int BN, int WM, int WN, int STAGES, bool kGauss = true>
 cudaError_t run_zgemm(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A, int lda,
                       const double2 *B, int ldb, double beta, double2 *C, int ldc, int splits = 1,
                       int kslice = 0, long long cstride = 0) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int smem = STAGES * (16 * (BM + 2) + BN * 20) * (int)sizeof(double2);
-  auto kern = zgemm_nn_kernel<BM, BN, WM, WN, STAGES>;
+  auto kern = zgemm_nn_kernel<BM, BN, WM, WN, STAGES, kGauss>;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
