@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(kTrdThreads, 1) hetrd_kernel(TrdArgs<C> a) {
 // ---- stage 2: divide and conquer on the tridiagonal (FP64) -----------------
 struct DcWs {
   double *Za, *Zb, *DEL, *UF;
-  double *lamA, *lamB, *dd, *ee, *zv;
+  double *lamA, *lamB, *dd, *ee;
   double *srt_d, *srt_z, *nd_d, *nd_z, *df_d, *rot_c, *rot_s, *nd_lam, *zh;
   int *srt_c, *nd_c, *df_c, *rot_a, *rot_b, *cnt;
   double *sc;  // [0] the tridiagonal's scale
@@ -1064,7 +1064,7 @@ HermWs<C> carve_herm(void *base, int n, bool want_expm, std::size_t *bytes) {
   c.Zb = L.take<double>(nn);
   c.DEL = L.take<double>(nn);
   c.UF = L.take<double>(nn);
-  double **dv[] = {&c.lamA, &c.lamB, &c.dd, &c.ee, &c.zv, &c.srt_d, &c.srt_z, &c.nd_d, &c.nd_z,
+  double **dv[] = {&c.lamA, &c.lamB, &c.dd, &c.ee, &c.srt_d, &c.srt_z, &c.nd_d, &c.nd_z,
                    &c.df_d, &c.rot_c, &c.rot_s, &c.nd_lam, &c.zh};
   for (double **p : dv) *p = L.take<double>(nv);
   int **iv[] = {&c.srt_c, &c.nd_c, &c.df_c, &c.rot_a, &c.rot_b};

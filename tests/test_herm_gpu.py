@@ -171,3 +171,22 @@ def test_heevd_structured(run, oracle, case):
     assert st.ok and info == 0
     wref, _ = oracle.heevd(a)
     _check_eig(a, w, u, wref, 1e-13, 1e-15)
+
+
+@pytest.mark.parametrize("suf,n", [("z", 1300), ("d", 2100)])
+def test_heevd_columns_in_l2(run, oracle, suf, n):
+    """Sizes whose own columns no longer fit in shared memory: the reduction
+    keeps them in L2 and its vectors in a per-CTA global scratch."""
+    a = self_adjoint(n, 5.0, 600 + n, suf == "z")
+    st, w, u, info = run.heevd(a, suf)
+    assert st.ok and info == 0
+    h = oracle.hermitian_from_triangle(a, False)
+    wref, _ = oracle.heevd(a, False)
+    _check_eig(h, w, u, wref, 1e-13, 1e-15)
+
+
+def test_expm_herm_columns_in_l2(run, oracle):
+    a = self_adjoint(1536, 20.0, 1536, True)
+    st, e, _, info = run.expm_herm(a, "z", upper=True)
+    assert st.ok and info == 0
+    assert rel_frob(e, oracle.expm_herm(a, upper=True)) <= FP64_REL
