@@ -1000,8 +1000,8 @@ template <> struct CtaPanel<double> {
 template <> struct CtaPanel<float2> {
   static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, KB = 32;
 };
-template <> struct CtaPanel<float> {
-  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, KB = 64;
+template <> struct CtaPanel<float> {  // 32 wide: the in-panel SIMT update costs h kb^2 / 2 per panel
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, KB = 32;
 };
 
 // Panel width of the one-CTA path for an n x n factorisation, 0 if n is too
