@@ -521,6 +521,12 @@ cudaError_t gemm_nn<double>(cudaStream_t s, int M, int N, int K, double alpha, c
       return v16 ? run_dgemm<128, 128, 64, 32, 3, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
                  : run_dgemm<128, 128, 64, 32, 3, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     }
+    const long long tiles64 = (long long)((M + 63) / 64) * ((N + 63) / 64);
+    if (tiles64 < 74) {
+      // small products (n <= ~512): 32 x 32 tiles put four times the CTAs on the SMs
+      return v16 ? run_dgemm<32, 32, 16, 16, 4, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
+                 : run_dgemm<32, 32, 16, 16, 4, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    }
     return v16 ? run_dgemm<64, 64, 32, 32, 4, true>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc)
                : run_dgemm<64, 64, 32, 32, 4, false>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
   });
