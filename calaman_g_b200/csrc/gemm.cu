@@ -536,7 +536,10 @@ template <>
 cudaError_t gemm_nn<double2>(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A,
                              int lda, const double2 *B, int ldb, double beta, double2 *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  const long long tiles64 = (long long)((M + 63) / 64) * ((N + 63) / 64);
   return timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
+    if (tiles64 < 74)  // small or skinny products: 32 x 32 tiles, four times the CTAs
+      return run_zgemm<32, 32, 16, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     return run_zgemm<64, 64, 32, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
   });
 }
