@@ -538,7 +538,10 @@ cudaError_t gemm_nn<double2>(cudaStream_t s, int M, int N, int K, double alpha, 
   if (M <= 0 || N <= 0) return cudaSuccess;
   const long long tiles64 = (long long)((M + 63) / 64) * ((N + 63) / 64);
   return timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
-    if (tiles64 < 74)  // small or skinny products: 32 x 32 tiles, four times the CTAs
+    // up to two waves of 64 x 64 tiles (n <= 1024 square, skinny products):
+    // 32 x 32 tiles, four times the CTAs, spread the last wave (1024^3: 1.73
+    // waves -> 6.9, 278 -> 235 us)
+    if (tiles64 <= 2 * 148)
       return run_zgemm<32, 32, 16, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     return run_zgemm<64, 64, 32, 16, 3>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
   });
