@@ -625,6 +625,9 @@ __global__ void __launch_bounds__(kDcThreads) dc_rotate_kernel(DcLevel L, DcWs w
   double *Z = L.Z + (std::size_t)b0 * L.n + b0 + r;  // Z(b0 + r, b0 + col) = Z[col * n]
   for (int t = 0; t < nr; ++t) {
     const int ca = w.rot_a[b0 + t], cb = w.rot_b[b0 + t];
+    // a NaN input can leave merged-order slots unwritten (equal ranks), so a
+    // column index read back through them is checked before it addresses memory
+    if ((unsigned)ca >= (unsigned)m || (unsigned)cb >= (unsigned)m) continue;
     const double c = w.rot_c[b0 + t], s = w.rot_s[b0 + t];
     const double xa = Z[(std::size_t)ca * L.n], xb = Z[(std::size_t)cb * L.n];
     Z[(std::size_t)ca * L.n] = c * xa + s * xb;
@@ -789,7 +792,10 @@ __global__ void __launch_bounds__(kDcThreads) dc_vectors_kernel(DcLevel L, DcWs 
     }
     ss = warp_sum(ss);
     const double inv = 1.0 / sqrt(ss);
-    for (int i = lane; i < k; i += 32) UF[(std::size_t)pos * m + w.nd_c[b0 + i]] = w.zh[b0 + i] / del[i] * inv;
+    for (int i = lane; i < k; i += 32) {
+      const int col = w.nd_c[b0 + i];  // in range unless a NaN input broke the merge order
+      if ((unsigned)col < (unsigned)m) UF[(std::size_t)pos * m + col] = w.zh[b0 + i] / del[i] * inv;
+    }
     if (lane == 0) L.lam_out[b0 + pos] = lam;
   } else {
     const int u = item - k;
@@ -799,7 +805,8 @@ __global__ void __launch_bounds__(kDcThreads) dc_vectors_kernel(DcLevel L, DcWs 
     below = __reduce_add_sync(0xffffffffu, below);
     if (lane == 0) {
       const int pos = below + count_below(w.nd_lam + b0, k, x, false);
-      UF[(std::size_t)pos * m + w.df_c[b0 + u]] = 1.0;
+      const int col = w.df_c[b0 + u];
+      if ((unsigned)col < (unsigned)m) UF[(std::size_t)pos * m + col] = 1.0;
       L.lam_out[b0 + pos] = x;
     }
   }

@@ -190,3 +190,17 @@ def test_expm_herm_columns_in_l2(run, oracle):
     st, e, _, info = run.expm_herm(a, "z", upper=True)
     assert st.ok and info == 0
     assert rel_frob(e, oracle.expm_herm(a, upper=True)) <= FP64_REL
+
+
+@pytest.mark.parametrize("suf", ["d", "z"])
+def test_nan_input_completes(run, suf):
+    """A NaN entry propagates (no fault, no hang): the divide-and-conquer merge
+    order it scrambles never turns into an out-of-range index."""
+    a = self_adjoint(70, 3.0, 70, suf == "z")
+    a[5, 3] = np.nan
+    a[3, 5] = np.nan
+    st, w, u, info = run.heevd(a, suf)
+    assert st.ok and info == 0
+    assert np.isnan(w).any() or np.isnan(u).any()
+    st, e, _, info = run.expm_herm(a, suf)
+    assert st.ok and np.isnan(e).any()
