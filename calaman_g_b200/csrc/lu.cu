@@ -27,6 +27,7 @@
 #include <cooperative_groups.h>
 #include <cfloat>
 #include <climits>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -770,7 +771,15 @@ __device__ __forceinline__ void lds_vec8(const T *src, T (&dst)[kCtaChunk]) {
   for (int i = 0; i < kCtaChunk; ++i) dst[i] = u.e[i];
 }
 
-template <typename T, int KBS, int RPT>
+// kRotate: the rotating-register column loop (measured faster for complex128
+// and float32 panels: C2 +3 %, C3 +4 %); otherwise the fully unrolled one
+// (faster for float64: the wider sub-panels make the rotation and the masked
+// update cost more than the smaller code saves).
+template <typename T> constexpr bool panel_rotates() {
+  return std::is_same<T, double2>::value || std::is_same<T, float>::value;
+}
+
+template <typename T, int KBS, int RPT, bool kRotate = panel_rotates<T>()>
 __global__ void __launch_bounds__(512, 1)
     lu_panel_cta_kernel(int n, T *__restrict__ A, int lda, int k, int kb, int *__restrict__ ipiv,
                         int *__restrict__ perm, int *__restrict__ g_map_pos, int *__restrict__ g_map_src,
@@ -801,6 +810,87 @@ __global__ void __launch_bounds__(512, 1)
       for (int c = 0; c < KBS; ++c)
         r[q][c] = (gi >= sb && gi < h && c < w) ? P[(std::size_t)(sb + c) * lda + gi] : elem<T>::zero();
     }
+    if constexpr (kRotate) {
+    // ---- factor the sub-panel, one pivot column at a time. Each row's
+    // registers rotate one place left after every step, so the pivot column
+    // is always r[q][0] and every step runs the same (rolled) code with
+    // static register indices; finished columns ride at the back of the row
+    // (still swapped with it) and the update is masked to the unfinished
+    // positions. After KBS steps (idle ones past w) the row is back in
+    // column order. ----
+#pragma unroll 1
+    for (int j = 0; j < KBS; ++j) {
+      if (j < w) {
+        const int a = sb + j;
+        double bv = -1.0;
+        int bi = INT_MAX;
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          const int gi = tid + q * NT;
+          if (gi >= a && gi < h) argmax_merge(bv, bi, abs1(r[q][0]), gi);
+        }
+        const ArgMax am = cta_argmax(argmax_key(bv, bi, bi != INT_MAX), red_key, red_idx);
+        double pv = __longlong_as_double((long long)am.key);
+        int p = am.idx;
+        bool forced = false;
+        if (p >= h || p < a) {  // no comparable candidate (NaN column): keep row a
+          p = a;
+          pv = 0.0;
+          forced = true;
+        }
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          const int gi = tid + q * NT;
+          if (gi == a) {
+#pragma unroll
+            for (int c = 0; c < KBS; ++c) xrow[0][c] = r[q][c];
+          }
+          if (gi == p) {
+#pragma unroll
+            for (int c = 0; c < KBS; ++c) xrow[1][c] = r[q][c];
+          }
+        }
+        if (tid == 0) {
+          plist[a] = p;
+          if (pv == 0.0 && flags[0] < 0) flags[0] = a;
+        }
+        __syncthreads();
+        const T piv = xrow[1][0];
+        const bool singular = forced || is_zero(piv);
+        const bool use_recip = abs1(piv) >= safe_min<T>();
+        const T rpiv = singular ? elem<T>::one() : divide(elem<T>::one(), piv);
+        const int lim = w - j;  // positions 1 .. lim-1 hold unfinished columns
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          const int gi = tid + q * NT;
+          if (gi < a || gi >= h) continue;
+          if (gi == a) {
+            if (p != a) {
+#pragma unroll
+              for (int c = 0; c < KBS; ++c) r[q][c] = xrow[1][c];
+            }
+            continue;
+          }
+          if (gi == p) {
+#pragma unroll
+            for (int c = 0; c < KBS; ++c) r[q][c] = xrow[0][c];
+          }
+          const T l = singular ? r[q][0] : (use_recip ? mul(r[q][0], rpiv) : divide(r[q][0], piv));
+          r[q][0] = l;
+#pragma unroll
+          for (int c = 1; c < KBS; ++c)
+            if (c < lim) r[q][c] = sub(r[q][c], mul(l, xrow[1][c]));
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const T t0 = r[q][0];
+#pragma unroll
+        for (int c = 0; c + 1 < KBS; ++c) r[q][c] = r[q][c + 1];
+        r[q][KBS - 1] = t0;
+      }
+    }
+    } else {
     // ---- factor the sub-panel, one pivot column at a time ----
 #pragma unroll
     for (int j = 0; j < KBS; ++j) {
@@ -864,6 +954,7 @@ __global__ void __launch_bounds__(512, 1)
         for (int c = j + 1; c < KBS; ++c)
           if (c < w) r[q][c] = sub(r[q][c], mul(l, xrow[1][c]));
       }
+    }
     }
     // ---- sub-panel back to memory, L11 to shared memory ----
 #pragma unroll
