@@ -689,15 +689,16 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
   auto blk = reinterpret_cast<T(*)[LD]>(b_smem);
   auto Ls = reinterpret_cast<T(*)[64]>(b_smem + sizeof(T) * kBPanel * LD);
   auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (LD + 64));
-  __shared__ T xrow[2][kBPanel];   // [0]: old row a, [1]: the pivot row
-  __shared__ __align__(16) T urow[kBPanel];  // the pivot row right of column j
-  __shared__ T xrcp[1];                       // the pivot's reciprocal
+  // per pivot step, alternating: slot 0 the pivot row, slot 1 row a before
+  // the exchange; the pivot's reciprocal
+  __shared__ __align__(16) T wrow[2][2][kBPanel];
+  __shared__ T wrcp[2][1];
   __shared__ T rdiag[kBPanel];     // reciprocals of U's diagonal block
   __shared__ int perm[NT];  // P: row i of P q is row perm[i] of q
   __shared__ int pos[NT];   // panel-local composite of the swaps
   __shared__ int piv[kBPanel];
-  __shared__ unsigned long long red_key[NT / 32];
-  __shared__ int red_idx[NT / 32];
+  __shared__ unsigned long long red_key[2][NT / 32];
+  __shared__ int red_idx[2][NT / 32];
   __shared__ int first_zero;
 
   if (t < n) perm[t] = kFactor ? t : lo.perm[t];
@@ -713,78 +714,93 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
       r[j] = (mine && j < jb) ? Q[(std::size_t)(k + j) * n + t] : elem<T>::zero();
     if (t < n) pos[t] = t;
     __syncthreads();
+    // One pivot column per step. Each row's registers rotate one place left
+    // after every step, so the pivot column is always r[0] and the rolled loop
+    // has static register indices; finished columns ride at the back (still
+    // exchanged with their row) and the update is masked to the unfinished
+    // positions. After kBPanel steps (idle ones past jb) the row is back in
+    // column order. Two barriers per step: the CTA argmax (warp winners form
+    // their row's reciprocal meanwhile), then the pivot row (slot 0) and row a
+    // (slot kX) are published. With one row per thread this measured faster
+    // than publishing every warp winner's row before a single barrier.
+    constexpr int kX = 1;  // the slot of row a
 #pragma unroll 1
-    for (int j = 0; j < jb; ++j) {
-      const int a = k + j;
-      T rj = elem<T>::zero();
-#pragma unroll
-      for (int c = 0; c < kBPanel; ++c)
-        if (c == j) rj = r[c];
-      // pivot: largest |Re| + |Im| among rows >= a, first index on ties
-      // warp winners form their row's reciprocal while the warps exchange
-      const ArgMax wa = warp_argmax(argmax_key(abs1(rj), t, mine && t >= a));
-      cta_argmax_publish(wa, red_key, red_idx);
-      T wrcp = elem<T>::one();
-      if (t == wa.idx && !is_zero(rj)) wrcp = divide(elem<T>::one(), rj);
-      __syncthreads();
-      const ArgMax am = cta_argmax_collect(red_key, red_idx);
-      const double bv = __longlong_as_double((long long)am.key);
-      int p = am.idx;
-      if (p >= n) p = a;  // no comparable candidate (NaN column): keep row a
-      if (t == a) {
-#pragma unroll
-        for (int c = 0; c < kBPanel; ++c) xrow[0][c] = r[c];
-      }
-      if (t == p) {
-#pragma unroll
-        for (int c = 0; c < kBPanel; ++c) {
-          xrow[1][c] = r[c];
-          urow[c] = (c > j && c < jb) ? r[c] : elem<T>::zero();  // the update's row, masked
-        }
-        xrcp[0] = wrcp;
-      }
-      if (t == 0) {
-        piv[j] = p;
-        if (p != a) {
-          const int tp = perm[a];
-          perm[a] = perm[p];
-          perm[p] = tp;
-          const int tq = pos[a];
-          pos[a] = pos[p];
-          pos[p] = tq;
-        }
-        if (!(bv > 0.0) && first_zero == 0) first_zero = a + 1;
-      }
-      __syncthreads();
-      if (p != a) {
+    for (int j = 0; j < kBPanel; ++j) {
+      if (j < jb) {
+        const int a = k + j, buf = j & 1;
+        // pivot: largest |Re| + |Im| among rows >= a, first index on ties
+        const ArgMax wa = warp_argmax(argmax_key(abs1(r[0]), t, mine && t >= a));
+        cta_argmax_publish(wa, red_key[buf], red_idx[buf]);
+        T myrcp = elem<T>::one();
+        if (t == wa.idx && !is_zero(r[0])) myrcp = divide(elem<T>::one(), r[0]);
+        __syncthreads();
+        const ArgMax am = cta_argmax_collect(red_key[buf], red_idx[buf]);
+        const double bv = __longlong_as_double((long long)am.key);
+        int p = am.idx;
+        const bool forced = p >= n;  // no comparable candidate (NaN column): keep row a
+        if (forced) p = a;
         if (t == a) {
 #pragma unroll
-          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[1][c];
-        } else if (t == p) {
+          for (int c = 0; c < kBPanel; ++c) wrow[buf][kX][c] = r[c];
+        }
+        if (t == p) {
 #pragma unroll
-          for (int c = 0; c < kBPanel; ++c) r[c] = xrow[0][c];
+          for (int c = 0; c < kBPanel; ++c) wrow[buf][0][c] = r[c];
+          wrcp[buf][0] = myrcp;
+        }
+        const T *prow = wrow[buf][0];
+        if (t == 0) {
+          piv[j] = p;
+          if (p != a) {
+            const int tp = perm[a];
+            perm[a] = perm[p];
+            perm[p] = tp;
+            const int tq = pos[a];
+            pos[a] = pos[p];
+            pos[p] = tq;
+          }
+          if (!(bv > 0.0) && first_zero == 0) first_zero = a + 1;
+        }
+        __syncthreads();
+        if (p != a) {
+          if (t == a) {
+#pragma unroll
+            for (int c = 0; c < kBPanel; c += 4) {
+              T u[4];
+              lds4(&prow[c], u);
+#pragma unroll
+              for (int i = 0; i < 4; ++i) r[c + i] = u[i];
+            }
+          } else if (t == p) {
+#pragma unroll
+            for (int c = 0; c < kBPanel; c += 4) {
+              T u[4];
+              lds4(&wrow[buf][kX][c], u);
+#pragma unroll
+              for (int i = 0; i < 4; ++i) r[c + i] = u[i];
+            }
+          }
+        }
+        const T pv = prow[0];
+        if (mine && t > a && !is_zero(pv)) {
+          T l = r[0];
+          l = (!forced && abs1(pv) >= sfmin) ? mul(l, wrcp[buf][0]) : divide(l, pv);
+          const int lim = jb - j;  // positions 1 .. lim-1 hold unfinished columns
+#pragma unroll
+          for (int c = 0; c < kBPanel; c += 4) {
+            T u[4];
+            lds4(&prow[c], u);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (c + i > 0 && c + i < lim) r[c + i] = sub(r[c + i], mul(l, u[i]));
+          }
+          r[0] = l;
         }
       }
-      const T pv = xrow[1][j];
-      if (mine && t > a && !is_zero(pv)) {
-        T l = elem<T>::zero();
+      const T t0 = r[0];
 #pragma unroll
-        for (int c = 0; c < kBPanel; ++c)
-          if (c == j) l = r[c];
-        l = abs1(pv) >= sfmin ? mul(l, xrcp[0]) : divide(l, pv);
-        // unconditional rank-1 update against the masked row (zero at and left
-        // of column j; |l| <= 1 under partial pivoting), then column j = l
-#pragma unroll
-        for (int c = 0; c < kBPanel; c += 4) {
-          T u[4];
-          lds4(&urow[c], u);
-#pragma unroll
-          for (int i = 0; i < 4; ++i) r[c + i] = sub(r[c + i], mul(l, u[i]));
-        }
-#pragma unroll
-        for (int c = 0; c < kBPanel; ++c)
-          if (c == j) r[c] = l;
-      }
+      for (int c = 0; c + 1 < kBPanel; ++c) r[c] = r[c + 1];
+      r[kBPanel - 1] = t0;
     }
     // panel back to memory; L11 to shared memory
     if (mine) {

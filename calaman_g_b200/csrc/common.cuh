@@ -275,6 +275,16 @@ __device__ __forceinline__ ArgMax cta_argmax_collect(const unsigned long long *r
   const ArgMax b = lane < nwarps ? ArgMax{red_key[lane], red_idx[lane]} : ArgMax{0ull, 0x7fffffff};
   return warp_argmax(b);
 }
+// As cta_argmax_collect, and wwarp = the warp whose entry won (meaningful
+// when the winner's index is a real row: rows are unique across warps).
+__device__ __forceinline__ ArgMax cta_argmax_collect_at(const unsigned long long *red_key, const int *red_idx,
+                                                        int &wwarp) {
+  const int lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const ArgMax b = lane < nwarps ? ArgMax{red_key[lane], red_idx[lane]} : ArgMax{0ull, 0x7fffffff};
+  const ArgMax m = warp_argmax(b);
+  wwarp = __ffs(__ballot_sync(0xffffffffu, lane < nwarps && b.idx == m.idx)) - 1;
+  return m;
+}
 
 // CTA-wide: every thread passes its own candidate and receives the winner.
 // red_key / red_idx: shared arrays of blockDim.x / 32 entries. Contains one

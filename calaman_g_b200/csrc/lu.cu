@@ -750,7 +750,7 @@ __global__ void __launch_bounds__(256)
 // One-CTA panel, two levels: the h x kb panel (kb <= 64) stays in global
 // memory (L2) and is factored in sub-panels of KBS columns; a sub-panel's rows
 // live in registers (thread t keeps rows t, t + NT, ... -- RPT of them), so a
-// pivot column costs one CTA-wide argmax and two barriers, with no cluster
+// pivot column costs one CTA-wide argmax and one or two barriers, with no cluster
 // barrier and no distributed shared memory. After each sub-panel the CTA
 // applies its swaps to the panel's other columns, solves the sub-panel's
 // U12 rows with the unit-lower L11, and updates the rest of the panel.
@@ -779,6 +779,87 @@ template <typename T> constexpr bool panel_rotates() {
   return std::is_same<T, double2>::value || std::is_same<T, float>::value;
 }
 
+// One pivot step's search and row exchange. The pivot is the largest
+// |Re| + |Im| of column col among rows >= a, first index on ties; the owner of
+// row a publishes that row into slot 16. kOneBarrier: every warp's winner
+// publishes its whole row into the warp's slot before the single barrier, and
+// after it every thread agrees on the pivot p and reads the pivot row from its
+// slot (the caller alternates buffers by step: a slot is rewritten two steps
+// later, after every reader has passed the intervening barrier). Otherwise the
+// CTA argmax (one barrier) comes first and the pivot's owner alone publishes
+// its row into slot 0 before a second barrier; measured faster with one row
+// per thread (float64, 256 rows: 2.5 %), slower with two or more. Returns the
+// slot of the pivot row. forced: no comparable candidate (NaN column), p = a.
+template <typename T, int KBS, int RPT, bool kOneBarrier>
+__device__ __forceinline__ int panel_pivot(const T (&r)[RPT][KBS], int col, int a, int h, T (*wrow)[KBS],
+                                           unsigned long long *red_key, int *red_idx, int &p, bool &forced,
+                                           double &pv) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  double bv = -1.0;
+  int bi = INT_MAX;
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    const int gi = tid + q * NT;
+    if (gi >= a && gi < h) argmax_merge(bv, bi, abs1(r[q][col]), gi);
+  }
+  if constexpr (kOneBarrier) {
+    const int lane = tid & 31, warp = tid >> 5;
+    const ArgMax wa = warp_argmax(argmax_key(bv, bi, bi != INT_MAX));
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int gi = tid + q * NT;
+      if (gi == a) {
+#pragma unroll
+        for (int c = 0; c < KBS; ++c) wrow[16][c] = r[q][c];
+      }
+      if (gi == wa.idx) {
+#pragma unroll
+        for (int c = 0; c < KBS; ++c) wrow[warp][c] = r[q][c];
+      }
+    }
+    if (lane == 0) {
+      red_key[warp] = wa.key;
+      red_idx[warp] = wa.idx;
+    }
+    __syncthreads();
+    int wp;
+    const ArgMax am = cta_argmax_collect_at(red_key, red_idx, wp);
+    pv = __longlong_as_double((long long)am.key);
+    p = am.idx;
+    forced = false;
+    if (p >= h || p < a) {
+      p = a;
+      pv = 0.0;
+      forced = true;
+    }
+    return forced ? 16 : wp;
+  } else {
+    const ArgMax am = cta_argmax(argmax_key(bv, bi, bi != INT_MAX), red_key, red_idx);
+    pv = __longlong_as_double((long long)am.key);
+    p = am.idx;
+    forced = false;
+    if (p >= h || p < a) {
+      p = a;
+      pv = 0.0;
+      forced = true;
+    }
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int gi = tid + q * NT;
+      if (gi == a) {
+#pragma unroll
+        for (int c = 0; c < KBS; ++c) wrow[16][c] = r[q][c];
+      }
+      if (gi == p) {
+#pragma unroll
+        for (int c = 0; c < KBS; ++c) wrow[0][c] = r[q][c];
+      }
+    }
+    __syncthreads();
+    return 0;
+  }
+}
+
 template <typename T, int KBS, int RPT, bool kRotate = panel_rotates<T>()>
 __global__ void __launch_bounds__(512, 1)
     lu_panel_cta_kernel(int n, T *__restrict__ A, int lda, int k, int kb, int *__restrict__ ipiv,
@@ -789,11 +870,13 @@ __global__ void __launch_bounds__(512, 1)
   const int NT = blockDim.x, nwarps = NT >> 5;
   const int h = n - k;
   T *P = A + (std::size_t)k * lda + k;  // the panel: P[c * lda + i], i < h, c < kb
-  __shared__ T xrow[2][KBS];            // [0]: old row a, [1]: the pivot row
+  // per pivot step, alternating: slots 0..15 each warp winner's row, slot 16
+  // row a before the exchange
+  __shared__ __align__(16) T wrow[2][17][KBS];
   __shared__ T l11[KBS][KBS + 1];
   __shared__ __align__(16) T u12[KBS][kMaxKb];
-  __shared__ unsigned long long red_key[16];
-  __shared__ int red_idx[16];
+  __shared__ unsigned long long red_key[2][16];
+  __shared__ int red_idx[2][16];
   __shared__ int plist[kMaxKb];
   __shared__ int flags[1];
   __shared__ int mpos[2 * kMaxKb], morg[2 * kMaxKb];
@@ -821,41 +904,17 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll 1
     for (int j = 0; j < KBS; ++j) {
       if (j < w) {
-        const int a = sb + j;
-        double bv = -1.0;
-        int bi = INT_MAX;
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          const int gi = tid + q * NT;
-          if (gi >= a && gi < h) argmax_merge(bv, bi, abs1(r[q][0]), gi);
-        }
-        const ArgMax am = cta_argmax(argmax_key(bv, bi, bi != INT_MAX), red_key, red_idx);
-        double pv = __longlong_as_double((long long)am.key);
-        int p = am.idx;
-        bool forced = false;
-        if (p >= h || p < a) {  // no comparable candidate (NaN column): keep row a
-          p = a;
-          pv = 0.0;
-          forced = true;
-        }
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          const int gi = tid + q * NT;
-          if (gi == a) {
-#pragma unroll
-            for (int c = 0; c < KBS; ++c) xrow[0][c] = r[q][c];
-          }
-          if (gi == p) {
-#pragma unroll
-            for (int c = 0; c < KBS; ++c) xrow[1][c] = r[q][c];
-          }
-        }
+        const int a = sb + j, buf = j & 1;
+        int p;
+        bool forced;
+        double pv;
+        const int ps = panel_pivot<T, KBS, RPT, (RPT > 1)>(r, 0, a, h, wrow[buf], red_key[buf], red_idx[buf], p, forced, pv);
+        const T *prow = wrow[buf][ps];
         if (tid == 0) {
           plist[a] = p;
           if (pv == 0.0 && flags[0] < 0) flags[0] = a;
         }
-        __syncthreads();
-        const T piv = xrow[1][0];
+        const T piv = prow[0];
         const bool singular = forced || is_zero(piv);
         const bool use_recip = abs1(piv) >= safe_min<T>();
         const T rpiv = singular ? elem<T>::one() : divide(elem<T>::one(), piv);
@@ -867,19 +926,19 @@ __global__ void __launch_bounds__(512, 1)
           if (gi == a) {
             if (p != a) {
 #pragma unroll
-              for (int c = 0; c < KBS; ++c) r[q][c] = xrow[1][c];
+              for (int c = 0; c < KBS; ++c) r[q][c] = prow[c];
             }
             continue;
           }
           if (gi == p) {
 #pragma unroll
-            for (int c = 0; c < KBS; ++c) r[q][c] = xrow[0][c];
+            for (int c = 0; c < KBS; ++c) r[q][c] = wrow[buf][16][c];
           }
           const T l = singular ? r[q][0] : (use_recip ? mul(r[q][0], rpiv) : divide(r[q][0], piv));
           r[q][0] = l;
 #pragma unroll
           for (int c = 1; c < KBS; ++c)
-            if (c < lim) r[q][c] = sub(r[q][c], mul(l, xrow[1][c]));
+            if (c < lim) r[q][c] = sub(r[q][c], mul(l, prow[c]));
         }
       }
 #pragma unroll
@@ -895,41 +954,17 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll
     for (int j = 0; j < KBS; ++j) {
       if (j >= w) break;
-      const int a = sb + j;
-      double bv = -1.0;
-      int bi = INT_MAX;
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        const int gi = tid + q * NT;
-        if (gi >= a && gi < h) argmax_merge(bv, bi, abs1(r[q][j]), gi);
-      }
-      const ArgMax am = cta_argmax(argmax_key(bv, bi, bi != INT_MAX), red_key, red_idx);
-      double pv = __longlong_as_double((long long)am.key);
-      int p = am.idx;
-      bool forced = false;
-      if (p >= h || p < a) {  // no comparable candidate (NaN column): keep row a
-        p = a;
-        pv = 0.0;
-        forced = true;
-      }
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        const int gi = tid + q * NT;
-        if (gi == a) {
-#pragma unroll
-          for (int c = 0; c < KBS; ++c) xrow[0][c] = r[q][c];
-        }
-        if (gi == p) {
-#pragma unroll
-          for (int c = 0; c < KBS; ++c) xrow[1][c] = r[q][c];
-        }
-      }
+      const int a = sb + j, buf = j & 1;
+      int p;
+      bool forced;
+      double pv;
+      const int ps = panel_pivot<T, KBS, RPT, (RPT > 1)>(r, j, a, h, wrow[buf], red_key[buf], red_idx[buf], p, forced, pv);
+      const T *prow = wrow[buf][ps];
       if (tid == 0) {
         plist[a] = p;
         if (pv == 0.0 && flags[0] < 0) flags[0] = a;
       }
-      __syncthreads();
-      const T piv = xrow[1][j];
+      const T piv = prow[j];
       const bool singular = forced || is_zero(piv);
       const bool use_recip = abs1(piv) >= safe_min<T>();
       const T rpiv = singular ? elem<T>::one() : divide(elem<T>::one(), piv);
@@ -940,19 +975,19 @@ __global__ void __launch_bounds__(512, 1)
         if (gi == a) {
           if (p != a) {
 #pragma unroll
-            for (int c = 0; c < KBS; ++c) r[q][c] = xrow[1][c];
+            for (int c = 0; c < KBS; ++c) r[q][c] = prow[c];
           }
           continue;
         }
         if (gi == p) {
 #pragma unroll
-          for (int c = 0; c < KBS; ++c) r[q][c] = xrow[0][c];
+          for (int c = 0; c < KBS; ++c) r[q][c] = wrow[buf][16][c];
         }
         const T l = singular ? r[q][j] : (use_recip ? mul(r[q][j], rpiv) : divide(r[q][j], piv));
         r[q][j] = l;
 #pragma unroll
         for (int c = j + 1; c < KBS; ++c)
-          if (c < w) r[q][c] = sub(r[q][c], mul(l, xrow[1][c]));
+          if (c < w) r[q][c] = sub(r[q][c], mul(l, prow[c]));
       }
     }
     }
