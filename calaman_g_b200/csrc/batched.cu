@@ -531,9 +531,12 @@ cudaError_t launch_group(cudaStream_t st, dim3 grid, const Item *items, const BP
 constexpr int kBU = 8;
 
 // CTAs per SM the LU kernel is compiled for: FP32 rows fit 128 registers
-// (two 256-thread CTAs), FP64 rows take up to 255 at 256 threads.
-template <typename T, int NT> struct BLuOcc {
-  static constexpr int kMinBlocks = (sizeof(T) == 4 ? 2 : 1) * (256 / NT);
+// (two 256-thread CTAs); FP64 as the solve kind says (Lu::kFp64Ctas): two
+// CTAs (128 registers, a few spilled, and both CTAs' shared memory fit)
+// measured faster for the expm solve, one (up to 255 registers) for the
+// adjoint's, which spills more at 128.
+template <typename T, int NT, typename Lu> struct BLuOcc {
+  static constexpr int kMinBlocks = (sizeof(T) == 4 ? 2 : Lu::kFp64Ctas) * (256 / NT);
 };
 
 // D(r0 + i, c) -= sum_{j < jb} L(i, j) blk[j][c] for i < mrows, c in [c0, c0 + ncols),
@@ -658,6 +661,7 @@ struct LuOps {
 // expm: factor q = V, solve for the quotient from p (in P0) into the output
 // (s = 0) or into X (s > 0, squared afterwards)
 struct ExpmLu {
+  static constexpr int kFp64Ctas = 2;
   template <typename T, typename Wd>
   static __device__ __forceinline__ LuOps<T> ops(const BItem<T, Wd> &it, const BPlan &pl, int) {
     return LuOps<T>{it.V, it.P0, pl.s > 0 ? it.X : it.E, pl.s > 0 ? it.n : it.lde, nullptr, it.id};
@@ -667,7 +671,7 @@ struct ExpmLu {
 // kFactor: LU with partial pivoting of Q, then the solve; otherwise the solve
 // alone with factors and permutation from an earlier kFactor launch.
 template <typename Item, typename T, typename Lu, bool kFactor, int NT>
-__global__ void __launch_bounds__(NT, BLuOcc<T, NT>::kMinBlocks)
+__global__ void __launch_bounds__(NT, BLuOcc<T, NT, Lu>::kMinBlocks)
     g_lu_kernel(const Item *__restrict__ items, const BPlan *__restrict__ plans, int *__restrict__ info,
                 int mode) {
   using R = typename elem<T>::real;
@@ -950,6 +954,9 @@ cudaError_t launch_lu(cudaStream_t st, const Item *items, const BPlan *plans, in
     auto kern = g_lu_kernel<Item, T, Lu, kFactor, NT>;
     constexpr std::size_t smem = lu_smem_bytes<T, NT>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    // the largest shared-memory carveout, so the CTAs the registers allow fit
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (e != cudaSuccess) return e;
     kern<<<to - from, NT, smem, st>>>(items + from, plans + from, info, mode);
     return launched();
@@ -1373,6 +1380,7 @@ struct VjpOps {
 
 // mode 0: factor q = V, R = q^-1 p (p in T1) into P0; mode 1: dR = q^-1 T2 into M0
 struct VjpLu {
+  static constexpr int kFp64Ctas = 1;
   template <typename T, typename Wd>
   static __device__ __forceinline__ LuOps<T> ops(const BVItem<T, Wd> &it, const BPlan &, int mode) {
     return mode == 0 ? LuOps<T>{it.V, it.T1, it.P0, it.n, it.perm, it.id}
