@@ -219,6 +219,25 @@ __global__ void __launch_bounds__(256) b_narrow_kernel(const BItem<T, Wd> *__res
 // output tile per CTA. What a phase multiplies is decided per matrix by an
 // operand policy (Ops::pade for the evaluation phases, Ops::square for the
 // squarings); blockIdx.y selects a sub-problem of the phase.
+// four consecutive shared-memory elements (src 16-byte aligned)
+template <typename T>
+__device__ __forceinline__ void lds4(const T *src, T (&dst)[4]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4 *>(src);
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+  } else if constexpr (sizeof(T) == 8) {
+    const double2 *s2 = reinterpret_cast<const double2 *>(src);
+    union { double2 v[2]; T e[4]; } u;
+    u.v[0] = s2[0];
+    u.v[1] = s2[1];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[i] = u.e[i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[i] = src[i];
+  }
+}
+
 template <typename U>
 struct GOps {
   const U *A = nullptr, *B = nullptr, *A2 = nullptr, *B2 = nullptr;
@@ -294,10 +313,10 @@ __global__ void __launch_bounds__(256)
   const int local = tile - tile_prefix[lo];
   const int m0 = (local % tn) * kGTile, n0 = (local / tn) * kGTile;
 
-  __shared__ U As[kGK][kGTile + 4];
-  __shared__ U Bs[kGK][kGTile + 4];
+  __shared__ __align__(16) U As[kGK][kGTile + 4];
+  __shared__ __align__(16) U Bs[kGK][kGTile + 4];
   const int t = threadIdx.x;
-  const int tx = t & 15, ty = t >> 4;  // rows tx + 16 i, columns ty + 16 j
+  const int tx = t & 15, ty = t >> 4;  // rows 4 tx + i, columns 4 ty + j: one vector load each
   U acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -335,10 +354,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int kk = 0; kk < kGK; ++kk) {
         U a[4], bv[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) bv[j] = Bs[kk][ty + 16 * j];
+        lds4(&As[kk][4 * tx], a);
+        lds4(&Bs[kk][4 * ty], bv);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -351,16 +368,16 @@ __global__ void __launch_bounds__(256)
   for (int j = 0; j < 4; ++j)
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int c = n0 + ty + 16 * j, r = m0 + tx + 16 * i;
+      const int c = n0 + 4 * ty + j, r = m0 + 4 * tx + i;
       old[i][j] = (o.acc && c < n && r < n) ? o.C[(std::size_t)c * o.ldc + r] : elem<U>::zero();
     }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    const int c = n0 + ty + 16 * j;
+    const int c = n0 + 4 * ty + j;
     if (c >= n) continue;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int r = m0 + tx + 16 * i;
+      const int r = m0 + 4 * tx + i;
       if (r >= n) continue;
       const U v = o.neg ? sub(old[i][j], acc[i][j]) : add(old[i][j], acc[i][j]);
       o.C[(std::size_t)c * o.ldc + r] = v;
@@ -546,24 +563,6 @@ template <typename T, int NT, typename Lu> struct BLuOcc {
 // block are staged in shared memory. c0 is a multiple of 4 and blk rows are
 // padded by 64 columns, so the 4-wide shared loads never leave their row.
 template <int NT> constexpr int blk_ld() { return NT + 64; }
-
-template <typename T>
-__device__ __forceinline__ void lds4(const T *src, T (&dst)[4]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 v = *reinterpret_cast<const float4 *>(src);
-    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
-  } else if constexpr (sizeof(T) == 8) {
-    const double2 *s2 = reinterpret_cast<const double2 *>(src);
-    union { double2 v[2]; T e[4]; } u;
-    u.v[0] = s2[0];
-    u.v[1] = s2[1];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) dst[i] = u.e[i];
-  } else {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) dst[i] = src[i];
-  }
-}
 
 // Triangular solves of one right-hand-side column against the diagonal block
 // in shared memory: unit lower (forward) and non-unit upper with the diagonal's
