@@ -2,7 +2,7 @@
 """Benchmark of the B200 matrix-exponential path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config expm_c128_1024]
+                    [--config expm_c128_1024] [--no-cpu] [--cpu-threads T]
 
 One step = one expm of the workload matrix through the C ABI
 (calaman_expm_<t>). The default workload is the complex128 1024 x 1024
@@ -23,6 +23,8 @@ Printed (rank 0, one JSON line):
 With torchrun (N > 1) every rank runs its own replica (a single expm does not
 shard) and value = N * K / (max over ranks of the timed seconds).
 `--impl reference` times the reference algorithm's CPU restatement alone.
+`--cpu-threads T` limits both CPU legs to T host threads (1: the
+single-threaded baseline); the default uses every host thread.
 """
 from __future__ import annotations
 
@@ -219,12 +221,23 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+CPU_THREADS = 0  # host threads of the CPU legs; 0: every host thread
+
+
+def cpu_threads() -> int:
+    return CPU_THREADS if CPU_THREADS > 0 else (os.cpu_count() or 1)
+
+
+def threads_phrase(n: int) -> str:
+    return "1 thread" if n == 1 else f"{n} threads"
+
+
 def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
     """The oracle (FP64 restatement of the reference algorithm) on all host
     threads: whole expm calls of the same matrix until min_seconds."""
     from oracle import oracle as O
 
-    cores = os.cpu_count() or 1
+    cores = cpu_threads()
     O.set_threads(cores)
     reps, t0 = 0, time.perf_counter()
     result = None
@@ -242,7 +255,7 @@ def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
             break
     return {"value": reps / el, "unit": "expm/s", "cores": cores, "kind": "port",
             "sample": f"{reps} full expm call(s) of the benchmark matrix ({cfg['desc']}), "
-                      f"{el:.1f} s, C oracle with {cores} threads"}, result
+                      f"{el:.1f} s, C oracle with {threads_phrase(cores)}"}, result
 
 
 def run_reference(args, cfg):
@@ -255,7 +268,7 @@ def run_reference(args, cfg):
         return
     from oracle import oracle as O
 
-    cores = os.cpu_count() or 1
+    cores = cpu_threads()
     O.set_threads(cores)
     kind = cfg.get("kind", "single")
     dtype = {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[cfg["suf"]]
@@ -324,7 +337,7 @@ def run_reference(args, cfg):
         "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                          "sample": f"{sample}; {args.steps} timed steps after {args.warmup} "
                                    f"warm-up, C oracle (FP64 restatement of the reference "
-                                   f"algorithm), {cores} threads"},
+                                   f"algorithm), {threads_phrase(cores)}"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if kind == "single" and plan_info:
@@ -573,6 +586,25 @@ def _bf16_peak():
             return float(json.load(f)["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (burst)"
     except (OSError, KeyError, ValueError):
         return 1590.0, "fallback 1.59 PFLOP/s (no MEASURED_PEAKS.json)"
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+
+
+def hbm_min(ns, esz, ms_per_step):
+    """The batch's minimum-HBM-traffic bound: every matrix read once and its
+    exponential written once (2 n^2 elements each), over the step time."""
+    peak, src = _hbm_peak()
+    nbytes = 2 * sum(n * n for n in ns) * esz
+    gbs = nbytes / (ms_per_step * 1e-3) / 1e9
+    return {"bytes_per_step": nbytes, "achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
+            "unit": "GB/s", "peak_source": src,
+            "what": "each matrix read once and its exponential written once, per GPU"}
 
 
 E2E_SUB_BATCHES = 4
@@ -848,6 +880,7 @@ def run_batched(args, cfg):
                          "kernel": "grouped dense-product phases (every grouped GEMM launch)",
                          "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
                          "peak_source": peak_src},
+            "hbm_min": hbm_min(ns, esz, total_ms / args.steps),
             "cpu_baseline": baseline,
             "e2e": {"value": e2e_value, "unit": "expm/s",
                     "h2d_bytes_per_step": sum(n * n for n in ns) * esz,
@@ -869,7 +902,7 @@ def batched_cpu_sample(mats, suf, seconds=10.0):
     """The oracle on the first matrices of the batch until `seconds` pass."""
     from oracle import oracle as O
 
-    cores = os.cpu_count() or 1
+    cores = cpu_threads()
     O.set_threads(cores)
     done, t0 = 0, time.perf_counter()
     for m in mats:
@@ -880,7 +913,7 @@ def batched_cpu_sample(mats, suf, seconds=10.0):
     el = time.perf_counter() - t0
     return {"value": done / el, "unit": "expm/s", "cores": cores, "kind": "port",
             "sample": f"the first {done} matrices of the batch ({el:.1f} s), C oracle with "
-                      f"{cores} threads"}
+                      f"{threads_phrase(cores)}"}
 
 
 def run_vjp(args, cfg):
@@ -1145,14 +1178,14 @@ def run_geodesic(args, cfg):
         if world == 1 and not args.no_cpu:
             from oracle import oracle as O
 
-            cores = os.cpu_count() or 1
+            cores = cpu_threads()
             O.set_threads(cores)
             t0 = time.perf_counter()
             ref = O.geodesic_points(w, hmat, cfg["step"], num)
             el = time.perf_counter() - t0
             baseline = {"value": 1.0 / el, "unit": "search/s", "cores": cores, "kind": "port",
                         "sample": f"one search's trial points in the reference's order (general expm, "
-                                  f"power chain, products), {el:.1f} s, {cores} threads"}
+                                  f"power chain, products), {el:.1f} s, {threads_phrase(cores)}"}
             got = host_o.numpy()
             worst = 0.0
             for j, r in enumerate(ref):
@@ -1197,7 +1230,18 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="expm_c128_1024", choices=sorted(CONFIGS))
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    p.add_argument("--cpu-threads", type=int, default=0,
+                   help="host threads of the CPU baseline and the reference arm (the C "
+                        "oracle's workers and numpy's BLAS); 0: every host thread")
     args = p.parse_args()
+    global CPU_THREADS
+    CPU_THREADS = max(0, args.cpu_threads)
+    if CPU_THREADS:
+        # numpy's BLAS (the adjoint restatement, xHEEVD, the geodesic power
+        # chain) obeys the same limit as the C oracle's own workers
+        from threadpoolctl import threadpool_limits
+
+        threadpool_limits(limits=CPU_THREADS)
     cfg = CONFIGS[args.config]
     kind = cfg.get("kind", "single")
     if args.impl == "reference":
