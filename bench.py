@@ -18,11 +18,13 @@ Printed (rank 0, one JSON line):
   roofline    dense-product throughput measured live with CUDA events around
               every GEMM launch in the timed steps, against the FP64 tensor
               peak measured in this run (cuBLAS complex128 GEMM, 4096^3);
-  cpu_baseline  the C oracle (FP64 restatement of the reference algorithm)
-              on this host's cores, on the same matrix.
+  cpu_baseline  the reference algorithm restated in FP64 with its products on
+              numpy's BLAS and its solve on LAPACK (the bundled OpenBLAS) on
+              this host's cores, on the same matrix; the C oracle (fixed
+              evaluation order) checks the result.
 With torchrun (N > 1) every rank runs its own replica (a single expm does not
 shard) and value = N * K / (max over ranks of the timed seconds).
-`--impl reference` times the reference algorithm's CPU restatement alone.
+`--impl reference` times that CPU restatement alone.
 `--cpu-threads T` limits both CPU legs to T host threads (1: the
 single-threaded baseline); the default uses every host thread.
 """
@@ -232,36 +234,52 @@ def threads_phrase(n: int) -> str:
     return "1 thread" if n == 1 else f"{n} threads"
 
 
+CPU_FORM = ("the reference algorithm restated with its products on numpy's BLAS and its solve "
+            "on LAPACK xGESV (bundled OpenBLAS), FP64")
+
+
 def cpu_baseline(a, cfg, min_seconds=8.0, max_reps=3):
-    """The oracle (FP64 restatement of the reference algorithm) on all host
-    threads: whole expm calls of the same matrix until min_seconds."""
+    """The CPU baseline on all host threads: whole calls of the timing
+    restatement (oracle.expm_blas: the reference algorithm with GEMM through
+    BLAS and LU through LAPACK) on the same matrix until min_seconds; then
+    one untimed call of the C oracle, whose result the accuracy check uses."""
     from oracle import oracle as O
 
     cores = cpu_threads()
     O.set_threads(cores)
+    single = cfg["suf"] in "sc"
+    x = a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
     reps, t0 = 0, time.perf_counter()
-    result = None
     while True:
-        x = a.astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
         if cfg.get("entry") == "expm_balanced":
-            result, plan = O.expm_balanced(x, single=cfg["suf"] in "sc")
+            O.expm_balanced(x, single=single, blas=True)
         elif cfg.get("entry") == "expm_herm":
-            result = O.expm_herm(x)
+            O.expm_herm(x)
         else:
-            result, plan, _ = O.expm(x, single=cfg["suf"] in "sc")
+            O.expm_blas(x, single=single)
         reps += 1
         el = time.perf_counter() - t0
         if el >= min_seconds or reps >= max_reps:
             break
+    if cfg.get("entry") == "expm_balanced":
+        result = O.expm_balanced(x, single=single)[0]
+    elif cfg.get("entry") == "expm_herm":
+        result = O.expm_herm(x)
+    else:
+        result = O.expm(x, single=single)[0]
+    form = ("LAPACK xHEEVD through numpy, then the column scale and one product on BLAS"
+            if cfg.get("entry") == "expm_herm" else CPU_FORM)
     return {"value": reps / el, "unit": "expm/s", "cores": cores, "kind": "port",
             "sample": f"{reps} full expm call(s) of the benchmark matrix ({cfg['desc']}), "
-                      f"{el:.1f} s, C oracle with {threads_phrase(cores)}"}, result
+                      f"{el:.1f} s, {form}, {threads_phrase(cores)}"}, result
 
 
 def run_reference(args, cfg):
-    """The reference algorithm's CPU restatement (the C oracle, all host
-    threads) on the same workload; rank 0 only. Batched: each step is the
-    first 32 matrices of the batch; adjoint: each step is one numpy
+    """The reference algorithm's CPU form on the same workload, all host
+    threads, rank 0 only: the FP64 restatement with its products on numpy's
+    BLAS and its solve on LAPACK (oracle.expm_blas; the C oracle's gebal
+    sweep for the balanced config, xHEEVD for expm_herm). Batched: each step
+    is the first 32 matrices of the batch; adjoint: each step is one numpy
     restatement of the adjoint (FP64, threaded BLAS)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -279,7 +297,7 @@ def run_reference(args, cfg):
 
         def one():
             for m in mats:
-                O.expm(m, single=single)
+                O.expm_blas(m, single=single)
         sample = "the first 32 matrices of the batch per step"
         plan_info = None
     elif kind == "geodesic":
@@ -287,9 +305,9 @@ def run_reference(args, cfg):
         per_step, unit = 1, "search/s"
 
         def one():
-            O.geodesic_points(w, hmat, cfg["step"], cfg["samples"])
+            O.geodesic_points(w, hmat, cfg["step"], cfg["samples"], blas=True)
         sample = ("the trial points of one search per step (general expm, then the power chain and "
-                  "products with numpy's threaded BLAS)")
+                  "products, all on numpy's threaded BLAS)")
         plan_info = None
     elif kind == "vjp":
         k = 1 if cfg["n"] > 512 else 8
@@ -308,13 +326,13 @@ def run_reference(args, cfg):
 
         if cfg.get("entry") == "expm_balanced":
             def one():
-                holder["plan"] = O.expm_balanced(x, single=single)[1]
+                holder["plan"] = O.expm_balanced(x, single=single, blas=True)[1]
         elif cfg.get("entry") == "expm_herm":
             def one():
                 O.expm_herm(x)
         else:
             def one():
-                holder["plan"] = O.expm(x, single=single)[1]
+                holder["plan"] = O.expm_blas(x, single=single)[1]
         sample = "one full expm of the benchmark matrix per step"
         if cfg.get("entry") == "expm_herm":
             sample += " (eigendecomposition route: LAPACK zheevd through numpy, threaded BLAS)"
@@ -336,8 +354,7 @@ def run_reference(args, cfg):
         "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded)", "config": config,
         "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port",
                          "sample": f"{sample}; {args.steps} timed steps after {args.warmup} "
-                                   f"warm-up, C oracle (FP64 restatement of the reference "
-                                   f"algorithm), {threads_phrase(cores)}"},
+                                   f"warm-up; {CPU_FORM}; {threads_phrase(cores)}"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if kind == "single" and plan_info:
@@ -899,20 +916,21 @@ def run_batched(args, cfg):
 
 
 def batched_cpu_sample(mats, suf, seconds=10.0):
-    """The oracle on the first matrices of the batch until `seconds` pass."""
+    """The timing restatement (oracle.expm_blas) on the first matrices of the
+    batch until `seconds` pass."""
     from oracle import oracle as O
 
     cores = cpu_threads()
     O.set_threads(cores)
     done, t0 = 0, time.perf_counter()
     for m in mats:
-        O.expm(m.astype(np.float64), single=suf == "s")
+        O.expm_blas(m.astype(np.float64), single=suf == "s")
         done += 1
         if time.perf_counter() - t0 >= seconds:
             break
     el = time.perf_counter() - t0
     return {"value": done / el, "unit": "expm/s", "cores": cores, "kind": "port",
-            "sample": f"the first {done} matrices of the batch ({el:.1f} s), C oracle with "
+            "sample": f"the first {done} matrices of the batch ({el:.1f} s), {CPU_FORM}, "
                       f"{threads_phrase(cores)}"}
 
 
@@ -1181,11 +1199,13 @@ def run_geodesic(args, cfg):
             cores = cpu_threads()
             O.set_threads(cores)
             t0 = time.perf_counter()
-            ref = O.geodesic_points(w, hmat, cfg["step"], num)
+            O.geodesic_points(w, hmat, cfg["step"], num, blas=True)
             el = time.perf_counter() - t0
             baseline = {"value": 1.0 / el, "unit": "search/s", "cores": cores, "kind": "port",
                         "sample": f"one search's trial points in the reference's order (general expm, "
-                                  f"power chain, products), {el:.1f} s, {threads_phrase(cores)}"}
+                                  f"power chain, products, all on numpy's BLAS), {el:.1f} s, "
+                                  f"{threads_phrase(cores)}"}
+            ref = O.geodesic_points(w, hmat, cfg["step"], num)  # the checker: the C oracle's expm
             got = host_o.numpy()
             worst = 0.0
             for j, r in enumerate(ref):
@@ -1231,14 +1251,14 @@ def main():
     p.add_argument("--config", default="expm_c128_1024", choices=sorted(CONFIGS))
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--cpu-threads", type=int, default=0,
-                   help="host threads of the CPU baseline and the reference arm (the C "
-                        "oracle's workers and numpy's BLAS); 0: every host thread")
+                   help="host threads of the CPU baseline and the reference arm (numpy's "
+                        "BLAS and the C oracle's workers); 0: every host thread")
     args = p.parse_args()
     global CPU_THREADS
     CPU_THREADS = max(0, args.cpu_threads)
     if CPU_THREADS:
-        # numpy's BLAS (the adjoint restatement, xHEEVD, the geodesic power
-        # chain) obeys the same limit as the C oracle's own workers
+        # numpy's BLAS (the timed restatements) obeys the same limit as the
+        # C oracle's own workers
         from threadpoolctl import threadpool_limits
 
         threadpool_limits(limits=CPU_THREADS)

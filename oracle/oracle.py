@@ -229,6 +229,43 @@ def expm(a, single: bool = False):
     return e, ExpmPlan(plan.m, plan.s, plan.num_gemms), info.value
 
 
+def expm_blas(a, single: bool = False):
+    """Timing restatement of expm(): the same plan, Pade degree, scaling and
+    product order (src/expm/expm.cppm:121-171, src/expm/pade.cppm:127-188:
+    A2, A4 = A2 A2, A6 = A4 A2, A8 = A4 A4, degree 13 nested), with every
+    product on numpy's BLAS and the solve on LAPACK xGESV (xGETRF + xGETRS),
+    the reference's own CPU form of the path (GEMM through BLAS, LU through
+    LAPACK; here the bundled OpenBLAS, threaded). FP64. Not bit-identical to
+    expm() (the BLAS sums in its own order); expm() stays the checker.
+    Returns (E, ExpmPlan)."""
+    a = _as_f64(a)
+    n = a.shape[0]
+    plan = expm_plan(norm1(a), single)
+    m, s = plan.m, plan.s
+    b = pade_coeffs(m)
+    x = np.asfortranarray(a * (2.0 ** (-s)))
+    eye = np.eye(n, dtype=x.dtype)
+    p = [x @ x]
+    npw = pade_num_powers(m)
+    if npw >= 2:
+        p.append(p[0] @ p[0])
+    if npw >= 3:
+        p.append(p[1] @ p[0])
+    if npw >= 4:
+        p.append(p[1] @ p[1])
+    if m != 13:
+        v = b[0] * eye + sum(b[2 * (k + 1)] * p[k] for k in range(npw))
+        w = b[1] * eye + sum(b[2 * (k + 1) + 1] * p[k] for k in range(npw))
+    else:
+        w = b[1] * eye + b[3] * p[0] + b[5] * p[1] + b[7] * p[2] + p[2] @ (b[9] * p[0] + b[11] * p[1] + b[13] * p[2])
+        v = b[0] * eye + b[2] * p[0] + b[4] * p[1] + b[6] * p[2] + p[2] @ (b[8] * p[0] + b[10] * p[1] + b[12] * p[2])
+    u = x @ w
+    r = np.linalg.solve(v - u, v + u)
+    for _ in range(s):
+        r = r @ r
+    return np.asfortranarray(r), plan
+
+
 def paterson_stockmeyer(a, coeffs, s_requested: int = 0) -> np.ndarray:
     a = np.asfortranarray(a, dtype=np.float64)
     c = np.ascontiguousarray(coeffs, dtype=np.float64)
@@ -338,10 +375,11 @@ def gebal_scale(a, max_sweeps: int = 1000):
     return b, d, sweeps.value
 
 
-def expm_balanced(a, single: bool = False):
-    """D exp(D^-1 A D) D^-1 with D from gebal_scale; returns (E, ExpmPlan of B)."""
+def expm_balanced(a, single: bool = False, blas: bool = False):
+    """D exp(D^-1 A D) D^-1 with D from gebal_scale; returns (E, ExpmPlan of B).
+    blas: the inner expm is the timing restatement expm_blas()."""
     b, d, _ = gebal_scale(a)
-    e, plan, _ = expm(b, single)
+    e, plan = expm_blas(b, single) if blas else expm(b, single)[:2]
     return np.asfortranarray(e * d[:, None] / d[None, :]), plan
 
 
@@ -410,13 +448,14 @@ def expm_herm(a, upper: bool = False) -> np.ndarray:
     return np.asfortranarray((u * np.exp(w)[None, :]) @ u.conj().T)
 
 
-def geodesic_points(w, h, step: float, num_samples: int):
+def geodesic_points(w, h, step: float, num_samples: int, blas: bool = False):
     """The rotation half of the cg_unitary sampling sweep in the reference's
     order (src/cg_unitary/geodesic_search.cppm:354-410): R_1 = expm(step H)
-    with the general expm, R_j = R_{j-1} R_1, W_j = R_j W, j = 1..N-1."""
+    with the general expm, R_j = R_{j-1} R_1, W_j = R_j W, j = 1..N-1.
+    blas: R_1 by the timing restatement expm_blas()."""
     w = _as_f64(w)
     h = _as_f64(h)
-    r1, _, _ = expm(step * h)
+    r1 = expm_blas(step * h)[0] if blas else expm(step * h)[0]
     out, r = [], None
     for j in range(1, num_samples):
         r = r1 if j == 1 else r @ r1

@@ -36,6 +36,7 @@ def test_reference_single_thread():
     d = _reference_line("--cpu-threads", "1")
     assert d["cpu_baseline"]["cores"] == 1
     assert d["cpu_baseline"]["sample"].endswith("1 thread")
+    assert "BLAS" in d["cpu_baseline"]["sample"]
     assert d["value"] > 0
 
 
