@@ -850,7 +850,10 @@ def run_batched(args, cfg):
     if rank == 0:
         pl = list(plans)
         flops = sum(expm_flops(n, p.m, p.s, False) for n, p in zip(ns, pl))
-        peak, peak_src = _bf16_peak()
+        if suf == "s":
+            peak, peak_src = _bf16_peak()
+        else:  # the FP64 tier: every product on the FP64 tensor cores (DMMA)
+            peak, peak_src = measure_fp64_peak(torch, dev, False), "cuBLAS float64 GEMM 4096^3 in this run"
         achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
         acc = {}
         if suf == "s":
