@@ -234,6 +234,70 @@ def threads_phrase(n: int) -> str:
     return "1 thread" if n == 1 else f"{n} threads"
 
 
+# ---- CPU legs over many small matrices: one single-threaded worker per host
+# thread, the matrices spread over the workers (largest first) -------------
+_POOL_ITEMS, _POOL_SINGLE = None, False
+
+
+def _pool_init(items, single):
+    global _POOL_ITEMS, _POOL_SINGLE
+    from threadpoolctl import threadpool_limits
+
+    from oracle import oracle as O
+
+    threadpool_limits(limits=1)
+    O.set_threads(1)
+    _POOL_ITEMS, _POOL_SINGLE = items, single
+
+
+def _pool_expm(i):
+    from oracle import oracle as O
+
+    O.expm_blas(_POOL_ITEMS[i], single=_POOL_SINGLE)
+    return i
+
+
+def _pool_ready(_):
+    time.sleep(0.2)  # held long enough that every task lands on a worker of its own
+    return os.getpid()
+
+
+def _pool_vjp(i):
+    from oracle import oracle as O
+
+    a, g = _POOL_ITEMS[i]
+    O.expm_vjp_frechet(a, g, single=_POOL_SINGLE)
+    return i
+
+
+class MatrixPool:
+    """A process pool over a fixed sample of matrices (or adjoint pairs),
+    started with spawn (no worker inherits a CUDA context), every worker
+    started before any timing; run() evaluates the whole sample once. Each
+    pass has a time limit, so a pool whose workers cannot start raises
+    instead of waiting for good."""
+
+    LIMIT_S = 600.0
+
+    def __init__(self, items, sizes, single, workers):
+        import concurrent.futures as cf
+        import multiprocessing as mp
+
+        self.order = sorted(range(len(items)), key=lambda i: -sizes[i])
+        self.ex = cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"),
+                                         initializer=_pool_init, initargs=(items, single))
+        # the executor starts workers on demand: one blocking task per worker
+        # brings them all up now
+        list(self.ex.map(_pool_ready, range(workers), timeout=self.LIMIT_S))
+
+    def run(self, fn):
+        for _ in self.ex.map(fn, self.order, chunksize=1, timeout=self.LIMIT_S):
+            pass
+
+    def close(self):
+        self.ex.shutdown()
+
+
 CPU_FORM = ("the reference algorithm restated with its products on numpy's BLAS and its solve "
             "on LAPACK xGESV (bundled OpenBLAS), FP64")
 
@@ -279,8 +343,10 @@ def run_reference(args, cfg):
     threads, rank 0 only: the FP64 restatement with its products on numpy's
     BLAS and its solve on LAPACK (oracle.expm_blas; the C oracle's gebal
     sweep for the balanced config, xHEEVD for expm_herm). Batched: each step
-    is the first 32 matrices of the batch; adjoint: each step is one numpy
-    restatement of the adjoint (FP64, threaded BLAS)."""
+    is the first 8 matrices per host thread, spread over single-threaded
+    worker processes (32 in order on one thread); adjoint: the numpy
+    restatement of the adjoint (FP64), one 2048^2 pair on threaded BLAS, or
+    4 pairs of 128^2 per host thread over the workers."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -291,14 +357,22 @@ def run_reference(args, cfg):
     kind = cfg.get("kind", "single")
     dtype = {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[cfg["suf"]]
     single = cfg["suf"] in "sc"
+    pool = None
     if kind == "batched":
-        mats = [m.astype(np.float64) for m in batched_workload(cfg, range(32))]
+        count = 32 if cores == 1 else 8 * cores
+        mats = [m.astype(np.float64) for m in batched_workload(cfg, range(count))]
         per_step, unit = len(mats), "expm/s"
+        if cores == 1:
+            def one():
+                for m in mats:
+                    O.expm_blas(m, single=single)
+        else:
+            pool = MatrixPool(mats, [m.shape[0] ** 3 for m in mats], single, cores)
 
-        def one():
-            for m in mats:
-                O.expm_blas(m, single=single)
-        sample = "the first 32 matrices of the batch per step"
+            def one():
+                pool.run(_pool_expm)
+        sample = (f"the first {count} matrices of the batch per step"
+                  + (f", spread over {cores} single-threaded worker processes" if pool else ""))
         plan_info = None
     elif kind == "geodesic":
         w, hmat = geodesic_inputs(cfg)
@@ -310,14 +384,20 @@ def run_reference(args, cfg):
                   "products, all on numpy's threaded BLAS)")
         plan_info = None
     elif kind == "vjp":
-        k = 1 if cfg["n"] > 512 else 8
+        k = 1 if cfg["n"] > 512 else (8 if cores == 1 else 4 * cores)
         pairs = [vjp_pair(cfg["n"], cfg["norm"], 7000 + i) for i in range(k)]
         per_step, unit = k, "vjp/s"
+        if k == 1 or cores == 1:
+            def one():
+                for a, g in pairs:
+                    O.expm_vjp_frechet(a, g, single=single)
+        else:
+            pool = MatrixPool(pairs, [1] * k, single, cores)
 
-        def one():
-            for a, g in pairs:
-                O.expm_vjp_frechet(a, g, single=single)
-        sample = f"{k} adjoint(s) per step (numpy restatement of the adjoint)"
+            def one():
+                pool.run(_pool_vjp)
+        sample = (f"{k} adjoint(s) per step (numpy restatement of the adjoint)"
+                  + (f", spread over {cores} single-threaded worker processes" if pool else ""))
         plan_info = None
     else:
         x = make_matrix(cfg).astype(np.complex128 if cfg["suf"] in "cz" else np.float64)
@@ -337,12 +417,14 @@ def run_reference(args, cfg):
         if cfg.get("entry") == "expm_herm":
             sample += " (eigendecomposition route: LAPACK zheevd through numpy, threaded BLAS)"
         plan_info = holder if cfg.get("entry") != "expm_herm" else None
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, 1 if pool else 0)):  # a pool's workers start in its first pass
         one()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         one()
     el = time.perf_counter() - t0
+    if pool:
+        pool.close()
     value = per_step * args.steps / el
     config = {"workload": args.config, "desc": cfg["desc"]}
     if plan_info:
@@ -920,11 +1002,28 @@ def run_batched(args, cfg):
 
 def batched_cpu_sample(mats, suf, seconds=10.0):
     """The timing restatement (oracle.expm_blas) on the first matrices of the
-    batch until `seconds` pass."""
+    batch: one thread, matrices in order until `seconds` pass; more threads,
+    the first 16 per thread spread over single-threaded worker processes,
+    whole passes over them until `seconds` pass (after a warm-up pass)."""
     from oracle import oracle as O
 
     cores = cpu_threads()
     O.set_threads(cores)
+    if cores > 1:
+        sample = [m.astype(np.float64) for m in mats[:16 * cores]]
+        pool = MatrixPool(sample, [m.shape[0] ** 3 for m in sample], suf == "s", cores)
+        pool.run(_pool_expm)
+        passes, t0 = 0, time.perf_counter()
+        while True:
+            pool.run(_pool_expm)
+            passes += 1
+            el = time.perf_counter() - t0
+            if el >= seconds:
+                break
+        pool.close()
+        return {"value": passes * len(sample) / el, "unit": "expm/s", "cores": cores, "kind": "port",
+                "sample": f"{passes} passes over the first {len(sample)} matrices of the batch ({el:.1f} s) "
+                          f"on {cores} single-threaded worker processes, {CPU_FORM}"}
     done, t0 = 0, time.perf_counter()
     for m in mats:
         O.expm_blas(m.astype(np.float64), single=suf == "s")

@@ -51,3 +51,16 @@ def test_hbm_min_bound():
     assert d["bytes_per_step"] == 2 * (16 * 16 + 256 * 256) * 4
     assert abs(d["achieved_gbs"] - d["bytes_per_step"] / 2e-3 / 1e9) < 1e-12
     assert d["peak_gbs"] == peak and abs(d["frac"] - d["achieved_gbs"] / peak) < 1e-15
+
+
+def test_batched_reference_spreads_over_workers():
+    """More than one host thread: the batched sample runs on single-threaded
+    worker processes (spawned), one step = 8 matrices per thread."""
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--config", "expm_batched_f32_8192", "--steps", "1", "--warmup", "0",
+                        "--cpu-threads", "2"], capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert r.returncode == 0, r.stderr
+    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][0])
+    assert d["cpu_baseline"]["cores"] == 2 and d["value"] > 0
+    assert "the first 16 matrices" in d["cpu_baseline"]["sample"]
+    assert "2 single-threaded worker processes" in d["cpu_baseline"]["sample"]
