@@ -1036,6 +1036,43 @@ def batched_cpu_sample(mats, suf, seconds=10.0):
                       f"{threads_phrase(cores)}"}
 
 
+def vjp_cpu_sample(pairs, single, seconds=10.0):
+    """The CPU baseline of the adjoint: the numpy restatement (FP64) of what
+    the library computes. One pair: whole calls on threaded BLAS until
+    `seconds` pass (3 at most); many pairs: passes over the first 4 per host
+    thread, spread over single-threaded worker processes (in order on one
+    thread), until `seconds` pass."""
+    from oracle import oracle as O
+
+    cores = cpu_threads()
+    O.set_threads(cores)
+    if len(pairs) > 1 and cores > 1:
+        sample = pairs[:4 * cores]
+        pool = MatrixPool(sample, [1] * len(sample), single, cores)
+        pool.run(_pool_vjp)
+        done, t0 = 0, time.perf_counter()
+        while True:
+            pool.run(_pool_vjp)
+            done += len(sample)
+            el = time.perf_counter() - t0
+            if el >= seconds:
+                break
+        pool.close()
+        where = f"{len(sample)} pairs per pass on {cores} single-threaded worker processes"
+    else:
+        done, t0 = 0, time.perf_counter()
+        while True:
+            a, g = pairs[done % len(pairs)]
+            O.expm_vjp_frechet(a, g, single=single)
+            done += 1
+            el = time.perf_counter() - t0
+            if el >= seconds or (len(pairs) == 1 and done >= 3):
+                break
+        where = threads_phrase(cores)
+    return {"value": done / el, "unit": "vjp/s", "cores": cores, "kind": "port",
+            "sample": f"{done} adjoint(s) ({el:.1f} s), the numpy restatement of the adjoint (FP64), {where}"}
+
+
 def run_vjp(args, cfg):
     """One step = the adjoint of expm for the whole workload through the C ABI:
     one calaman_expm_vjp_<t> call (2048^2), or one calaman_expm_vjp_batched_<t>
@@ -1182,6 +1219,9 @@ def run_vjp(args, cfg):
             got = host_d[i].numpy().T.astype(np.float64)
             acc.setdefault("rel_frob_vs_oracle", []).append(
                 float(np.linalg.norm(got - ref) / np.linalg.norm(ref)))
+        baseline = None
+        if world == 1 and not args.no_cpu:
+            baseline = vjp_cpu_sample(pairs, suf == "s")
         line = {
             "metric": METRIC.replace("expm/s", "vjp/s"), "value": value, "unit": "vjp/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1198,7 +1238,7 @@ def run_vjp(args, cfg):
                          "kernel": "dense products (every GEMM launch in the timed steps)",
                          "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
                          "peak_source": peak_src},
-            "cpu_baseline": None,
+            "cpu_baseline": baseline,
             "e2e": {"value": e2e_value, "unit": "vjp/s",
                     "h2d_bytes_per_step": 2 * count * n * n * esz,
                     "d2h_bytes_per_step": count * n * n * esz,

@@ -64,3 +64,19 @@ def test_batched_reference_spreads_over_workers():
     assert d["cpu_baseline"]["cores"] == 2 and d["value"] > 0
     assert "the first 16 matrices" in d["cpu_baseline"]["sample"]
     assert "2 single-threaded worker processes" in d["cpu_baseline"]["sample"]
+
+
+def test_vjp_cpu_sample_one_thread():
+    """The adjoint lines' CPU baseline: the numpy restatement, timed whole."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    pairs = [bench.vjp_pair(64, 6.0, 7000 + i) for i in range(3)]
+    old = bench.CPU_THREADS
+    bench.CPU_THREADS = 1
+    try:
+        d = bench.vjp_cpu_sample(pairs, True, seconds=0.2)
+    finally:
+        bench.CPU_THREADS = old
+    assert d["unit"] == "vjp/s" and d["value"] > 0 and d["cores"] == 1 and d["kind"] == "port"
+    assert d["sample"].endswith("1 thread")
