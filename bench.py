@@ -2,28 +2,40 @@
 """Benchmark of the B200 matrix-exponential path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config expm_c128_1024] [--no-cpu] [--cpu-threads T]
+                    [--config expm_batched_f32_8192] [--no-cpu] [--cpu-threads T]
 
-One step = one expm of the workload matrix through the C ABI
-(calaman_expm_<t>). The default workload is the complex128 1024 x 1024
-matrix A = -iH, H = (X + X^H)/2 with X complex N(0,1) (GUE), rescaled to
-1-norm 50 (Pade degree 13, 4 squarings): seeded synthetic data of the shape
-the reference's headline configuration names.
+Default workload: 8192 float32 matrices, n uniform on {16, 32, ..., 256},
+N(0,1) entries rescaled to a 1-norm log-uniform in [0.1, 100] (seeded
+synthetic data). One step = one calaman_expm_batched_s call over the whole
+batch (the mixed tier: per-matrix (m, s), error <= 1e-6 against FP64). The
+same matrices, widened, also go through the plain FP64 tier
+(calaman_expm_batched_d) in the same run: `vs_fp64_tier` is the ratio of the
+two, the comparison the metric names. `--config` selects the single-matrix
+workloads (one calaman_expm_<t> call per step; the complex128 1024 x 1024
+A = -iH (GUE), 1-norm 50 case is `expm_c128_1024`), the adjoint and the
+other entry points.
 
 Printed (rank 0, one JSON line):
-  value       expm/s over all ranks, inputs resident in HBM, L2 flushed
-              (256 MiB write, untimed) before every timed step;
-  e2e         the same through the C ABI with pinned host buffers: H2D of A,
-              expm, D2H of exp(A), all inside the timed region;
-  roofline    dense-product throughput measured live with CUDA events around
-              every GEMM launch in the timed steps, against the FP64 tensor
-              peak measured in this run (cuBLAS complex128 GEMM, 4096^3);
+  value       units/s over all ranks, inputs resident in HBM (single
+              matrices: L2 flushed, 256 MiB write, untimed, before every
+              timed step; batches: inputs larger than L2), no
+              instrumentation in the timed steps;
+  e2e         the same through the C ABI with pinned host buffers: H2D of
+              the inputs, the call, D2H of the results, all timed;
+  roofline    dense-product throughput from a separate instrumented call
+              (CUDA events around every GEMM launch, algorithmic flops)
+              against the FP64 tensor peak measured in this run (cuBLAS
+              GEMM, 4096^3) or, for the single-precision tiers, the measured
+              BF16 peak (frac_executed counts the executed BF16 products);
   cpu_baseline  the reference algorithm restated in FP64 with its products on
               numpy's BLAS and its solve on LAPACK (the bundled OpenBLAS) on
-              this host's cores, on the same matrix; the C oracle (fixed
-              evaluation order) checks the result.
-With torchrun (N > 1) every rank runs its own replica (a single expm does not
-shard) and value = N * K / (max over ranks of the timed seconds).
+              this host's cores, on a bounded sample of the same workload;
+              the C oracle (fixed evaluation order) checks the result.
+With torchrun (N > 1) every rank runs its own replica of a single-matrix
+workload, or its cost-balanced share of a batch N times the size (weak
+scaling), and value = units over all ranks / max over ranks of the timed
+seconds. `--gpus N` without a launcher re-runs itself under
+torch.distributed.run with N ranks.
 `--impl reference` times that CPU restatement alone.
 `--cpu-threads T` limits both CPU legs to T host threads (1: the
 single-threaded baseline); the default uses every host thread.
@@ -45,6 +57,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "expm/s & TFLOP/s at rel err<=1e-6 vs FP64"
+# the metric's own comparison: the mixed batched tier against the plain FP64
+# tier on the same 8192 matrices
+DEFAULT_CONFIG = "expm_batched_f32_8192"
 
 CONFIGS = {
     # name: (n, type suffix, 1-norm, generator)
@@ -560,7 +575,6 @@ def run_ours(args, cfg):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = lib.calamanGetLaunchCount()
-    assert lib.calamanSetKernelTiming(h, 1).ok
     with ClockSampler(local) as clocks:
         with torch.cuda.stream(stream):
             for i in range(args.steps):
@@ -570,10 +584,17 @@ def run_ours(args, cfg):
                 ends[i].record(stream)
         torch.cuda.synchronize()
         launches = lib.calamanGetLaunchCount() - launches0
+        total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+        # instrumented steps (not in value): CUDA events around every GEMM launch
+        assert lib.calamanSetKernelTiming(h, 1).ok
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.zero_()
+                step()
+        torch.cuda.synchronize()
         kt = capi.KernelTiming()
         assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
         lib.calamanSetKernelTiming(h, 0)
-        total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
         # ---- e2e: pinned host in, pinned host out, through the C ABI ----
         e2e_ms = 0.0
@@ -601,7 +622,6 @@ def run_ours(args, cfg):
     if rank == 0:
         flops = herm_flops(n, cplx) if herm else expm_flops(n, plan.m, plan.s, cplx)
         achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
-        executed = None
         if suf == "s":
             # split-BF16 x6 tensor-core products: six BF16 products per FP32 product
             peak, peak_src = _bf16_peak()
@@ -610,6 +630,9 @@ def run_ours(args, cfg):
             peak = measure_fp64_peak(torch, dev, cplx)
             peak_src = ("cuBLAS complex128/float64 GEMM 4096^3 measured in this run "
                         "(MEASURED_PEAKS.json has no FP64 figure)")
+            # complex products run as three real products (Gauss): 6/8 of the
+            # algorithmic flops are executed on the tensor cores
+            executed = (0.75 * achieved if cplx else achieved) if achieved else None
         got = host_e.numpy().reshape(n, n).T
         acc = {}
         if oracle_result is not None:
@@ -632,11 +655,15 @@ def run_ours(args, cfg):
             "tflops": flops * value / 1e12,
             "algorithmic_flops_per_expm": flops,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (executed or achieved) / peak if achieved else None,
+                         "frac": achieved / peak if achieved else None,
                          "executed_tflops": executed,
+                         "frac_executed": executed / peak if executed else None,
                          "traffic": read_traffic(f"zgemm_{n}" if cplx else f"dgemm_{n}"),
-                         "kernel": "dense products (every GEMM launch in the timed steps); "
-                                   "achieved = algorithmic flops, frac from executed flops",
+                         "kernel": "dense products (every GEMM launch of instrumented steps run "
+                                   "after the timed ones); achieved and frac: algorithmic flops "
+                                   "(2n^3 real, 8n^3 complex per product); frac_executed: the "
+                                   "flops the tensor cores execute (3 real products per complex "
+                                   "one; 6 BF16 products per split-BF16 FP32 one)",
                          "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
                          "peak_source": peak_src},
             "cpu_baseline": baseline,
@@ -804,10 +831,65 @@ def _vjp_sub_batches(lib, capi, torch, dev, suf, n, count, dA, dG, dD, host_a, h
     return out
 
 
+def _batched_entry(lib, capi, torch, dev, suf, ns, offs, dIn, dOut, stream, info):
+    """A calaman_expm_batched_<suf> call over every matrix of the batch:
+    returns (call, plans, handle, workspace)."""
+    count = len(ns)
+    esz = dIn.element_size()
+    IntArr, PtrArr = ctypes.c_int * count, ctypes.c_void_p * count
+    h_n = IntArr(*ns)
+    h_A = PtrArr(*[dIn.data_ptr() + o * esz for o in offs])
+    h_E = PtrArr(*[dOut.data_ptr() + o * esz for o in offs])
+    h = ctypes.c_void_p()
+    assert lib.calamanCreate(ctypes.byref(h)).ok
+    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
+    nb = ctypes.c_size_t()
+    intp = ctypes.cast(h_n, capi.c_int_p)
+    assert getattr(lib, f"calaman_expm_batched_bufferSize_{suf}")(h, count, intp, ctypes.byref(nb)).ok
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    plans = (capi.ExpmPlan * count)()
+    fn = getattr(lib, f"calaman_expm_batched_{suf}")
+
+    def call():
+        st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), count, intp,
+                ctypes.cast(h_A, ctypes.POINTER(ctypes.c_void_p)), intp,
+                ctypes.cast(h_E, ctypes.POINTER(ctypes.c_void_p)), intp,
+                ctypes.c_void_p(work.data_ptr()), nb.value,
+                ctypes.cast(info.data_ptr(), capi.c_int_p), plans)
+        if not st.ok:
+            raise RuntimeError(f"expm_batched_{suf} failed: {st!r}")
+
+    call._keep = (h_n, h_A, h_E)
+    return call, plans, h, work
+
+
+def _time_steps(torch, stream, call, steps):
+    """CUDA-event time (ms) of `steps` back-to-back calls on `stream`."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for i in range(steps):
+            starts[i].record(stream)
+            call()
+            ends[i].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+
+
 def run_batched(args, cfg):
     """One step = one calaman_expm_batched_<t> call over the whole batch.
     Under torchrun the batch is split across ranks (matrices are
-    independent; balanced by sum n^3), no collective on the data path."""
+    independent; balanced by sum n^3), no collective on the data path.
+
+    For the mixed tier (float32 in/out) the same matrices, widened to
+    float64, also go through the plain FP64 tier in the same run, timed the
+    same way: `vs_fp64_tier` = mixed value / FP64-tier value, the ratio the
+    metric names, and `accuracy` = the mixed tier's worst relative Frobenius
+    error against the FP64 tier over every matrix.
+
+    `value` is timed with no instrumentation; the roofline's kernel figures
+    come from a separate pass with CUDA events around every grouped-GEMM
+    launch (calamanSetKernelTiming)."""
     torch, world, rank, local, dev, dist = _init_dist()
     from calaman_g_b200 import capi
 
@@ -846,56 +928,23 @@ def run_batched(args, cfg):
     dA = host_in.to(dev)
     dE = torch.empty_like(dA)
     esz = dA.element_size()
-    IntArr = ctypes.c_int * count
-    PtrArr = ctypes.c_void_p * count
-    h_n = IntArr(*ns)
-    h_A = PtrArr(*[dA.data_ptr() + o * esz for o in offs])
-    h_E = PtrArr(*[dE.data_ptr() + o * esz for o in offs])
     stream = torch.cuda.Stream(device=dev)
-    h = ctypes.c_void_p()
-    assert lib.calamanCreate(ctypes.byref(h)).ok
-    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
-    nb = ctypes.c_size_t()
-    intp = ctypes.cast(h_n, capi.c_int_p)
-    assert getattr(lib, f"calaman_expm_batched_bufferSize_{suf}")(h, count, intp, ctypes.byref(nb)).ok
-    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
     info = torch.zeros(2 * count, dtype=torch.int32, device=dev)
-    plans = (capi.ExpmPlan * count)()
-    fn = getattr(lib, f"calaman_expm_batched_{suf}")
-
-    def step():
-        st = fn(h, h, ctypes.c_void_p(stream.cuda_stream), count, intp,
-                ctypes.cast(h_A, ctypes.POINTER(ctypes.c_void_p)), intp,
-                ctypes.cast(h_E, ctypes.POINTER(ctypes.c_void_p)), intp,
-                ctypes.c_void_p(work.data_ptr()), nb.value,
-                ctypes.cast(info.data_ptr(), capi.c_int_p), plans)
-        if not st.ok:
-            raise RuntimeError(f"expm_batched failed: {st!r}")
+    step, plans, h, work = _batched_entry(lib, capi, torch, dev, suf, ns, offs, dA, dE, stream, info)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
     torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = lib.calamanGetLaunchCount()
-    assert lib.calamanSetKernelTiming(h, 1).ok
     with ClockSampler(local) as clocks:
-        with torch.cuda.stream(stream):
-            for i in range(args.steps):
-                starts[i].record(stream)
-                step()
-                ends[i].record(stream)
-        torch.cuda.synchronize()
+        # ---- value: inputs resident in HBM (larger than L2), no instrumentation
+        total_ms = _time_steps(torch, stream, step, args.steps)
         launches = lib.calamanGetLaunchCount() - launches0
-        kt = capi.KernelTiming()
-        assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
-        lib.calamanSetKernelTiming(h, 0)
-        total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-        # e2e as a user would pipeline it: the batch in sub-batches on their own
+        # ---- e2e as a user would pipeline it: the batch in sub-batches on their own
         # streams (one handle each), so one sub-batch's copies overlap another's
         # compute; every step still copies all inputs in and all results out
         subs = _sub_batches(lib, capi, torch, dev, suf, ns, offs, dA, dE, host_in, host_out, info,
@@ -918,10 +967,35 @@ def run_batched(args, cfg):
             e2e_ms += a_ev.elapsed_time(b_ev)
         for sb in subs:
             lib.calamanDestroy(sb["h"])
+        # ---- the plain FP64 tier on the same matrices, timed the same way
+        fp64_ms = None
+        if suf == "s":
+            h64in = torch.from_numpy(host_in.numpy().astype(np.float64)).to(dev)
+            e64 = torch.empty_like(h64in)
+            info64 = torch.zeros(2 * count, dtype=torch.int32, device=dev)
+            step64, plans64, h64, w64 = _batched_entry(lib, capi, torch, dev, "d", ns, offs, h64in, e64,
+                                                       stream, info64)
+            with torch.cuda.stream(stream):
+                for _ in range(args.warmup):
+                    step64()
+            torch.cuda.synchronize()
+            fp64_ms = _time_steps(torch, stream, step64, args.steps)
+    # ---- instrumented pass (not timed into value): CUDA events around every
+    # grouped-GEMM launch give the dense products' own throughput
+    assert lib.calamanSetKernelTiming(h, 1).ok
+    with torch.cuda.stream(stream):
+        step()
     torch.cuda.synchronize()
+    kt = capi.KernelTiming()
+    assert lib.calamanGetKernelTiming(h, ctypes.byref(kt)).ok
+    lib.calamanSetKernelTiming(h, 0)
     if any(info.cpu().tolist()):
         raise RuntimeError("an LU reported a zero pivot")
-    total_ms, e2e_ms = _max_over_ranks(torch, dist, dev, [total_ms, e2e_ms])
+    reduced = [total_ms, e2e_ms] + ([fp64_ms] if fp64_ms is not None else [])
+    reduced = _max_over_ranks(torch, dist, dev, reduced)
+    total_ms, e2e_ms = reduced[0], reduced[1]
+    if fp64_ms is not None:
+        fp64_ms = reduced[2]
     total_count = count
     if dist:
         tc = torch.tensor([count], dtype=torch.float64, device=dev)
@@ -932,36 +1006,32 @@ def run_batched(args, cfg):
     if rank == 0:
         pl = list(plans)
         flops = sum(expm_flops(n, p.m, p.s, False) for n, p in zip(ns, pl))
-        if suf == "s":
-            peak, peak_src = _bf16_peak()
-        else:  # the FP64 tier: every product on the FP64 tensor cores (DMMA)
-            peak, peak_src = measure_fp64_peak(torch, dev, False), "cuBLAS float64 GEMM 4096^3 in this run"
+        peak64 = measure_fp64_peak(torch, dev, False)
         achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
         acc = {}
+        fp64_tier = None
         if suf == "s":
-            # the FP32 tier against the FP64 tier (same widened values), all matrices
-            out32 = host_out.numpy()
-            h64 = torch.from_numpy(host_in.numpy().astype(np.float64)).to(dev)
-            e64 = torch.empty_like(h64)
-            nb64 = ctypes.c_size_t()
-            assert lib.calaman_expm_batched_bufferSize_d(h, count, intp, ctypes.byref(nb64)).ok
-            w64 = torch.empty(nb64.value, dtype=torch.uint8, device=dev)
-            A64 = PtrArr(*[h64.data_ptr() + o * 8 for o in offs])
-            E64 = PtrArr(*[e64.data_ptr() + o * 8 for o in offs])
-            st = lib.calaman_expm_batched_d(h, h, ctypes.c_void_p(stream.cuda_stream), count, intp,
-                                            ctypes.cast(A64, ctypes.POINTER(ctypes.c_void_p)), intp,
-                                            ctypes.cast(E64, ctypes.POINTER(ctypes.c_void_p)), intp,
-                                            ctypes.c_void_p(w64.data_ptr()), nb64.value,
-                                            ctypes.cast(info.data_ptr(), capi.c_int_p), None)
-            assert st.ok, st
+            # the mixed tier against the FP64 tier (same widened values), all matrices
+            with torch.cuda.stream(stream):
+                step()
+                host_out.copy_(dE, non_blocking=True)
             torch.cuda.synchronize()
+            out32 = host_out.numpy()
             ref = e64.cpu().numpy()
-            del w64, h64, e64
             worst = 0.0
             for n, o in zip(ns, offs):
                 x, y = out32[o:o + n * n].astype(np.float64), ref[o:o + n * n]
                 worst = max(worst, float(np.linalg.norm(x - y) / np.linalg.norm(y)))
             acc["max_rel_frob_vs_fp64_tier"] = worst
+            acc["bar"] = 1e-6
+            v64 = total_count * args.steps / (fp64_ms * 1e-3)
+            flops64 = sum(expm_flops(n, p.m, p.s, False) for n, p in zip(ns, list(plans64)))
+            fp64_tier = {"value": v64, "unit": "expm/s", "ms_per_step": fp64_ms / args.steps,
+                         "tflops": flops64 * v64 / count / 1e12,
+                         "entry": "calaman_expm_batched_d (every product on the FP64 tensor cores, "
+                                  "FP64 LU), the same matrices widened to float64"}
+            lib.calamanDestroy(h64)
+            del w64, h64in, e64
         baseline = None
         if world == 1 and not args.no_cpu:
             baseline = batched_cpu_sample(mats, suf, seconds=10.0)
@@ -977,11 +1047,19 @@ def run_batched(args, cfg):
                        "l2": "inputs (%.0f MB) larger than L2" % (host_in.numel() * esz / 1e6),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "tflops": flops * value / count / 1e12,
-            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if achieved else None, "traffic": None,
-                         "kernel": "grouped dense-product phases (every grouped GEMM launch)",
-                         "launches": kt.gemm_launches, "kernel_ms_per_step": kt.gemm_ms / args.steps,
-                         "peak_source": peak_src},
+        }
+        if fp64_tier:
+            line["vs_fp64_tier"] = value / fp64_tier["value"]
+            line["fp64_tier"] = fp64_tier
+        line.update({
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                         "frac": achieved / peak64 if achieved else None,
+                         "flops": "algorithmic (2 n^3 per product)", "traffic": None,
+                         "kernel": "grouped dense-product phases (every grouped GEMM launch of one "
+                                   "instrumented call), against the FP64 tensor peak",
+                         "launches": kt.gemm_launches, "kernel_ms_per_call": kt.gemm_ms,
+                         "peak_source": "cuBLAS float64 GEMM 4096^3 measured in this run "
+                                        "(MEASURED_PEAKS.json has no FP64 figure)"},
             "hbm_min": hbm_min(ns, esz, total_ms / args.steps),
             "cpu_baseline": baseline,
             "e2e": {"value": e2e_value, "unit": "expm/s",
@@ -992,7 +1070,7 @@ def run_batched(args, cfg):
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "accuracy": acc,
-        }
+        })
         print(json.dumps(line), flush=True)
     lib.calamanDestroy(h)
     if dist:
@@ -1384,18 +1462,35 @@ def run_geodesic(args, cfg):
         dist.destroy_process_group()
 
 
+def _relaunch_under_torchrun(nproc):
+    """`--gpus N` without a launcher: run this same command as N ranks of one
+    node under torch.distributed.run (rendezvous on 127.0.0.1)."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__),
+           *sys.argv[1:]]
+    sys.stdout.flush()
+    os.execv(sys.executable, cmd)
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", default="expm_c128_1024", choices=sorted(CONFIGS))
+    p.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     p.add_argument("--cpu-threads", type=int, default=0,
                    help="host threads of the CPU baseline and the reference arm (numpy's "
                         "BLAS and the C oracle's workers); 0: every host thread")
     args = p.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        _relaunch_under_torchrun(args.gpus)
     global CPU_THREADS
     CPU_THREADS = max(0, args.cpu_threads)
     if CPU_THREADS:

@@ -12,7 +12,13 @@
 // The array is kNoAllocScratchBytes (4 MiB) and every GPU that loads the
 // library holds it until the process exits. Its device address is looked up
 // once per device, on the first call made with that device current; make that
-// first call before any stream capture. Every call shares the one array, so
+// first call before any stream capture. The address is kept for the life of
+// the process: a cudaDeviceReset after the first call on a device (which
+// reloads the module into a new context, where the array may sit elsewhere)
+// is not supported. Like calaman_expm_d, every call synchronises its stream
+// once, to read the 1-norm back for the (m, s) plan; a caller that already
+// knows the plan and must not synchronise uses calaman_pade_d and the
+// squarings itself. Every call shares the one array, so
 // calls that overlap on the GPU (other streams, other host threads) race on
 // it; serialise them. Nothing in the array needs to start at zero: each call
 // initialises everything it reads, and the array keeps the last call's data.

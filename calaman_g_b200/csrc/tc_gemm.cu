@@ -215,13 +215,25 @@ __global__ void __launch_bounds__(kThreads, 1)
         umma(tmem, smem_desc(a0 + k * 32), smem_desc(b0 + k * 32), (it > 0 || k > 0) ? 1u : 0u);
       umma_commit(&empty[s]);
     }
-    if (ok) umma_commit(acc_full);
-    else *(volatile int *)abort_flag = 1;
+    if (!ok) *(volatile int *)abort_flag = 1;
+    // The commit tracks every MMA issued above, so it is made on the abort
+    // path too; this thread then waits for it, so no MMA still reads shared
+    // memory or writes TMEM when the CTA frees its TMEM and exits.
+    umma_commit(acc_full);
+    if (!mbar_wait(acc_full, 0)) record_error(prm.err, 4);
   } else if (warp >= 2) {
     // ---- epilogue ----
     const int q = warp & 3;  // TMEM lane quarter this warp may access
-    bool ok = mbar_wait(acc_full, 0);
-    if (!ok) record_error(prm.err, 3);
+    // bounded wait for the accumulator; gives up early once the CTA aborted
+    bool ok = false;
+    for (long long i = 0; i < kSpinLimit; ++i) {
+      if (mbar_try_wait(acc_full, 0)) {
+        ok = true;
+        break;
+      }
+      if ((i & 1023) == 1023 && *(volatile int *)abort_flag) break;
+    }
+    if (!ok && !*(volatile int *)abort_flag) record_error(prm.err, 3);
     if (ok && !*(volatile int *)abort_flag) {
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int m = m0 + q * 32 + lane;

@@ -372,7 +372,9 @@ calamanStatus_t calaman_lacn2_d(calamanBlasHandle_t blas, int n, double *d_v, do
  * library, for n <= 256; larger n returns CALAMAN_STATUS_NOT_SUPPORTED. The
  * array is resident on every GPU that loads the library until exit. Its
  * address is looked up on the first call made on each device: make that
- * first call before any stream capture. All calls share the array, so calls
+ * first call before any stream capture. The address is kept for the life of
+ * the process, so cudaDeviceReset after that first call is not supported.
+ * All calls share the array, so calls
  * that overlap on the GPU race on it: serialise them. Nothing in it needs to
  * start at zero; it keeps the last call's data. Same results, status codes
  * and single stream synchronisation as calaman_expm_d. */

@@ -38,7 +38,7 @@ def run(cuda):
     r.close()
 
 
-def test_matches_expm_on_two_calls_in_a_row(run):
+def test_matches_expm_on_two_calls_in_a_row(run, oracle):
     cases = [gaussian_scaled(200, 5.0, 11), gaussian_scaled(256, 40.0, 12)]  # m=13 s=0; s=3
     for a in cases:
         st, plan, got, info = noalloc(run, a)
@@ -47,6 +47,9 @@ def test_matches_expm_on_two_calls_in_a_row(run):
         assert (plan.m, plan.s) == (plan2.m, plan2.s)
         assert info == [0, 0] and list(info2) == [0, 0]
         assert rel_frob(got, want) <= TOL
+        ref, oplan, _ = oracle.expm(a)  # and the FP64 oracle itself
+        assert (plan.m, plan.s) == (oplan.m, oplan.s)
+        assert rel_frob(got, ref) <= TOL
 
 
 def test_rejects_sizes_beyond_the_static_workspace(run):
