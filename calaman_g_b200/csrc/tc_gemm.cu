@@ -25,10 +25,13 @@
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace clm {
 
 namespace {
+
+using namespace tc;
 
 constexpr int TM = 128;       // UMMA M (TMEM lanes)
 constexpr int TN = 256;       // UMMA N (TMEM columns)
@@ -38,7 +41,6 @@ constexpr int STAGES = 4;
 constexpr int kThreads = 192;
 constexpr int kA = TM * TK * 2;  // bytes of one A stage
 constexpr int kB = TN * TK * 2;  // bytes of one B stage
-constexpr long long kSpinLimit = 1ll << 26;
 
 struct TcParams {
   int M, N, nkb;        // nkb: k-blocks per part product (Kpad / TK)
@@ -51,91 +53,14 @@ struct TcParams {
   int *err;
 };
 
-__device__ __forceinline__ uint32_t saddr(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(saddr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait on the phase of the given parity; false when it ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (long long i = 0; i < kSpinLimit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x,
-                                            int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(saddr(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(saddr(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile whose
-// 8-row groups are 1024 bytes apart (sm_100 descriptor version 1).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFFu);  // start address (16-byte units)
-  d |= (uint64_t)1u << 16;                 // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024u >> 4) << 32;       // stride byte offset: 8 rows x 128 B
-  d |= (uint64_t)1u << 46;                 // descriptor version
-  d |= (uint64_t)2u << 61;                 // swizzle: 128 B
-  return d;
-}
-
 // Instruction descriptor: bf16 x bf16 -> f32, both K-major, M = TM, N = TN.
-constexpr uint32_t kIdesc = (1u << 4)              // D format f32
-                            | (1u << 7)            // A format bf16
-                            | (1u << 10)           // B format bf16
-                            | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+constexpr uint32_t kIdesc = idesc_bf16_f32(TM, TN);
 
 __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(acc));
+  mma_f16(tmem_d, a, b, kIdesc, acc);
 }
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   saddr(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
-      "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-        "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
-        "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
-        "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void record_error(int *err, int code) {
-  if (err) atomicCAS(err, 0, code);
-}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) { mma_commit(bar); }
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) { return smem_desc_sw128(addr); }
 
 __global__ void __launch_bounds__(kThreads, 1)
     tc_split_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
@@ -321,34 +246,9 @@ __global__ void split_b_kernel(int K, int N, const float *__restrict__ B, int ld
 }
 
 // ---- host side ----------------------------------------------------------------
-using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (fn == nullptr) {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
-  return fn;
-}
-
 // A row-major bf16 matrix of `rows` x `cols` (cols contiguous), boxes of box_rows x 64.
 bool make_map(CUtensorMap *map, void *ptr, long long rows, long long cols, int box_rows) {
-  EncodeTiledFn fn = encode_fn();
-  if (fn == nullptr) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return make_rowmajor_map_sw128(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, ptr, rows, cols * 2, box_rows);
 }
 
 struct SplitLayout {
@@ -367,6 +267,31 @@ SplitLayout split_layout(int M, int N, int K, int nparts) {
 }
 
 }  // namespace
+
+EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  if (fn == nullptr) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+bool make_rowmajor_map_sw128(CUtensorMap *map, CUtensorMapDataType type, int elem_bytes, void *ptr,
+                             long long rows, long long row_bytes, int box_rows) {
+  EncodeTiledFn fn = tensor_map_encoder();
+  if (fn == nullptr || row_bytes % 16 != 0 || row_bytes < 128) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)(row_bytes / elem_bytes), (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+  const cuuint32_t box[2] = {(cuuint32_t)(128 / elem_bytes), (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, type, 2, ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms) {
   return split_layout(M, N, K, terms == 3 ? 2 : 3).total;
