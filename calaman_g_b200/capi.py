@@ -138,6 +138,11 @@ for _suf, _real in (("s", c_float), ("d", c_double), ("c", c_float), ("z", c_dou
 SIGNATURES["calaman_getrf_bufferSize"] = (Status, [c_int, c_size_t_p])
 SIGNATURES["calaman_gemm_bf16x_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_size_t_p])
 SIGNATURES["calaman_gemm_bf16x_s"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
+SIGNATURES["calaman_gemm_ozaki_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_int, c_size_t_p])
+SIGNATURES["calaman_gemm_ozaki_d"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
+SIGNATURES["calaman_gemm_ozaki_z"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
+SIGNATURES["calaman_gemm_ozaki_wait_check"] = (Status, [c_void_p, ctypes.c_longlong, c_void_p, c_size_t,
+                                                        c_int_p])
 SIGNATURES["calaman_expm_noalloc_d"] = (Status, [_H, c_void_p, c_int, c_void_p, c_int, c_void_p,
                                                  c_int, c_int_p, ctypes.POINTER(ExpmPlan)])
 # expm_batched: blas, solver, stream, batch, h_n, h_A, h_lda, h_E, h_lde, work, bytes, info, plans

@@ -623,6 +623,52 @@ calamanStatus_t calaman_gemm_bf16x_s(calamanStream_t stream, int m, int n, int k
   return ok_status();
 }
 
+calamanStatus_t calaman_gemm_ozaki_bufferSize(int m, int n, int k, int is_complex, int digits,
+                                              size_t *bytes) {
+  if (m < 1 || n < 1 || k < 1 || bytes == nullptr || !oz_gemm_supported(k, is_complex != 0, digits))
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  *bytes = oz_gemm_workspace_bytes(m, n, k, is_complex != 0, digits);
+  return ok_status();
+}
+
+#define CLM_OZ_API(SUF, T, PT, CPT, CPLX)                                                           \
+  calamanStatus_t calaman_gemm_ozaki_##SUF(calamanStream_t stream, int m, int n, int k, double alpha, \
+                                          CPT A, int lda, CPT B, int ldb, double beta, PT C, int ldc, \
+                                          int digits, void *work, size_t work_bytes) {              \
+    if (m < 1 || n < 1 || k < 1 || lda < m || ldb < k || ldc < m || A == nullptr || B == nullptr ||  \
+        C == nullptr || work == nullptr || !oz_gemm_supported(k, CPLX, digits))                      \
+      return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                             \
+    if (work_bytes < oz_gemm_workspace_bytes(m, n, k, CPLX, digits))                                \
+      return blas_status(CALAMAN_STATUS_ALLOC_FAILED);                                              \
+    CLM_CUDA(oz_gemm<T>(static_cast<cudaStream_t>(stream), m, n, k, alpha,                          \
+                        reinterpret_cast<const T *>(A), lda, reinterpret_cast<const T *>(B), ldb,   \
+                        beta, reinterpret_cast<T *>(C), ldc, work, work_bytes, digits));            \
+    return ok_status();                                                                             \
+  }
+CLM_OZ_API(d, double, double *, const double *, false)
+CLM_OZ_API(z, double2, void *, const void *, true)
+#undef CLM_OZ_API
+
+calamanStatus_t calaman_gemm_ozaki_wait_check(calamanStream_t stream, long long spin, void *work,
+                                              size_t work_bytes, int *code) {
+  constexpr int n = 128;
+  const std::size_t ws = oz_gemm_workspace_bytes(n, n, n, false, 2);
+  const std::size_t mat = (std::size_t)n * n * sizeof(double);
+  if (work == nullptr || code == nullptr || spin < 1) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (work_bytes < align_up(ws, 256) + 3 * mat) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char *w = static_cast<char *>(work);
+  double *A = reinterpret_cast<double *>(w + align_up(ws, 256));
+  double *B = A + (std::size_t)n * n, *C = B + (std::size_t)n * n;
+  CLM_CUDA(cudaMemsetAsync(work, 0, align_up(ws, 256) + 3 * mat, st));
+  CLM_CUDA(oz_gemm<double>(st, n, n, n, 1.0, A, n, B, n, 0.0, C, n, work, ws, 2, spin, /*skip_loads=*/1));
+  int h = 0;
+  CLM_CUDA(cudaMemcpyAsync(&h, work, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CLM_CUDA(cudaStreamSynchronize(st));
+  *code = h;
+  return ok_status();
+}
+
 calamanStatus_t calaman_getrf_bufferSize(int n, size_t *bytes) {
   if (n < 1 || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   *bytes = lu_scratch_bytes(n);

@@ -74,6 +74,20 @@ cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const
                         const float *B, int ldb, double beta, float *C, int ldc, void *ws,
                         std::size_t ws_bytes, int terms);
 
+// FP64 / complex128 GEMM on the INT8 tensor cores by the Ozaki splitting
+// scheme (oz_gemm.cu): `ks` signed 7-bit digits per operand element (row
+// scaling of A, column scaling of B), digit pairs of total weight < ks, exact
+// int32 level sums; needs oz_gemm_workspace_bytes of scratch. spin: tries of
+// every bounded wait (0: the default limit); skip_loads: test-only, the
+// producer issues no copy so that the waits run out and the kernel returns its
+// error code in the first workspace word.
+std::size_t oz_gemm_workspace_bytes(int M, int N, int K, bool cplx, int ks);
+bool oz_gemm_supported(int K, bool cplx, int ks);
+template <typename T>
+cudaError_t oz_gemm(cudaStream_t s, int M, int N, int K, double alpha, const T *A, int lda, const T *B,
+                    int ldb, double beta, T *C, int ldc, void *ws, std::size_t ws_bytes, int ks,
+                    long long spin = 0, int skip_loads = 0);
+
 // ---- LU with partial pivoting and the n-RHS solve -------------------------
 // Scratch the LU needs beyond the matrix: ipiv (n ints), perm (n ints) and a
 // small swap map; bytes for an n x n factorisation.

@@ -481,6 +481,35 @@ calamanStatus_t calaman_gemm_bf16x_s(calamanStream_t stream, int m, int n, int k
 calamanStatus_t calamanSetFloatSplit(calamanHandle_t handle, int terms);
 calamanStatus_t calamanGetFloatSplit(calamanHandle_t handle, int *terms);
 
+/* FP64 / complex128 GEMM C = alpha A B + beta C (column-major, no transposes,
+ * real alpha and beta) on the INT8 tensor cores by the Ozaki splitting scheme:
+ * each row of A and each column of B is scaled by the power of two of its
+ * largest magnitude and cut into `digits` signed 7-bit digits; the digit
+ * products of total weight < digits are summed exactly in int32 and combined
+ * in FP64. Error about 2^(-7 digits) relative to |A||B| row by column
+ * (digits = 7: 49 bits, FP64-grade for the expm path). Stands in for the
+ * reference's wwr::gemm FP64 products (src/expm/pade.cppm:115-136,162,176,180;
+ * src/expm/expm.cppm:160-165) where it is faster than the FP64 tensor cores.
+ * digits in 2..8, k (2k for _z) small enough that digits * 127^2 * k < 2^31.
+ * `work` holds the digit planes (calaman_gemm_ozaki_bufferSize bytes, 256-byte
+ * aligned); its first word receives a nonzero code if a bounded wait of the
+ * kernel ran out. Never synchronises. */
+calamanStatus_t calaman_gemm_ozaki_bufferSize(int m, int n, int k, int is_complex, int digits,
+                                              size_t *bytes);
+calamanStatus_t calaman_gemm_ozaki_d(calamanStream_t stream, int m, int n, int k, double alpha,
+                                     const double *A, int lda, const double *B, int ldb, double beta,
+                                     double *C, int ldc, int digits, void *work, size_t work_bytes);
+calamanStatus_t calaman_gemm_ozaki_z(calamanStream_t stream, int m, int n, int k, double alpha,
+                                     const void *A, int lda, const void *B, int ldb, double beta,
+                                     void *C, int ldc, int digits, void *work, size_t work_bytes);
+/* Self-test of the tensor-core kernels' bounded waits: runs the Ozaki GEMM
+ * kernel once (128^3) with its producer issuing no copy and every wait limited
+ * to `spin` tries, so that the waits run out; synchronises and returns in *code
+ * the error code the kernel recorded (nonzero: the kernel gave up and unwound
+ * instead of hanging). `work`: at least 1 MiB of device memory. */
+calamanStatus_t calaman_gemm_ozaki_wait_check(calamanStream_t stream, long long spin, void *work,
+                                              size_t work_bytes, int *code);
+
 /* LU with partial pivoting and the n-right-hand-side solve that pade() runs on
  * q_m(A) (the reference calls the solver library's getrf/getrs through
  * WarpWraps, src/expm/pade.cppm:186-188). LAPACK semantics: P A = L U, pivot
