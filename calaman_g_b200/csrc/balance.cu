@@ -231,14 +231,14 @@ template <typename T>
 calamanStatus_t expm_entry(calamanHandle_t blas, calamanStream_t stream, int n, const T *A, int lda, T *E,
                            int lde, void *work, std::size_t lwork, int *d_info, calamanExpmPlan_t *plan);
 template <typename T>
-std::size_t expm_workspace_bytes(int n);
+std::size_t expm_workspace_bytes(calamanHandle_t h, int n);
 
 namespace {
 
 template <typename T>
-std::size_t balanced_bytes(int n) {
+std::size_t balanced_bytes(calamanHandle_t h, int n) {
   BalWs<T> w;
-  return w.carve(nullptr, n) + expm_workspace_bytes<T>(n);
+  return w.carve(nullptr, n) + expm_workspace_bytes<T>(h, n);
 }
 
 template <typename T>
@@ -247,7 +247,7 @@ calamanStatus_t expm_balanced_api(calamanHandle_t blas, calamanStream_t stream, 
                                   calamanExpmPlan_t *plan) {
   if (n < 1 || n > kMaxDim || lda < n || lde < n || work == nullptr)
     return blas_status(CALAMAN_STATUS_INVALID_VALUE);
-  if (lwork < balanced_bytes<T>(n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  if (lwork < balanced_bytes<T>(blas, n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
   if (A == nullptr || E == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   BalWs<T> ws;
@@ -283,9 +283,9 @@ calamanStatus_t calaman_gebal_bufferSize(int n, int *lwork_ints) {
     return gebal_run<T>(static_cast<cudaStream_t>(stream), job, n, reinterpret_cast<T *>(A), lda, ilo, \
                         ihi, d_scale, d_work, max_sweeps > 0 ? max_sweeps : kGebalMaxSweeps, sweeps);  \
   }                                                                                                    \
-  calamanStatus_t calaman_expm_balanced_bufferSize_##SUF(calamanSolverHandle_t, int n, size_t *bytes) { \
+  calamanStatus_t calaman_expm_balanced_bufferSize_##SUF(calamanSolverHandle_t h, int n, size_t *bytes) { \
     if (n < 1 || n > kMaxDim || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);     \
-    *bytes = balanced_bytes<T>(n);                                                                     \
+    *bytes = balanced_bytes<T>(h, n);                                                                  \
     return ok_status();                                                                                \
   }                                                                                                    \
   calamanStatus_t calaman_expm_balanced_##SUF(calamanBlasHandle_t blas, calamanSolverHandle_t,         \

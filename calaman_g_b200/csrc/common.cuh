@@ -224,6 +224,13 @@ struct GemmScratch {
   void *ptr = nullptr;
   std::size_t bytes = 0;
   int terms = 6;  // 3 or 6 bf16 part products
+  // FP64 / complex128 products emulated on the INT8 tensor cores (oz_gemm):
+  // digit planes, digits per operand, and the smallest M, N and K that take
+  // that path (smaller products stay on the FP64 tensor cores)
+  void *oz = nullptr;
+  std::size_t oz_bytes = 0;
+  int oz_digits = 0;
+  int oz_min_dim = 0;
 };
 extern thread_local GemmScratch *tl_gemm_scratch;
 struct GemmScratchScope {
@@ -311,5 +318,6 @@ struct calamanContext {
   int sm_count = 0;
   double *h_pinned = nullptr;  // pinned host slots for the 1-norm readback
   int split_terms = 6;         // bf16 part products per FP32 product (3 or 6)
+  int fp64_digits = -1;        // FP64 products: -1 by size, 0 FP64 tensor cores, else Ozaki digits
   clm::KernelTimer timer;
 };

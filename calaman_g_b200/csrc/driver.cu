@@ -29,7 +29,9 @@ struct PadeWs {
   void *lu = nullptr;
   void *tc = nullptr;
   std::size_t tc_bytes = 0;
-  std::size_t carve(void *base, int n, int m) {
+  void *oz = nullptr;  // digit planes of the emulated FP64 products (oz_bytes > 0)
+  std::size_t oz_bytes = 0;
+  std::size_t carve(void *base, int n, int m, std::size_t ozb) {
     Layout L(base);
     const std::size_t nn = (std::size_t)n * n;
     const int np = pade_num_powers(m);
@@ -40,9 +42,12 @@ struct PadeWs {
     lu = L.take<char>(lu_scratch_bytes(n));
     tc_bytes = tc_scratch_bytes<T>(n);
     if (tc_bytes) tc = L.take<char>(tc_bytes);
+    oz_bytes = ozb;
+    if (oz_bytes) oz = L.take<char>(oz_bytes);
     return L.used;
   }
 };
+
 
 // expm(): [As (also the squaring scratch) | colsum | norm | (single tiers: two
 // FP64 n x n squaring buffers) | pade region]
@@ -66,31 +71,28 @@ struct ExpmWs {
 };
 
 template <typename T>
-std::size_t pade_bytes(int n, int m) {
+std::size_t pade_bytes(calamanHandle_t h, int n, int m) {
   PadeWs<T> w;
-  return w.carve(nullptr, n, m);
+  return w.carve(nullptr, n, m, oz_scratch_bytes<T>(h, n));
 }
 
 template <typename T>
-std::size_t expm_bytes(int n) {
+std::size_t expm_bytes(calamanHandle_t h, int n) {
   ExpmWs<T> e;
   std::size_t worst = 0;
-  for (int m : {3, 5, 7, 9, 13}) worst = std::max(worst, pade_bytes<T>(n, m));
+  for (int m : {3, 5, 7, 9, 13}) worst = std::max(worst, pade_bytes<T>(h, n, m));
   return e.carve(nullptr, n) + worst;
 }
 
 // ---- pade<T>, src/expm/pade.cppm:77-191 -------------------------------------
 template <typename T>
 calamanStatus_t pade_run(cudaStream_t st, int m, int n, const T *A, int lda, T *R, int ldr,
-                         void *work, int *d_info, int split_terms) {
+                         void *work, int *d_info, calamanHandle_t h) {
   const double *b = pade_coeffs(m);
   PadeWs<T> ws;
-  ws.carve(work, n, m);
-  GemmScratch gs;
-  gs.ptr = ws.tc;
-  gs.bytes = ws.tc_bytes;
-  gs.terms = split_terms;
-  GemmScratchScope gss(ws.tc ? &gs : nullptr);
+  ws.carve(work, n, m, oz_scratch_bytes<T>(h, n));
+  GemmScratch gs = lend_scratch<T>(h, n, ws.tc, ws.tc_bytes, ws.oz, ws.oz_bytes);
+  GemmScratchScope gss((ws.tc || ws.oz) ? &gs : nullptr);
   const int np = pade_num_powers(m);
   auto mm = [&](const T *X, int ldx, const T *Y, int ldy, double beta, T *Z) {
     return gemm_nn<T>(st, n, n, n, 1.0, X, ldx, Y, ldy, beta, Z, n);
@@ -133,12 +135,11 @@ calamanStatus_t pade_api(calamanHandle_t blas, calamanStream_t stream, int m, in
                          int lda, T *R, int ldr, void *work, std::size_t lwork, int *d_info) {
   if (pade_coeffs(m) == nullptr || n < 1 || n > kMaxDim || lda < n || ldr < n || work == nullptr)
     return blas_status(CALAMAN_STATUS_INVALID_VALUE);
-  if (lwork < pade_bytes<T>(n, m)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  if (lwork < pade_bytes<T>(blas, n, m)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
   if (A == nullptr || R == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   PointerModeScope pm(blas);
   TimerScope ts(timer_of(blas));
-  return pade_run<T>(static_cast<cudaStream_t>(stream), m, n, A, lda, R, ldr, work, d_info,
-                     split_terms_of(blas));
+  return pade_run<T>(static_cast<cudaStream_t>(stream), m, n, A, lda, R, ldr, work, d_info, blas);
 }
 
 // ---- expm<T>, src/expm/expm.cppm:87-174 -------------------------------------
@@ -149,7 +150,7 @@ calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, co
   using R = typename elem<T>::real;
   if (n < 1 || n > kMaxDim || lda < n || lde < n || work == nullptr)
     return blas_status(CALAMAN_STATUS_INVALID_VALUE);
-  if (lwork < expm_bytes<T>(n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  if (lwork < expm_bytes<T>(blas, n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
   if (A == nullptr || E == nullptr || d_info == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   PointerModeScope pm(blas);
   TimerScope ts(timer_of(blas));
@@ -176,7 +177,13 @@ calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, co
     src = ws.As;
     ld_src = n;
   }
-  CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info, split_terms_of(blas)));
+  CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info, blas));
+
+  // the squarings borrow the (now free) Pade region's digit planes
+  PadeWs<T> pw;
+  pw.carve(ws.pade, n, chosen.m, oz_scratch_bytes<T>(blas, n));
+  GemmScratch gs = lend_scratch<T>(blas, n, nullptr, 0, pw.oz, pw.oz_bytes);
+  GemmScratchScope gss(pw.oz ? &gs : nullptr);
 
   if (elem<T>::single && chosen.s > 0) {
     // single tiers: the squarings, where errors grow, run in FP64 tensor cores
@@ -347,13 +354,13 @@ calamanStatus_t expm_entry(calamanHandle_t blas, calamanStream_t stream, int n, 
   return expm_api<T>(blas, stream, n, A, lda, E, lde, work, lwork, d_info, plan);
 }
 template <typename T>
-std::size_t expm_workspace_bytes(int n) {
-  return expm_bytes<T>(n);
+std::size_t expm_workspace_bytes(calamanHandle_t h, int n) {
+  return expm_bytes<T>(h, n);
 }
 #define CLM_INST_ENTRY(T)                                                                              \
   template calamanStatus_t expm_entry<T>(calamanHandle_t, calamanStream_t, int, const T *, int, T *, int, \
                                          void *, std::size_t, int *, calamanExpmPlan_t *);              \
-  template std::size_t expm_workspace_bytes<T>(int);
+  template std::size_t expm_workspace_bytes<T>(calamanHandle_t, int);
 CLM_INST_ENTRY(float)
 CLM_INST_ENTRY(double)
 CLM_INST_ENTRY(float2)
@@ -454,16 +461,16 @@ int calaman_pade_num_powers(int m) { return pade_coeffs(m) ? pade_num_powers(m) 
 int calaman_pade_num_gemms(int m) { return pade_coeffs(m) ? pade_num_gemms(m) : 0; }
 
 #define CLM_BUFSZ(SUF, T)                                                                     \
-  calamanStatus_t calaman_expm_bufferSize_##SUF(calamanSolverHandle_t, int n, size_t *bytes) { \
+  calamanStatus_t calaman_expm_bufferSize_##SUF(calamanSolverHandle_t h, int n, size_t *bytes) { \
     if (n < 1 || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);          \
-    *bytes = expm_bytes<T>(n);                                                                \
+    *bytes = expm_bytes<T>(h, n);                                                             \
     return ok_status();                                                                       \
   }                                                                                           \
-  calamanStatus_t calaman_pade_bufferSize_##SUF(calamanSolverHandle_t, int m, int n,          \
+  calamanStatus_t calaman_pade_bufferSize_##SUF(calamanSolverHandle_t h, int m, int n,        \
                                                 size_t *bytes) {                              \
     if (pade_coeffs(m) == nullptr || n < 1 || bytes == nullptr)                               \
       return blas_status(CALAMAN_STATUS_INVALID_VALUE);                                       \
-    *bytes = pade_bytes<T>(n, m);                                                             \
+    *bytes = pade_bytes<T>(h, n, m);                                                          \
     return ok_status();                                                                       \
   }
 CLM_BUFSZ(s, float)
@@ -586,6 +593,19 @@ CLM_GEMM_API(d, double, double *, const double *)
 CLM_GEMM_API(c, float2, void *, const void *)
 CLM_GEMM_API(z, double2, void *, const void *)
 #undef CLM_GEMM_API
+
+calamanStatus_t calamanSetDoubleEmulation(calamanHandle_t handle, int digits) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (digits < -1 || digits == 1 || digits > 8) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  handle->fp64_digits = digits;
+  return ok_status();
+}
+
+calamanStatus_t calamanGetDoubleEmulation(calamanHandle_t handle, int *digits) {
+  if (handle == nullptr || digits == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  *digits = handle->fp64_digits;
+  return ok_status();
+}
 
 calamanStatus_t calamanSetFloatSplit(calamanHandle_t handle, int terms) {
   if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);

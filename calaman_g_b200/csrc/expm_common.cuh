@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cmath>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -91,6 +92,48 @@ inline calamanExpmPlan_t plan_for(R norm1) {
 // scratch sized for the largest (n x n x n) product of the evaluation.
 template <typename T> inline std::size_t tc_scratch_bytes(int n) {
   return std::is_same<T, float>::value ? tc_gemm_workspace_bytes(n, n, n, 6) : 0;
+}
+
+// FP64 / complex128 products on the INT8 tensor cores (Ozaki scheme): by
+// default for products of at least kOzAutoMinDim in every dimension, where it
+// measured faster than the FP64 tensor cores (2048^3: 405 against 551 us real,
+// 1383 against 1856 us complex), with kOzAutoDigits digits (49 bits); a handle
+// can turn it off or force it with a digit count (calamanSetDoubleEmulation).
+inline constexpr int kOzAutoMinDim = 1536;
+inline constexpr int kOzAutoDigits = 7;
+inline constexpr int kOzForcedMinDim = 128;
+
+template <typename T> inline int oz_digits_for(calamanHandle_t h, int n) {
+  if (!std::is_same<T, double>::value && !std::is_same<T, double2>::value) return 0;
+  const int d = h ? h->fp64_digits : -1;
+  if (d == 0) return 0;
+  const int digits = d < 0 ? kOzAutoDigits : d;
+  const int min_dim = d < 0 ? kOzAutoMinDim : kOzForcedMinDim;
+  if (n < min_dim || !oz_gemm_supported(n, elem<T>::complex, digits)) return 0;
+  return digits;
+}
+template <typename T> inline int oz_min_dim_for(calamanHandle_t h) {
+  return (h && h->fp64_digits > 0) ? kOzForcedMinDim : kOzAutoMinDim;
+}
+template <typename T> inline std::size_t oz_scratch_bytes(calamanHandle_t h, int n) {
+  const int d = oz_digits_for<T>(h, n);
+  return d ? oz_gemm_workspace_bytes(n, n, n, elem<T>::complex, d) : 0;
+}
+
+// The GEMM scratch a driver lends for one call: split-BF16 operand parts
+// (FP32 tiers) and the emulated FP64 products' digit planes.
+template <typename T>
+inline GemmScratch lend_scratch(calamanHandle_t h, int n, void *tc, std::size_t tc_bytes, void *oz,
+                         std::size_t oz_bytes) {
+  GemmScratch gs;
+  gs.ptr = tc;
+  gs.bytes = tc_bytes;
+  gs.terms = split_terms_of(h);
+  gs.oz = oz;
+  gs.oz_bytes = oz_bytes;
+  gs.oz_digits = oz ? oz_digits_for<T>(h, n) : 0;
+  gs.oz_min_dim = oz_min_dim_for<T>(h);
+  return gs;
 }
 
 // The FP64 twin of a single-precision element type: the single tiers run

@@ -510,10 +510,28 @@ inline double real_flops(int M, int N, int K) { return 2.0 * M * (double)N * K; 
 
 }  // namespace
 
+// The emulated path, when the driver lent digit-plane scratch and the product
+// is large enough (GemmScratch::oz_min_dim in every dimension).
+template <typename T>
+bool use_oz(int M, int N, int K) {
+  const GemmScratch *g = tl_gemm_scratch;
+  return g && g->oz && g->oz_digits > 0 && M >= g->oz_min_dim && N >= g->oz_min_dim &&
+         K >= g->oz_min_dim && oz_gemm_supported(K, elem<T>::complex, g->oz_digits) &&
+         oz_gemm_workspace_bytes(M, N, K, elem<T>::complex, g->oz_digits) <= g->oz_bytes;
+}
+
 template <>
 cudaError_t gemm_nn<double>(cudaStream_t s, int M, int N, int K, double alpha, const double *A,
                             int lda, const double *B, int ldb, double beta, double *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  if (use_oz<double>(M, N, K)) {
+    const GemmScratch *g = tl_gemm_scratch;
+    return timed_launch(
+        s, real_flops(M, N, K),
+        [&] { return oz_gemm<double>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, g->oz, g->oz_bytes,
+                                     g->oz_digits); },
+        /*count=*/false);  // its kernels count themselves
+  }
   const bool v16 = aligned16(A) && aligned16(B) && (lda % 2 == 0) && (ldb % 2 == 0);
   // 64 x 64 tiles (measured faster than 128 x 128 at 2048^3 and 4096^3: 558
   // vs 658 us, 4.27 vs 4.53 ms); up to two waves of them, 32 x 32 tiles put
@@ -533,6 +551,14 @@ template <>
 cudaError_t gemm_nn<double2>(cudaStream_t s, int M, int N, int K, double alpha, const double2 *A,
                              int lda, const double2 *B, int ldb, double beta, double2 *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  if (use_oz<double2>(M, N, K)) {
+    const GemmScratch *g = tl_gemm_scratch;
+    return timed_launch(
+        s, 4.0 * real_flops(M, N, K),
+        [&] { return oz_gemm<double2>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, g->oz, g->oz_bytes,
+                                      g->oz_digits); },
+        /*count=*/false);
+  }
   const long long tiles64 = (long long)((M + 63) / 64) * ((N + 63) / 64);
   return timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
     // up to two waves of 64 x 64 tiles (n <= 1024 square, skinny products):

@@ -51,7 +51,7 @@ constexpr int OTM = 128;            // UMMA M (TMEM lanes)
 constexpr int OTN = 128;            // UMMA N (TMEM columns per accumulator)
 constexpr int OTK = 128;            // k-block: one 128-byte swizzle atom of int8
 constexpr int OUK = 32;             // UMMA K for 8-bit inputs
-constexpr int OSTAGES = 4;
+constexpr int OSTAGES = 6;
 constexpr int kOzThreads = 320;
 constexpr int kOzEpiWarps = 8;
 constexpr int kOA = OTM * OTK;      // bytes of one A stage

@@ -39,8 +39,10 @@ struct VjpWs {
   void *lu = nullptr;
   void *tc = nullptr;
   std::size_t tc_bytes = 0;
+  void *oz = nullptr;
+  std::size_t oz_bytes = 0;
   Wd *wide = nullptr;
-  std::size_t carve(void *base, int n, int m) {
+  std::size_t carve(void *base, int n, int m, std::size_t ozb) {
     Layout L(base);
     const std::size_t nn = (std::size_t)n * n;
     const int np = pade_num_powers(m);
@@ -58,17 +60,19 @@ struct VjpWs {
     lu = L.take<char>(lu_scratch_bytes(n));
     tc_bytes = tc_scratch_bytes<T>(n);
     if (tc_bytes) tc = L.take<char>(tc_bytes);
+    oz_bytes = ozb;
+    if (oz_bytes) oz = L.take<char>(oz_bytes);
     if (elem<T>::single) wide = L.take<Wd>(4 * nn);
     return L.used;
   }
 };
 
 template <typename T>
-std::size_t vjp_bytes(int n) {
+std::size_t vjp_bytes(calamanHandle_t h, int n) {
   std::size_t worst = 0;
   for (int m : {3, 5, 7, 9, 13}) {
     VjpWs<T> w;
-    worst = std::max(worst, w.carve(nullptr, n, m));
+    worst = std::max(worst, w.carve(nullptr, n, m, oz_scratch_bytes<T>(h, n)));
   }
   return worst;
 }
@@ -95,7 +99,7 @@ calamanStatus_t vjp_api(calamanHandle_t blas, calamanStream_t stream, int n, con
   if (n < 1 || n > kMaxDim || lda < n || ldg < n || ldga < n || (E != nullptr && lde < n) ||
       work == nullptr)
     return blas_status(CALAMAN_STATUS_INVALID_VALUE);
-  if (lwork < vjp_bytes<T>(n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  if (lwork < vjp_bytes<T>(blas, n)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
   if (A == nullptr || G == nullptr || gradA == nullptr || d_info == nullptr)
     return blas_status(CALAMAN_STATUS_INVALID_VALUE);
   PointerModeScope pm(blas);
@@ -104,7 +108,7 @@ calamanStatus_t vjp_api(calamanHandle_t blas, calamanStream_t stream, int n, con
 
   // the plan expm(A) uses: ||A||_1 in FP64 on the device, one readback
   VjpWs<T> probe;
-  probe.carve(work, n, 13);
+  probe.carve(work, n, 13, 0);
   CLM_CUDA(launch_norm1<T>(st, n, A, lda, nullptr, probe.norm));
   double norm = 0.0;
   double *host = (blas && blas->h_pinned) ? blas->h_pinned : &norm;
@@ -118,12 +122,9 @@ calamanStatus_t vjp_api(calamanHandle_t blas, calamanStream_t stream, int n, con
   const double *b = pade_coeffs(m);
 
   VjpWs<T> ws;
-  ws.carve(work, n, m);
-  GemmScratch gs;
-  gs.ptr = ws.tc;
-  gs.bytes = ws.tc_bytes;
-  gs.terms = split_terms_of(blas);
-  GemmScratchScope gss(ws.tc ? &gs : nullptr);
+  ws.carve(work, n, m, oz_scratch_bytes<T>(blas, n));
+  GemmScratch gs = lend_scratch<T>(blas, n, ws.tc, ws.tc_bytes, ws.oz, ws.oz_bytes);
+  GemmScratchScope gss((ws.tc || ws.oz) ? &gs : nullptr);
   auto mm = [&](const T *X, const T *Y, double beta, T *Z) {
     return gemm_nn<T>(st, n, n, n, 1.0, X, n, Y, n, beta, Z, n);
   };
@@ -230,9 +231,9 @@ using namespace clm;
 extern "C" {
 
 #define CLM_VJP_API(SUF, T, PT, CPT)                                                               \
-  calamanStatus_t calaman_expm_vjp_bufferSize_##SUF(calamanSolverHandle_t, int n, size_t *bytes) { \
+  calamanStatus_t calaman_expm_vjp_bufferSize_##SUF(calamanSolverHandle_t h, int n, size_t *bytes) { \
     if (n < 1 || n > kMaxDim || bytes == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE); \
-    *bytes = vjp_bytes<T>(n);                                                                      \
+    *bytes = vjp_bytes<T>(h, n);                                                                   \
     return ok_status();                                                                            \
   }                                                                                                \
   calamanStatus_t calaman_expm_vjp_##SUF(calamanBlasHandle_t blas, calamanSolverHandle_t,          \

@@ -477,6 +477,15 @@ calamanStatus_t calaman_gemm_bf16x_bufferSize(int m, int n, int k, int terms, si
 calamanStatus_t calaman_gemm_bf16x_s(calamanStream_t stream, int m, int n, int k, double alpha,
                                      const float *A, int lda, const float *B, int ldb, double beta,
                                      float *C, int ldc, int terms, void *work, size_t work_bytes);
+/* How the handle's FP64 / complex128 calls (expm, pade, expm_vjp,
+ * expm_balanced and their squarings) run their n x n products: -1 (default)
+ * on the INT8 tensor cores by the Ozaki scheme with 7 digits when n >= 1536,
+ * where that measured faster, and on the FP64 tensor cores otherwise; 0
+ * always on the FP64 tensor cores; 2..8 always emulated with that many digits
+ * (n >= 128). The workspace queries take the same handle: size the workspace
+ * after setting this. Batched calls always use the FP64 tensor cores. */
+calamanStatus_t calamanSetDoubleEmulation(calamanHandle_t handle, int digits);
+calamanStatus_t calamanGetDoubleEmulation(calamanHandle_t handle, int *digits);
 /* The split level the handle's _s expm/pade calls use (default 6). */
 calamanStatus_t calamanSetFloatSplit(calamanHandle_t handle, int terms);
 calamanStatus_t calamanGetFloatSplit(calamanHandle_t handle, int *terms);
