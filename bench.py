@@ -622,10 +622,19 @@ def run_ours(args, cfg):
     if rank == 0:
         flops = herm_flops(n, cplx) if herm else expm_flops(n, plan.m, plan.s, cplx)
         achieved = kt.gemm_flops / (kt.gemm_ms * 1e-3) / 1e12 if kt.gemm_ms > 0 else None
+        oz_digits = 7 if (suf in "dz" and n >= 1536) else 0  # the library's default policy
         if suf == "s":
             # split-BF16 x6 tensor-core products: six BF16 products per FP32 product
             peak, peak_src = _bf16_peak()
             executed = 6.0 * achieved if achieved else None
+        elif oz_digits:
+            # Ozaki-scheme products on the INT8 tensor cores: digits (digits + 1) / 2
+            # int8 products per real product (complex: 4 real products' worth)
+            peak = measure_fp64_peak(torch, dev, cplx)
+            peak_src = ("cuBLAS complex128/float64 GEMM 4096^3 measured in this run: the FP64 peak the "
+                        "emulated products are measured against")
+            pairs = oz_digits * (oz_digits + 1) / 2
+            executed = (pairs * (1.0 if cplx else 1.0) * achieved) if achieved else None
         else:
             peak = measure_fp64_peak(torch, dev, cplx)
             peak_src = ("cuBLAS complex128/float64 GEMM 4096^3 measured in this run "
@@ -657,7 +666,11 @@ def run_ours(args, cfg):
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if achieved else None,
                          "executed_tflops": executed,
-                         "frac_executed": executed / peak if executed else None,
+                         "frac_executed": (executed / (2.0 * _bf16_peak()[0]) if oz_digits else executed / peak)
+                         if executed else None,
+                         "products": (f"Ozaki INT8 tensor cores, {oz_digits} digits (frac_executed: int8 "
+                                      "ops against twice the measured BF16 peak)") if oz_digits else
+                                     ("split-BF16 x6 tensor cores" if suf == "s" else "FP64 tensor cores"),
                          "traffic": read_traffic(f"zgemm_{n}" if cplx else f"dgemm_{n}"),
                          "kernel": "dense products (every GEMM launch of instrumented steps run "
                                    "after the timed ones); achieved and frac: algorithmic flops "
@@ -876,6 +889,40 @@ def _time_steps(torch, stream, call, steps):
     return sum(a.elapsed_time(b) for a, b in zip(starts, ends))
 
 
+def _plain_fp64_pass(lib, capi, torch, dev, stream, ns, offs, dIn, dOut):
+    """CUDA-event time (ms) of calaman_expm_d called once per matrix over the
+    whole batch, after a warm-up over its first matrices."""
+    h = ctypes.c_void_p()
+    assert lib.calamanCreate(ctypes.byref(h)).ok
+    assert lib.calamanSetStream(h, ctypes.c_void_p(stream.cuda_stream)).ok
+    nb = ctypes.c_size_t()
+    assert lib.calaman_expm_bufferSize_d(h, max(ns), ctypes.byref(nb)).ok
+    work = torch.empty(nb.value, dtype=torch.uint8, device=dev)
+    info = torch.zeros(2, dtype=torch.int32, device=dev)
+    infop = ctypes.cast(info.data_ptr(), capi.c_int_p)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def one(i):
+        n = ns[i]
+        st = lib.calaman_expm_d(h, h, sp, n, ctypes.c_void_p(dIn.data_ptr() + offs[i] * 8), n,
+                                ctypes.c_void_p(dOut.data_ptr() + offs[i] * 8), n,
+                                ctypes.c_void_p(work.data_ptr()), nb.value, infop, None)
+        if not st.ok:
+            raise RuntimeError(f"expm_d failed: {st!r}")
+
+    for i in range(min(64, len(ns))):
+        one(i)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for i in range(len(ns)):
+        one(i)
+    b.record(stream)
+    torch.cuda.synchronize()
+    lib.calamanDestroy(h)
+    return a.elapsed_time(b)
+
+
 def run_batched(args, cfg):
     """One step = one calaman_expm_batched_<t> call over the whole batch.
     Under torchrun the batch is split across ranks (matrices are
@@ -968,7 +1015,7 @@ def run_batched(args, cfg):
         for sb in subs:
             lib.calamanDestroy(sb["h"])
         # ---- the plain FP64 tier on the same matrices, timed the same way
-        fp64_ms = None
+        fp64_ms = plain_ms = None
         if suf == "s":
             h64in = torch.from_numpy(host_in.numpy().astype(np.float64)).to(dev)
             e64 = torch.empty_like(h64in)
@@ -980,6 +1027,10 @@ def run_batched(args, cfg):
                     step64()
             torch.cuda.synchronize()
             fp64_ms = _time_steps(torch, stream, step64, args.steps)
+            # ---- the plain FP64 GPU expm: calaman_expm_d once per matrix, the
+            # reference's one-matrix-per-call API (each call reads its 1-norm
+            # back, one stream synchronisation per matrix); one pass over the batch
+            plain_ms = _plain_fp64_pass(lib, capi, torch, dev, stream, ns, offs, h64in, e64)
     # ---- instrumented pass (not timed into value): CUDA events around every
     # grouped-GEMM launch give the dense products' own throughput
     assert lib.calamanSetKernelTiming(h, 1).ok
@@ -1030,6 +1081,12 @@ def run_batched(args, cfg):
                          "tflops": flops64 * v64 / count / 1e12,
                          "entry": "calaman_expm_batched_d (every product on the FP64 tensor cores, "
                                   "FP64 LU), the same matrices widened to float64"}
+            if plain_ms is not None and world == 1:
+                vp_ = count / (plain_ms * 1e-3)
+                fp64_tier["plain_expm"] = {
+                    "value": vp_, "unit": "expm/s", "ms_per_batch": plain_ms,
+                    "entry": "calaman_expm_d once per matrix over the same float64 matrices (one pass): "
+                             "the one-matrix-per-call FP64 expm, as the reference evaluates it"}
             lib.calamanDestroy(h64)
             del w64, h64in, e64
         baseline = None
@@ -1050,6 +1107,8 @@ def run_batched(args, cfg):
         }
         if fp64_tier:
             line["vs_fp64_tier"] = value / fp64_tier["value"]
+            if "plain_expm" in fp64_tier:
+                line["vs_plain_fp64_expm"] = value / fp64_tier["plain_expm"]["value"]
             line["fp64_tier"] = fp64_tier
         line.update({
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",

@@ -17,6 +17,14 @@
 // the depth, [Cr; Ci] = [[Ar, -Ai]; [Ai, Ar]] [Br; Bi], rows r and M + r
 // sharing one exponent and the two halves of column c of B' one exponent.
 //
+// Square products (M = N = K) split off both diagonals first, X = Dx + Yx,
+// Z = Dz + Yz: the digits cut only the off-diagonal parts (their rows and
+// columns scaled by their own maxima) and the epilogue adds the rest exactly
+// in FP64, X Z = Yx Yz + Dx Z + X Dz - Dx Dz. The expm path's operands are
+// often close to a multiple of I plus a small part (W, the quotient before its
+// squarings, the powers of a skew-Hermitian matrix), whose diagonal would
+// otherwise set every row's scale and cost the off-diagonal entries ~10 bits.
+//
 // Digits are written once per operand by slicing kernels into K-major int8
 // buffers (rows of Kp bytes, zero padded to the tile grid), so the GEMM's
 // producer reads every operand tile with one TMA copy, 128-byte swizzled.
@@ -73,6 +81,11 @@ struct OzParams {
   int *err;
   long long spin;      // bounded-wait tries (kSpinLimit in normal use)
   int skip_loads;      // 1: the producer issues no copy (exercises the abort path)
+  // diagonal split (square products): the caller's A and B as doubles
+  // (complex: interleaved), their leading dimensions in elements
+  int diag;
+  const double *A, *B;
+  int lda, ldb;
 };
 
 // Bounded wait that also gives up once the CTA's abort flag is raised.
@@ -110,7 +123,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   uint64_t *acc_full = empty + OSTAGES;  // [2]
   uint64_t *acc_empty = acc_full + 2;    // [2]
   uint64_t *mma_done = acc_empty + 2;
-  int *col_exp = reinterpret_cast<int *>(mma_done + 1);  // [OTN]
+  double2 *col_dz = reinterpret_cast<double2 *>(mma_done + 2);  // [OTN] Z[c,c] (diagonal split)
+  int *col_exp = reinterpret_cast<int *>(col_dz + OTN);          // [OTN]
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(col_exp + OTN);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
@@ -134,6 +148,12 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   if (threadIdx.x < OTN) {
     const int c = n0 + threadIdx.x;
     col_exp[threadIdx.x] = c < prm.N ? exp_of_bits(prm.bmax[c]) : 0;
+    double2 dz = make_double2(0.0, 0.0);
+    if (prm.diag && c < prm.N) {
+      const std::size_t at = (std::size_t)c * prm.ldb + c;
+      dz = prm.cplx ? make_double2(prm.B[2 * at], prm.B[2 * at + 1]) : make_double2(prm.B[at], 0.0);
+    }
+    col_dz[threadIdx.x] = dz;
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, 2 * OTN);
@@ -240,11 +260,34 @@ __global__ void __launch_bounds__(kOzThreads, 1)
       const int er = exp_of_bits(prm.amax[row]) - 14;
       const bool imag = prm.cplx && row >= prm.M;
       const int r = imag ? row - prm.M : row;
+      double2 dx = make_double2(0.0, 0.0);  // X[r,r]
+      if (prm.diag) {
+        const std::size_t at = (std::size_t)r * prm.lda + r;
+        dx = prm.cplx ? make_double2(prm.A[2 * at], prm.A[2 * at + 1]) : make_double2(prm.A[at], 0.0);
+      }
 #pragma unroll
       for (int j = 0; j < 64; ++j) {
         const int cl = half * 64 + j, c = n0 + cl;
         if (c < prm.N) {
-          const double x = prm.alpha * scalbn(acc[j], er + col_exp[cl]);
+          double v = scalbn(acc[j], er + col_exp[cl]);
+          if (prm.diag) {
+            // + Dx Z + X Dz - Dx Dz (the part of this row's real or imaginary half)
+            const std::size_t az = (std::size_t)c * prm.ldb + r, ax = (std::size_t)c * prm.lda + r;
+            const double2 dz = col_dz[cl];
+            if (prm.cplx) {
+              const double2 z = make_double2(prm.B[2 * az], prm.B[2 * az + 1]);
+              const double2 x = make_double2(prm.A[2 * ax], prm.A[2 * ax + 1]);
+              double2 t = make_double2(dx.x * z.x - dx.y * z.y + x.x * dz.x - x.y * dz.y,
+                                       dx.x * z.y + dx.y * z.x + x.x * dz.y + x.y * dz.x);
+              if (r == c) t = make_double2(t.x - (dx.x * dz.x - dx.y * dz.y), t.y - (dx.x * dz.y + dx.y * dz.x));
+              v += imag ? t.y : t.x;
+            } else {
+              double t = fma(dx.x, prm.B[az], prm.A[ax] * dz.x);
+              if (r == c) t -= dx.x * dz.x;
+              v += t;
+            }
+          }
+          const double x = prm.alpha * v;
           const std::size_t at = prm.cplx ? 2 * ((std::size_t)c * prm.ldc + r) + (imag ? 1 : 0)
                                           : (std::size_t)c * prm.ldc + r;
           prm.C[at] = prm.beta == 0.0 ? x : fma(prm.beta, prm.C[at], x);
@@ -266,13 +309,14 @@ __global__ void __launch_bounds__(kOzThreads, 1)
 // 32 rows x 32 k-lanes, the k-lanes reduced through shared memory.
 template <typename T>
 __global__ void __launch_bounds__(1024) oz_row_max_kernel(int M, int K, const T *__restrict__ A, int lda,
-                                                          unsigned long long *__restrict__ amax) {
+                                                          int diag, unsigned long long *__restrict__ amax) {
   __shared__ double red[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int r = blockIdx.x * 32 + tx;
   double m = 0.0;
   if (r < M)
     for (int k = ty; k < K; k += 32) {
+      if (diag && k == r) continue;
       const T x = A[(std::size_t)k * lda + r];
       if constexpr (elem<T>::complex) m = fmax(m, fmax(fabs((double)x.x), fabs((double)x.y)));
       else m = fmax(m, fabs((double)x));
@@ -291,11 +335,12 @@ __global__ void __launch_bounds__(1024) oz_row_max_kernel(int M, int K, const T 
 // warp per column.
 template <typename T>
 __global__ void __launch_bounds__(256) oz_col_max_kernel(int K, int N, const T *__restrict__ B, int ldb,
-                                                         unsigned long long *__restrict__ bmax) {
+                                                         int diag, unsigned long long *__restrict__ bmax) {
   const int c = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (c >= N) return;
   double m = 0.0;
   for (int k = lane; k < K; k += 32) {
+    if (diag && k == c) continue;
     const T x = B[(std::size_t)c * ldb + k];
     if constexpr (elem<T>::complex) m = fmax(m, fmax(fabs((double)x.x), fabs((double)x.y)));
     else m = fmax(m, fabs((double)x));
@@ -331,12 +376,14 @@ __device__ __forceinline__ void digits16(const double (&x)[16], int e, uint4 (&o
 // Element (r, k) of the real A operand: A itself, or for complex the block
 // [[Ar, -Ai]; [Ai, Ar]] of 2M rows and 2K columns.
 template <typename T>
-__device__ __forceinline__ double a_elem(const T *A, int lda, int M, int K, int r, int k) {
+__device__ __forceinline__ double a_elem(const T *A, int lda, int M, int K, int r, int k, int diag) {
   if constexpr (elem<T>::complex) {
     const bool lo = r < M, left = k < K;
+    if (diag && (lo ? r : r - M) == (left ? k : k - K)) return 0.0;
     const T x = A[(std::size_t)(left ? k : k - K) * lda + (lo ? r : r - M)];
     return lo ? (left ? (double)x.x : -(double)x.y) : (left ? (double)x.y : (double)x.x);
   } else {
+    if (diag && r == k) return 0.0;
     return (double)A[(std::size_t)k * lda + r];
   }
 }
@@ -346,7 +393,7 @@ __device__ __forceinline__ double a_elem(const T *A, int lda, int M, int K, int 
 // each thread then cuts 16 consecutive k of one row.
 template <typename T, int KS>
 __global__ void __launch_bounds__(256) oz_slice_a_kernel(int M, int K, const T *__restrict__ A, int lda,
-                                                         int Mrows, int Kr, int Mrp, int Kp,
+                                                         int Mrows, int Kr, int Mrp, int Kp, int diag,
                                                          const unsigned long long *__restrict__ amax,
                                                          int8_t *__restrict__ digits) {
   __shared__ double tile[64][65];
@@ -355,7 +402,7 @@ __global__ void __launch_bounds__(256) oz_slice_a_kernel(int M, int K, const T *
   for (int idx = t; idx < 64 * 64; idx += 256) {
     const int rr = idx & 63, kk = idx >> 6;
     const int r = r0 + rr, k = k0 + kk;
-    tile[kk][rr] = (r < Mrows && k < Kr) ? a_elem<T>(A, lda, M, K, r, k) : 0.0;
+    tile[kk][rr] = (r < Mrows && k < Kr) ? a_elem<T>(A, lda, M, K, r, k, diag) : 0.0;
   }
   __syncthreads();
   const int rr = t >> 2, kg = (t & 3) * 16;
@@ -376,7 +423,7 @@ __global__ void __launch_bounds__(256) oz_slice_a_kernel(int M, int K, const T *
 // complex, [Br; Bi]); each thread cuts 16 consecutive k of one column.
 template <typename T, int KS>
 __global__ void __launch_bounds__(128) oz_slice_b_kernel(int K, int N, const T *__restrict__ B, int ldb,
-                                                         int Kr, int Np, int Kp,
+                                                         int Kr, int Np, int Kp, int diag,
                                                          const unsigned long long *__restrict__ bmax,
                                                          int8_t *__restrict__ digits) {
   const int c = blockIdx.y;
@@ -387,7 +434,7 @@ __global__ void __launch_bounds__(128) oz_slice_b_kernel(int K, int N, const T *
   for (int j = 0; j < 16; ++j) {
     const int k = k0 + j;
     double v = 0.0;
-    if (c < N && k < Kr) {
+    if (c < N && k < Kr && !(diag && (k < K ? k : k - K) == c)) {
       if constexpr (elem<T>::complex) {
         const T z = B[(std::size_t)c * ldb + (k < K ? k : k - K)];
         v = k < K ? (double)z.x : (double)z.y;
@@ -432,25 +479,25 @@ OzLayout oz_layout(int M, int N, int K, bool cplx, int ks) {
 
 template <typename T, int KS>
 cudaError_t slice_operands(cudaStream_t s, int M, int N, int K, const T *A, int lda, const T *B, int ldb,
-                           const OzLayout &L, char *w) {
+                           int diag, const OzLayout &L, char *w) {
   auto *amax = reinterpret_cast<unsigned long long *>(w + L.amax_off);
   auto *bmax = reinterpret_cast<unsigned long long *>(w + L.bmax_off);
   auto *da = reinterpret_cast<int8_t *>(w + L.a_off);
   auto *db = reinterpret_cast<int8_t *>(w + L.b_off);
   cudaError_t e;
-  oz_row_max_kernel<T><<<(M + 31) / 32, 1024, 0, s>>>(M, K, A, lda, amax);
+  oz_row_max_kernel<T><<<(M + 31) / 32, 1024, 0, s>>>(M, K, A, lda, diag, amax);
   if ((e = launched()) != cudaSuccess) return e;
-  oz_col_max_kernel<T><<<(N + 7) / 8, 256, 0, s>>>(K, N, B, ldb, bmax);
+  oz_col_max_kernel<T><<<(N + 7) / 8, 256, 0, s>>>(K, N, B, ldb, diag, bmax);
   if ((e = launched()) != cudaSuccess) return e;
   oz_slice_a_kernel<T, KS><<<dim3(L.Mrp / 64, L.Kp / 64), 256, 0, s>>>(M, K, A, lda, L.Mrows, L.Kr, L.Mrp,
-                                                                       L.Kp, amax, da);
+                                                                       L.Kp, diag, amax, da);
   if ((e = launched()) != cudaSuccess) return e;
   oz_slice_b_kernel<T, KS><<<dim3((L.Kp / 16 + 127) / 128, L.Np), 128, 0, s>>>(K, N, B, ldb, L.Kr, L.Np, L.Kp,
-                                                                               bmax, db);
+                                                                               diag, bmax, db);
   return launched();
 }
 
-constexpr int kOzSmem = OSTAGES * (kOA + kOB) + 1024 + 256 + OTN * 4 + 64;
+constexpr int kOzSmem = OSTAGES * (kOA + kOB) + 1024 + 256 + OTN * (4 + 16) + 64;
 
 }  // namespace
 
@@ -475,15 +522,16 @@ cudaError_t oz_gemm(cudaStream_t s, int M, int N, int K, double alpha, const T *
   const OzLayout L = oz_layout(M, N, K > 0 ? K : 1, cplx, ks);
   if (ws == nullptr || ws_bytes < L.total) return cudaErrorInvalidValue;
   char *w = static_cast<char *>(ws);
+  const int diag = (M == N && N == K) ? 1 : 0;
   cudaError_t e;
   switch (ks) {
-  case 2: e = slice_operands<T, 2>(s, M, N, K, A, lda, B, ldb, L, w); break;
-  case 3: e = slice_operands<T, 3>(s, M, N, K, A, lda, B, ldb, L, w); break;
-  case 4: e = slice_operands<T, 4>(s, M, N, K, A, lda, B, ldb, L, w); break;
-  case 5: e = slice_operands<T, 5>(s, M, N, K, A, lda, B, ldb, L, w); break;
-  case 6: e = slice_operands<T, 6>(s, M, N, K, A, lda, B, ldb, L, w); break;
-  case 7: e = slice_operands<T, 7>(s, M, N, K, A, lda, B, ldb, L, w); break;
-  default: e = slice_operands<T, 8>(s, M, N, K, A, lda, B, ldb, L, w); break;
+  case 2: e = slice_operands<T, 2>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
+  case 3: e = slice_operands<T, 3>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
+  case 4: e = slice_operands<T, 4>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
+  case 5: e = slice_operands<T, 5>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
+  case 6: e = slice_operands<T, 6>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
+  case 7: e = slice_operands<T, 7>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
+  default: e = slice_operands<T, 8>(s, M, N, K, A, lda, B, ldb, diag, L, w); break;
   }
   if (e != cudaSuccess) return e;
 
@@ -513,6 +561,11 @@ cudaError_t oz_gemm(cudaStream_t s, int M, int N, int K, double alpha, const T *
   p.err = reinterpret_cast<int *>(w);
   p.spin = spin > 0 ? spin : kSpinLimit;
   p.skip_loads = skip_loads;
+  p.diag = diag;
+  p.A = reinterpret_cast<const double *>(A);
+  p.B = reinterpret_cast<const double *>(B);
+  p.lda = lda;
+  p.ldb = ldb;
 
   static bool configured = false;
   if (!configured) {

@@ -131,3 +131,19 @@ def test_bounded_waits_run_out_and_the_context_survives(lib):
     a, b = rand((128, 128), 11), rand((128, 128), 12)
     c, _ = run_oz(lib, a, b, np.zeros((128, 128)), 1.0, 0.0, 7)
     assert rel(c, a @ b, a, b) <= bound(7)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_square_products_split_off_the_diagonal(lib, cplx):
+    """I-dominated square operands (the shape of W and of the quotient before
+    its squarings): the diagonals are taken out of the digits and added back
+    exactly, so the small off-diagonal part keeps the full digit precision."""
+    n = 512
+    g1, g2 = rand((n, n), 21, cplx), rand((n, n), 22, cplx)
+    x = 3.0 * np.eye(n) + 1e-3 * g1
+    z = -2.0 * np.eye(n) + 1e-3 * g2
+    c, _ = run_oz(lib, x, z, np.zeros((n, n), dtype=x.dtype), 1.0, 0.0, 7)
+    want = x @ z
+    off = ~np.eye(n, dtype=bool)
+    assert np.linalg.norm((c - want)[off]) / np.linalg.norm(want[off]) <= 1e-13
+    assert np.linalg.norm(c - want) / np.linalg.norm(want) <= 1e-14
