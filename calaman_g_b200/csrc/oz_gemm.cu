@@ -20,7 +20,8 @@
 // Square products (M = N = K) split off both diagonals first, X = Dx + Yx,
 // Z = Dz + Yz: the digits cut only the off-diagonal parts (their rows and
 // columns scaled by their own maxima) and the epilogue adds the rest exactly
-// in FP64, X Z = Yx Yz + Dx Z + X Dz - Dx Dz. The expm path's operands are
+// in FP64 by a pass after the GEMM, X Z = Yx Yz + Dx Z + X Dz - Dx Dz. The
+// expm path's operands are
 // often close to a multiple of I plus a small part (W, the quotient before its
 // squarings, the powers of a skew-Hermitian matrix), whose diagonal would
 // otherwise set every row's scale and cost the off-diagonal entries ~10 bits.
@@ -81,11 +82,6 @@ struct OzParams {
   int *err;
   long long spin;      // bounded-wait tries (kSpinLimit in normal use)
   int skip_loads;      // 1: the producer issues no copy (exercises the abort path)
-  // diagonal split (square products): the caller's A and B as doubles
-  // (complex: interleaved), their leading dimensions in elements
-  int diag;
-  const double *A, *B;
-  int lda, ldb;
 };
 
 // Bounded wait that also gives up once the CTA's abort flag is raised.
@@ -123,8 +119,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   uint64_t *acc_full = empty + OSTAGES;  // [2]
   uint64_t *acc_empty = acc_full + 2;    // [2]
   uint64_t *mma_done = acc_empty + 2;
-  double2 *col_dz = reinterpret_cast<double2 *>(mma_done + 2);  // [OTN] Z[c,c] (diagonal split)
-  int *col_exp = reinterpret_cast<int *>(col_dz + OTN);          // [OTN]
+  int *col_exp = reinterpret_cast<int *>(mma_done + 1);  // [OTN]
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(col_exp + OTN);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
@@ -148,12 +143,6 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   if (threadIdx.x < OTN) {
     const int c = n0 + threadIdx.x;
     col_exp[threadIdx.x] = c < prm.N ? exp_of_bits(prm.bmax[c]) : 0;
-    double2 dz = make_double2(0.0, 0.0);
-    if (prm.diag && c < prm.N) {
-      const std::size_t at = (std::size_t)c * prm.ldb + c;
-      dz = prm.cplx ? make_double2(prm.B[2 * at], prm.B[2 * at + 1]) : make_double2(prm.B[at], 0.0);
-    }
-    col_dz[threadIdx.x] = dz;
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, 2 * OTN);
@@ -230,6 +219,10 @@ __global__ void __launch_bounds__(kOzThreads, 1)
     const int q = warp & 3;                 // TMEM lane quarter this warp may access
     const int half = (warp - 2) >> 2;       // columns [64 half, 64 half + 64) of the tile
     const int row = m0 + q * 32 + lane;
+    const bool live = row < prm.Mrows;
+    const int er = live ? exp_of_bits(prm.amax[row]) - 14 : 0;
+    const bool imag = prm.cplx && row >= prm.M;
+    const int r = imag ? row - prm.M : row;
     double acc[64];
 #pragma unroll
     for (int j = 0; j < 64; ++j) acc[j] = 0.0;
@@ -256,41 +249,28 @@ __global__ void __launch_bounds__(kOzThreads, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[b]);
     }
-    if (ok && row < prm.Mrows) {
-      const int er = exp_of_bits(prm.amax[row]) - 14;
-      const bool imag = prm.cplx && row >= prm.M;
-      const int r = imag ? row - prm.M : row;
-      double2 dx = make_double2(0.0, 0.0);  // X[r,r]
-      if (prm.diag) {
-        const std::size_t at = (std::size_t)r * prm.lda + r;
-        dx = prm.cplx ? make_double2(prm.A[2 * at], prm.A[2 * at + 1]) : make_double2(prm.A[at], 0.0);
-      }
+    if (ok && live) {
+      // element (r, c) of C as a double; complex: its real or imaginary half
+      const std::size_t step = prm.cplx ? 2 * (std::size_t)prm.ldc : (std::size_t)prm.ldc;
+      double *cbase = prm.C + (prm.cplx ? 2 * (std::size_t)r + (imag ? 1 : 0) : (std::size_t)r) +
+                      (std::size_t)(n0 + half * 64) * step;
+      // four columns at a time: their old values are all loaded before the
+      // first of their stores
 #pragma unroll
-      for (int j = 0; j < 64; ++j) {
-        const int cl = half * 64 + j, c = n0 + cl;
-        if (c < prm.N) {
-          double v = scalbn(acc[j], er + col_exp[cl]);
-          if (prm.diag) {
-            // + Dx Z + X Dz - Dx Dz (the part of this row's real or imaginary half)
-            const std::size_t az = (std::size_t)c * prm.ldb + r, ax = (std::size_t)c * prm.lda + r;
-            const double2 dz = col_dz[cl];
-            if (prm.cplx) {
-              const double2 z = make_double2(prm.B[2 * az], prm.B[2 * az + 1]);
-              const double2 x = make_double2(prm.A[2 * ax], prm.A[2 * ax + 1]);
-              double2 t = make_double2(dx.x * z.x - dx.y * z.y + x.x * dz.x - x.y * dz.y,
-                                       dx.x * z.y + dx.y * z.x + x.x * dz.y + x.y * dz.x);
-              if (r == c) t = make_double2(t.x - (dx.x * dz.x - dx.y * dz.y), t.y - (dx.x * dz.y + dx.y * dz.x));
-              v += imag ? t.y : t.x;
-            } else {
-              double t = fma(dx.x, prm.B[az], prm.A[ax] * dz.x);
-              if (r == c) t -= dx.x * dz.x;
-              v += t;
-            }
+      for (int j0 = 0; j0 < 64; j0 += 4) {
+        double old[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int c = n0 + half * 64 + j0 + j;
+          old[j] = (prm.beta != 0.0 && c < prm.N) ? cbase[(j0 + j) * step] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int cl = half * 64 + j0 + j, c = n0 + cl;
+          if (c < prm.N) {
+            const double x = prm.alpha * scalbn(acc[j0 + j], er + col_exp[cl]);
+            cbase[(j0 + j) * step] = prm.beta == 0.0 ? x : fma(prm.beta, old[j], x);
           }
-          const double x = prm.alpha * v;
-          const std::size_t at = prm.cplx ? 2 * ((std::size_t)c * prm.ldc + r) + (imag ? 1 : 0)
-                                          : (std::size_t)c * prm.ldc + r;
-          prm.C[at] = prm.beta == 0.0 ? x : fma(prm.beta, prm.C[at], x);
         }
       }
     }
@@ -316,10 +296,11 @@ __global__ void __launch_bounds__(1024) oz_row_max_kernel(int M, int K, const T 
   double m = 0.0;
   if (r < M)
     for (int k = ty; k < K; k += 32) {
-      if (diag && k == r) continue;
       const T x = A[(std::size_t)k * lda + r];
-      if constexpr (elem<T>::complex) m = fmax(m, fmax(fabs((double)x.x), fabs((double)x.y)));
-      else m = fmax(m, fabs((double)x));
+      double v;
+      if constexpr (elem<T>::complex) v = fmax(fabs((double)x.x), fabs((double)x.y));
+      else v = fabs((double)x);
+      m = fmax(m, (diag && k == r) ? 0.0 : v);
     }
   red[ty][tx] = m;
   __syncthreads();
@@ -340,10 +321,11 @@ __global__ void __launch_bounds__(256) oz_col_max_kernel(int K, int N, const T *
   if (c >= N) return;
   double m = 0.0;
   for (int k = lane; k < K; k += 32) {
-    if (diag && k == c) continue;
     const T x = B[(std::size_t)c * ldb + k];
-    if constexpr (elem<T>::complex) m = fmax(m, fmax(fabs((double)x.x), fabs((double)x.y)));
-    else m = fmax(m, fabs((double)x));
+    double v;
+    if constexpr (elem<T>::complex) v = fmax(fabs((double)x.x), fabs((double)x.y));
+    else v = fabs((double)x);
+    m = fmax(m, (diag && k == c) ? 0.0 : v);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -453,6 +435,22 @@ __global__ void __launch_bounds__(128) oz_slice_b_kernel(int K, int N, const T *
   for (int i = 0; i < KS; ++i) *reinterpret_cast<uint4 *>(dst + i * plane) = d[i];
 }
 
+// After the emulated product of the off-diagonal parts of a square product:
+// C += alpha (Dx Z + X Dz - Dx Dz), Dx = diag(X), Dz = diag(Z). Coalesced
+// along rows, one element per thread.
+template <typename T>
+__global__ void __launch_bounds__(256) oz_diag_terms_kernel(int n, double alpha, const T *__restrict__ X, int ldx,
+                                                            const T *__restrict__ Z, int ldz, T *__restrict__ C,
+                                                            int ldc) {
+  const int r = blockIdx.x * 256 + threadIdx.x, c = blockIdx.y;
+  if (r >= n) return;
+  const T dx = X[(std::size_t)r * ldx + r], dz = Z[(std::size_t)c * ldz + c];
+  T t = add(mul(dx, Z[(std::size_t)c * ldz + r]), mul(X[(std::size_t)c * ldx + r], dz));
+  if (r == c) t = sub(t, mul(dx, dz));
+  T &out = C[(std::size_t)c * ldc + r];
+  out = add(out, scale(t, alpha));
+}
+
 struct OzLayout {
   int Mrows, Kr, Mrp, Np, Kp;
   std::size_t amax_off, bmax_off, a_off, b_off, total;
@@ -497,7 +495,7 @@ cudaError_t slice_operands(cudaStream_t s, int M, int N, int K, const T *A, int 
   return launched();
 }
 
-constexpr int kOzSmem = OSTAGES * (kOA + kOB) + 1024 + 256 + OTN * (4 + 16) + 64;
+constexpr int kOzSmem = OSTAGES * (kOA + kOB) + 1024 + 256 + OTN * 4 + 64;
 
 }  // namespace
 
@@ -561,11 +559,6 @@ cudaError_t oz_gemm(cudaStream_t s, int M, int N, int K, double alpha, const T *
   p.err = reinterpret_cast<int *>(w);
   p.spin = spin > 0 ? spin : kSpinLimit;
   p.skip_loads = skip_loads;
-  p.diag = diag;
-  p.A = reinterpret_cast<const double *>(A);
-  p.B = reinterpret_cast<const double *>(B);
-  p.lda = lda;
-  p.ldb = ldb;
 
   static bool configured = false;
   if (!configured) {
@@ -575,6 +568,8 @@ cudaError_t oz_gemm(cudaStream_t s, int M, int N, int K, double alpha, const T *
     configured = true;
   }
   oz_gemm_kernel<<<dim3(L.Mrp / OTM, L.Np / OTN), kOzThreads, kOzSmem, s>>>(ma, mb, p);
+  if ((e = launched()) != cudaSuccess || !diag) return e;
+  oz_diag_terms_kernel<T><<<dim3((M + 255) / 256, N), 256, 0, s>>>(M, alpha, A, lda, B, ldb, C, ldc);
   return launched();
 }
 
