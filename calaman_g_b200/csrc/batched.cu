@@ -24,8 +24,11 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "dmma.cuh"
 #include "expm_common.cuh"
+#include "tcgen05.cuh"
 
 namespace clm {
 namespace {
@@ -522,6 +525,268 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// ---- grouped FP32 GEMM on the tcgen05 tensor cores (split-BF16 x6) --------
+// One CTA per 128 x 128 output tile of one matrix (tiles of all matrices
+// numbered consecutively, as above, with 128-tiles), C (+)= +-(A B [+ A2 B2])
+// with the operand policy of the phase. FP32 operands are read straight from
+// the matrices (no part buffers): eight producer warps load a 128 x 64 k-block
+// of A and of B, split every element into bf16 parts h + m + l and write the
+// six part tiles K-major in the 128-byte-swizzled layout tcgen05.mma reads;
+// one thread of the ninth warp issues the six part products (l h, h l, m m,
+// m h, h m, h h; smallest first) into one FP32 accumulator in TMEM, N = the
+// tile's columns rounded up to 16. A two-stage ring overlaps the split of one
+// k-block with the products of the other; the producer warps then read the
+// accumulator back (tcgen05.ld) and apply the phase's epilogue. Waits are
+// bounded; a CTA that gives up records a code in *err and unwinds.
+constexpr int kTcM = 128, kTcN = 128, kTcK = 64;   // tile, k-block of bf16 (one 128-byte row)
+constexpr int kTcStages = 1;                        // one stage: two CTAs share an SM and overlap
+constexpr int kTcProd = 8;                          // producer (and epilogue) warps
+constexpr int kTcThreads = (kTcProd + 1) * 32;
+constexpr int kTcPart = kTcM * kTcK * 2;            // one part of one operand tile: 16 KB
+constexpr int kTcStage = 6 * kTcPart;               // A h m l, B h m l
+constexpr int kTcSmem = kTcStages * kTcStage + 1024 + 256;
+
+// Eight consecutive k of one row of an operand tile, split into three parts
+// and stored at 16-byte chunk `ch` of row `row` (128-byte swizzle).
+__device__ __forceinline__ uint32_t bf2_bits(__nv_bfloat162 v) {
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void split_store8(const float (&x)[8], unsigned char *part0, int row, int ch) {
+  uint32_t w[3][4];
+#pragma unroll
+  for (int j = 0; j < 8; j += 2) {  // two elements per packed conversion
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x[j], x[j + 1]);
+    const float2 hf = __bfloat1622float2(h);
+    const float r0 = x[j] - hf.x, r1 = x[j + 1] - hf.y;
+    const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+    const float2 mf = __bfloat1622float2(m);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+    w[0][j >> 1] = bf2_bits(h);
+    w[1][j >> 1] = bf2_bits(m);
+    w[2][j >> 1] = bf2_bits(l);
+  }
+  const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((ch ^ (row & 7)) << 4);
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+    *reinterpret_cast<uint4 *>(part0 + p * kTcPart + off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+}
+
+template <typename Item, typename Ops>
+__global__ void __launch_bounds__(kTcThreads, 2)
+    g_tc_kernel(const Item *__restrict__ items, const BPlan *__restrict__ plans,
+                const int *__restrict__ tile_prefix, int batch, int phase, int *err) {
+  using namespace tc;
+  const int tile = blockIdx.x;
+  int lo = 0, hi = batch - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_prefix[mid] <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const Item it = items[lo];
+  const BPlan pl = plans[lo];
+  GOps<float> o;
+  if (!Ops::pade(it, pl, phase, blockIdx.y, o)) return;  // uniform over the CTA
+  const int n = it.n;
+  const int tn = (n + kTcM - 1) / kTcM;
+  const int local = tile - tile_prefix[lo];
+  const int m0 = (local % tn) * kTcM, n0 = (local / tn) * kTcN;
+  const int cols = min(kTcN, n - n0);
+  const int Nt = (cols + 15) & ~15;
+  const int nkb = (n + kTcK - 1) / kTcK;
+  const int total = (o.A2 ? 2 : 1) * nkb;
+
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  unsigned char *base = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(tc_smem) + 1023) & ~uintptr_t(1023));
+  uint64_t *full = reinterpret_cast<uint64_t *>(base + kTcStages * kTcStage);
+  uint64_t *empty = full + kTcStages;
+  uint64_t *acc_full = empty + kTcStages;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_full + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(&full[s], kTcProd * 32);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(acc_full, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == kTcProd) {
+    tmem_alloc(tmem_slot, kTcN);
+    fence_before();
+  }
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < kTcProd) {
+    // ---- producers: split k-block after k-block into the ring ----
+    const int t = threadIdx.x;
+    bool ok = true;
+    for (int i = 0; i < total && ok; ++i) {
+      const int s = i % kTcStages;
+      const uint32_t ph = (uint32_t)((i / kTcStages) & 1);
+      for (long long w = 0;; ++w) {
+        if (mbar_try_wait(&empty[s], ph ^ 1u)) break;
+        if (w >= kSpinLimit || ((w & 255) == 255 && *(volatile int *)abort_flag)) {
+          record_error(err, 11);
+          *(volatile int *)abort_flag = 1;
+          ok = false;
+          break;
+        }
+      }
+      if (!ok) break;
+      const bool second = i >= nkb;
+      const float *Am = second ? o.A2 : o.A;
+      const float *Bm = second ? o.B2 : o.B;
+      const int lda = second ? o.lda2 : o.lda, ldb = second ? o.ldb2 : o.ldb;
+      const int k0 = (second ? i - nkb : i) * kTcK;
+      unsigned char *sa = base + s * kTcStage, *sb = sa + 3 * kTcPart;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {  // A: 128 rows x 8 chunks of 8 k; lanes along rows
+        const int id = t + q * (kTcProd * 32);
+        const int row = id & 127, ch = id >> 7;
+        const int gm = m0 + row;
+        float x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int k = k0 + ch * 8 + j;
+          x[j] = (gm < n && k < n) ? Am[(std::size_t)k * lda + gm] : 0.f;
+        }
+        split_store8(x, sa, row, ch);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {  // B: 128 columns x 8 chunks of 8 k; lanes along k
+        const int id = t + q * (kTcProd * 32);
+        const int ch = id & 7, row = id >> 3;
+        const int gc = n0 + row, kc = k0 + ch * 8;
+        float x[8];
+        const float *src = Bm + (std::size_t)gc * ldb + kc;
+        if (gc < n && kc + 8 <= n && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+          const float4 u = *reinterpret_cast<const float4 *>(src);
+          const float4 v = *reinterpret_cast<const float4 *>(src + 4);
+          x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w, x[4] = v.x, x[5] = v.y, x[6] = v.z, x[7] = v.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 8; ++j) x[j] = (gc < n && kc + j < n) ? src[j] : 0.f;
+        }
+        split_store8(x, sb, row, ch);
+      }
+      // the generic-proxy stores become visible to the tensor cores' reads
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&full[s]);
+    }
+    // ---- epilogue ----
+    bool got = false;
+    for (long long w = 0; w < kSpinLimit; ++w) {
+      if (mbar_try_wait(acc_full, 0)) {
+        got = true;
+        break;
+      }
+      if ((w & 255) == 255 && *(volatile int *)abort_flag) break;
+    }
+    if (!got && !*(volatile int *)abort_flag) record_error(err, 13);
+    if (got && !*(volatile int *)abort_flag) {
+      fence_after();
+      const int q = warp & 3, half = warp >> 2;
+      const int row = m0 + q * 32 + lane;
+#pragma unroll
+      for (int c0 = 0; c0 < 64; c0 += 32) {
+        const int cb = n0 + half * 64 + c0;
+        if (cb >= n) break;  // warp-uniform
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * 64 + c0), v);
+        if (row < n) {
+#pragma unroll
+          for (int j0 = 0; j0 < 32; j0 += 8) {  // old values of eight columns before their stores
+            float old[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int c = cb + j0 + j;
+              old[j] = (o.acc && c < n) ? o.C[(std::size_t)c * o.ldc + row] : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int c = cb + j0 + j;
+              if (c < n) {
+                const float a = __uint_as_float(v[j0 + j]);
+                o.C[(std::size_t)c * o.ldc + row] = o.neg ? old[j] - a : old[j] + a;
+              }
+            }
+          }
+        }
+      }
+    }
+  } else if (lane == 0) {
+    // ---- MMA issuer ----
+    const uint32_t idesc = idesc_bf16_f32(kTcM, Nt);
+    // (A part, B part) of the six products: l h, h l, m m, m h, h m, h h
+    const int pa[6] = {2, 0, 1, 1, 0, 0}, pb[6] = {0, 2, 1, 0, 1, 0};
+    bool ok = true;
+    for (int i = 0; i < total; ++i) {
+      const int s = i % kTcStages;
+      const uint32_t ph = (uint32_t)((i / kTcStages) & 1);
+      bool got = false;
+      for (long long w = 0; w < kSpinLimit; ++w) {
+        if (mbar_try_wait(&full[s], ph)) {
+          got = true;
+          break;
+        }
+        if ((w & 255) == 255 && *(volatile int *)abort_flag) break;
+      }
+      if (!got) {
+        record_error(err, 12);
+        *(volatile int *)abort_flag = 1;
+        ok = false;
+        break;
+      }
+      fence_after();
+      const uint32_t sa = saddr(base + s * kTcStage), sb = sa + 3 * kTcPart;
+#pragma unroll
+      for (int tt = 0; tt < 6; ++tt)
+#pragma unroll
+        for (int k = 0; k < kTcK / 16; ++k)  // +32 bytes per 16-element k step inside the row
+          mma_f16(tmem, smem_desc_sw128(sa + pa[tt] * kTcPart + k * 32),
+                  smem_desc_sw128(sb + pb[tt] * kTcPart + k * 32), idesc, (i > 0 || tt > 0 || k > 0) ? 1u : 0u);
+      mma_commit(&empty[s]);
+    }
+    (void)ok;
+    mma_commit(acc_full);  // tracks every MMA above, on the abort path too
+    if (!mbar_wait(acc_full, 0)) record_error(err, 14);
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == kTcProd) {
+    fence_after();
+    tmem_dealloc(tmem, kTcN);
+  }
+}
+
+inline int tiles128_of(int n) {
+  const int t = (n + kTcM - 1) / kTcM;
+  return t * t;
+}
+
+// The FP32 evaluation phases on the tensor cores (128-tile numbering).
+template <typename Item, typename Ops>
+cudaError_t launch_group_tc(cudaStream_t st, dim3 grid, const Item *items, const BPlan *plans,
+                            const int *prefix128, int count, int phase, int *err) {
+  static bool configured = false;
+  auto kern = g_tc_kernel<Item, Ops>;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  kern<<<grid, kTcThreads, kTcSmem, st>>>(items, plans, prefix128, count, phase, err);
+  return launched();
+}
+
 // Launch a grouped product phase on the engine of its element type: DMMA
 // tiles for double, the SIMT kernel otherwise.
 template <typename Item, typename U, typename Ops, bool kSquare>
@@ -999,7 +1264,7 @@ struct BLayout {
   using Hi = typename Wide<T>::type;
   static constexpr bool kSplit = !std::is_same<T, Hi>::value;
   std::size_t items_lo = 0, items_hi = 0, plans_lo = 0, plans_hi = 0, prefix_lo = 0, prefix_hi = 0,
-              norms = 0, conv_in = 0, conv_out = 0, total = 0;
+              prefix128_lo = 0, err = 0, norms = 0, conv_in = 0, conv_out = 0, total = 0;
   std::vector<std::size_t> slab;
   template <typename C> static std::size_t slab_of(int n) {
     using W = typename Wide<C>::type;
@@ -1019,6 +1284,8 @@ struct BLayout {
     plans_hi = L.used;  L.take<BPlan>(kSplit ? batch : 0);
     prefix_lo = L.used; L.take<int>(batch + 1);
     prefix_hi = L.used; L.take<int>(kSplit ? batch + 1 : 0);
+    prefix128_lo = L.used; L.take<int>(batch + 1);
+    err = L.used;       L.take<int>(1);
     norms = L.used;     L.take<double>(batch);
     conv_in = L.used;   L.take<BConv>(kSplit ? batch : 0);
     conv_out = L.used;  L.take<BConv>(kSplit ? batch : 0);
@@ -1102,16 +1369,24 @@ double phase_flops(const std::vector<int> &ns, const std::vector<BPlan> &pls, in
   return f;
 }
 
+// d_prefix128 / tiles128: the 128-tile numbering of the FP32 tensor-core
+// products (FP32 items only; the FP64 items' products stay on DMMA tiles).
 template <typename C>
 cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *d_items,
                        const BPlan *d_plans, const int *d_prefix, int count, int tiles, int max_n,
                        int max_s, int *d_info, const std::vector<int> &ns,
-                       const std::vector<BPlan> &pls) {
+                       const std::vector<BPlan> &pls, const int *d_prefix128 = nullptr, int tiles128 = 0,
+                       int *d_err = nullptr) {
   using W = typename Wide<C>::type;
   cudaError_t e;
   const dim3 ew((unsigned)count, (unsigned)((max_n * max_n + kEwChunk - 1) / kEwChunk));
   auto gemm = [&](int phase, int ysub) -> cudaError_t {
     return timed_group(st, phase_flops(ns, pls, phase, 0), [&] {
+      if constexpr (std::is_same<C, float>::value) {
+        if (d_prefix128)
+          return launch_group_tc<BItem<C, W>, ExpmOps>(st, dim3(tiles128, ysub), d_items, d_plans, d_prefix128,
+                                                       count, phase, d_err);
+      }
       return launch_group<BItem<C, W>, C, ExpmOps, false>(st, dim3(tiles, ysub), d_items, d_plans, d_prefix,
                                                            count, phase, 0);
     });
@@ -1183,6 +1458,8 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
   auto *d_phi = reinterpret_cast<BPlan *>(base + lay.plans_hi);
   auto *d_xlo = reinterpret_cast<int *>(base + lay.prefix_lo);
   auto *d_xhi = reinterpret_cast<int *>(base + lay.prefix_hi);
+  auto *d_x128 = reinterpret_cast<int *>(base + lay.prefix128_lo);
+  auto *d_err = reinterpret_cast<int *>(base + lay.err);
   auto *d_norms = reinterpret_cast<double *>(base + lay.norms);
   auto *d_cin = reinterpret_cast<BConv *>(base + lay.conv_in);
   auto *d_cout = reinterpret_cast<BConv *>(base + lay.conv_out);
@@ -1217,7 +1494,7 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
   std::vector<BItem<T, Hi>> lo_items;
   std::vector<BItem<Hi, Hi>> hi_items;
   std::vector<BPlan> lo_plans, hi_plans;
-  std::vector<int> lo_prefix(1, 0), hi_prefix(1, 0), lo_n, hi_n;
+  std::vector<int> lo_prefix(1, 0), hi_prefix(1, 0), lo_prefix128(1, 0), lo_n, hi_n;
   std::vector<BConv> cin, cout;
   int lo_max_n = 0, hi_max_n = 0, lo_max_s = 0, hi_max_s = 0;
   // matrices in ascending n: the LU runs one launch per size class
@@ -1232,6 +1509,7 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
       lo_items.push_back(lo[i]);
       lo_plans.push_back(bp);
       lo_prefix.push_back(lo_prefix.back() + tiles_of(n));
+      lo_prefix128.push_back(lo_prefix128.back() + tiles128_of(n));
       lo_n.push_back(n);
       lo_max_n = std::max(lo_max_n, n);
       lo_max_s = std::max(lo_max_s, p.s);
@@ -1262,8 +1540,13 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
     CLM_CUDA(cudaMemcpyAsync(d_lo, lo_items.data(), sizeof(BItem<T, Hi>) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_plo, lo_plans.data(), sizeof(BPlan) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_xlo, lo_prefix.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
+    const bool tc = std::is_same<T, float>::value;
+    if (tc) {
+      CLM_CUDA(cudaMemcpyAsync(d_x128, lo_prefix128.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
+      CLM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    }
     CLM_CUDA(run_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info, lo_n,
-                               lo_plans));
+                               lo_plans, tc ? d_x128 : nullptr, lo_prefix128.back(), d_err));
   }
   if (nhi > 0) {
     CLM_CUDA(cudaMemcpyAsync(d_hi, hi_items.data(), sizeof(BItem<Hi, Hi>) * nhi, cudaMemcpyHostToDevice, st));
