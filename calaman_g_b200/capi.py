@@ -138,6 +138,10 @@ for _suf, _real in (("s", c_float), ("d", c_double), ("c", c_float), ("z", c_dou
 SIGNATURES["calaman_getrf_bufferSize"] = (Status, [c_int, c_size_t_p])
 SIGNATURES["calaman_gemm_bf16x_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_size_t_p])
 SIGNATURES["calaman_gemm_bf16x_s"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
+SIGNATURES["calaman_gemm_bf16x_bufferSize_c"] = (Status, [c_int, c_int, c_int, c_int, c_size_t_p])
+SIGNATURES["calaman_gemm_bf16x_c"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
+SIGNATURES["calamanSetWorkspace"] = (Status, [_H, c_void_p, c_size_t])
+SIGNATURES["calaman_poly_tensor_workspace_s"] = (c_size_t, [c_int])
 SIGNATURES["calamanSetDoubleEmulation"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetDoubleEmulation"] = (Status, [_H, c_int_p])
 SIGNATURES["calaman_gemm_ozaki_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_int, c_size_t_p])

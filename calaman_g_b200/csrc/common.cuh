@@ -319,5 +319,7 @@ struct calamanContext {
   double *h_pinned = nullptr;  // pinned host slots for the 1-norm readback
   int split_terms = 6;         // bf16 part products per FP32 product (3 or 6)
   int fp64_digits = -1;        // FP64 products: -1 by size, 0 FP64 tensor cores, else Ozaki digits
+  void *work = nullptr;        // caller-attached device workspace (calamanSetWorkspace)
+  std::size_t work_bytes = 0;
   clm::KernelTimer timer;
 };

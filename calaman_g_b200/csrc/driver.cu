@@ -221,6 +221,22 @@ R norm1_api(calamanStream_t stream, int n, const T *A, int lda, R *d_colsum) {
   return host;
 }
 
+// The horner / paterson_stockmeyer workspaces are sized exactly as the
+// reference's (its tests pin them), so their FP32 products take the tensor
+// cores only when the caller has attached a workspace to the handle
+// (calamanSetWorkspace, as cublasSetWorkspace does): the split-BF16 operand
+// parts live there. Without one they run on the SIMT kernel.
+template <typename T>
+GemmScratch handle_scratch(calamanHandle_t h) {
+  GemmScratch gs;
+  if (std::is_same<T, float>::value && h && h->work) {
+    gs.ptr = h->work;
+    gs.bytes = h->work_bytes;
+    gs.terms = h->split_terms;
+  }
+  return gs;
+}
+
 // ---- horner<T>, src/horner/interface.cppm:104-194 ---------------------------
 template <typename T>
 std::size_t horner_bytes(int n) {
@@ -238,6 +254,8 @@ calamanStatus_t horner_api(calamanHandle_t h, int n, const T *c, int degree, con
   if (h == nullptr) return bad;
   TimerScope ts(timer_of(h));
   cudaStream_t st = h->stream;
+  GemmScratch gs = handle_scratch<T>(h);
+  GemmScratchScope gss(gs.ptr ? &gs : nullptr);
   T *buf[2] = {P, static_cast<T *>(work)};
   const int ld[2] = {ldp, n};
   int cur = (degree % 2 == 0) ? 0 : 1;
@@ -312,6 +330,8 @@ calamanStatus_t ps_api(calamanHandle_t h, int n, const T *c, int degree, const T
   if (h == nullptr) return bad;
   TimerScope ts(timer_of(h));
   cudaStream_t st = h->stream;
+  GemmScratch gs = handle_scratch<T>(h);
+  GemmScratchScope gss(gs.ptr ? &gs : nullptr);
   const std::size_t stride = ps_stride<T>(n);
   Layout L(work);
   T *powers = plan.num_powers > 0 ? L.take<T>((std::size_t)plan.num_powers * stride) : nullptr;
@@ -687,6 +707,43 @@ calamanStatus_t calaman_gemm_ozaki_wait_check(calamanStream_t stream, long long 
   CLM_CUDA(cudaStreamSynchronize(st));
   *code = h;
   return ok_status();
+}
+
+calamanStatus_t calaman_gemm_bf16x_bufferSize_c(int m, int n, int k, int terms, size_t *bytes) {
+  if (m < 1 || n < 1 || k < 1 || (terms != 3 && terms != 6) || bytes == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  *bytes = tc_gemm_workspace_bytes(m, n, k, terms, true);
+  return ok_status();
+}
+
+calamanStatus_t calaman_gemm_bf16x_c(calamanStream_t stream, int m, int n, int k, double alpha, const void *A,
+                                     int lda, const void *B, int ldb, double beta, void *C, int ldc, int terms,
+                                     void *work, size_t work_bytes) {
+  if (m < 1 || n < 1 || k < 1 || lda < m || ldb < k || ldc < m || (terms != 3 && terms != 6) ||
+      A == nullptr || B == nullptr || C == nullptr || work == nullptr)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (work_bytes < tc_gemm_workspace_bytes(m, n, k, terms, true)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  GemmScratch gs;
+  gs.ptr = work;
+  gs.bytes = work_bytes;
+  gs.terms = terms;
+  GemmScratchScope gss(&gs);
+  CLM_CUDA(gemm_nn<float2>(static_cast<cudaStream_t>(stream), m, n, k, alpha, static_cast<const float2 *>(A), lda,
+                           static_cast<const float2 *>(B), ldb, beta, static_cast<float2 *>(C), ldc));
+  return ok_status();
+}
+
+calamanStatus_t calamanSetWorkspace(calamanHandle_t handle, void *d_work, size_t bytes) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if ((d_work == nullptr) != (bytes == 0) || (reinterpret_cast<std::uintptr_t>(d_work) & 255u) != 0)
+    return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  handle->work = d_work;
+  handle->work_bytes = bytes;
+  return ok_status();
+}
+
+size_t calaman_poly_tensor_workspace_s(int n) {
+  return n < 1 ? 0 : tc_gemm_workspace_bytes(n, n, n, 6);
 }
 
 calamanStatus_t calaman_getrf_bufferSize(int n, size_t *bytes) {

@@ -88,10 +88,13 @@ inline calamanExpmPlan_t plan_for(R norm1) {
   return calamanExpmPlan_t{13, s, pade_num_gemms(13) + s};
 }
 
-// FP32 products run as split-BF16 tensor-core GEMMs and need operand-part
-// scratch sized for the largest (n x n x n) product of the evaluation.
+// FP32 and complex64 products run as split-BF16 tensor-core GEMMs and need
+// operand-part scratch sized for the largest (n x n x n) product of the
+// evaluation.
 template <typename T> inline std::size_t tc_scratch_bytes(int n) {
-  return std::is_same<T, float>::value ? tc_gemm_workspace_bytes(n, n, n, 6) : 0;
+  if (std::is_same<T, float>::value) return tc_gemm_workspace_bytes(n, n, n, 6);
+  if (std::is_same<T, float2>::value) return tc_gemm_workspace_bytes(n, n, n, 6, true);
+  return 0;
 }
 
 // FP64 / complex128 products on the INT8 tensor cores (Ozaki scheme): by

@@ -592,6 +592,13 @@ template <>
 cudaError_t gemm_nn<float2>(cudaStream_t s, int M, int N, int K, double alpha, const float2 *A,
                             int lda, const float2 *B, int ldb, double beta, float2 *C, int ldc) {
   if (M <= 0 || N <= 0) return cudaSuccess;
+  GemmScratch *g = tl_gemm_scratch;
+  if (g && K > 0 && g->ptr && tc_gemm_workspace_bytes(M, N, K, g->terms, true) <= g->bytes) {
+    return timed_launch(
+        s, 4.0 * real_flops(M, N, K),
+        [&] { return tc_gemm_c64(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, g->ptr, g->bytes, g->terms); },
+        /*count=*/false);
+  }
   return timed_launch(s, 4.0 * real_flops(M, N, K), [&] {
     dim3 grid((M + 63) / 64, (N + 63) / 64);
     simt_gemm_nn_kernel<float2><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);

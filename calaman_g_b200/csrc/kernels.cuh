@@ -67,11 +67,15 @@ template <typename T>
 cudaError_t gemm_nn_splitk(cudaStream_t s, int M, int N, int K, double alpha, const T *A, int lda, const T *B,
                            int ldb, double beta, T *C, int ldc, T *partial, int max_splits);
 
-// FP32 GEMM on the tcgen05 tensor cores as split-BF16 part products (terms =
-// 3 or 6), accumulated in FP32 TMEM; needs tc_gemm_workspace_bytes of scratch.
-std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms);
+// FP32 / complex64 GEMM on the tcgen05 tensor cores as split-BF16 part
+// products (terms = 3 or 6), accumulated in FP32 TMEM; needs
+// tc_gemm_workspace_bytes of scratch (cplx: for the complex product).
+std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms, bool cplx = false);
 cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const float *A, int lda,
                         const float *B, int ldb, double beta, float *C, int ldc, void *ws,
+                        std::size_t ws_bytes, int terms);
+cudaError_t tc_gemm_c64(cudaStream_t s, int M, int N, int K, double alpha, const float2 *A, int lda,
+                        const float2 *B, int ldb, double beta, float2 *C, int ldc, void *ws,
                         std::size_t ws_bytes, int terms);
 
 // FP64 / complex128 GEMM on the INT8 tensor cores by the Ozaki splitting

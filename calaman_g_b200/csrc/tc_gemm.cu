@@ -9,6 +9,10 @@
 // smallest first, all accumulated into one FP32 accumulator in TMEM:
 //     x3: (m,h) (h,m) (h,h)                          ~16-bit operands
 //     x6: (l,h) (h,l) (m,m) (m,h) (h,m) (h,h)         ~24-bit operands
+// Complex64 products are one real product of twice the rows and twice the
+// depth, [Cr; Ci] = [[Ar, -Ai]; [Ai, Ar]] [Br; Bi]: the split kernels read the
+// interleaved operands in that block form and the epilogue writes rows < M to
+// the real and rows >= M to the imaginary halves of C.
 // The parts are written once per operand by split kernels into a K-major
 // layout (rows of Kpad bf16, zero padded to the tile grid), so the GEMM's
 // producer warp reads every operand tile with one TMA copy, 128-byte swizzled.
@@ -23,6 +27,8 @@
 // and the CTA unwinds (draining its own TMA copies, freeing its TMEM).
 #include <cuda.h>
 #include <cuda_bf16.h>
+
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "tcgen05.cuh"
@@ -43,7 +49,8 @@ constexpr int kA = TM * TK * 2;  // bytes of one A stage
 constexpr int kB = TN * TK * 2;  // bytes of one B stage
 
 struct TcParams {
-  int M, N, nkb;        // nkb: k-blocks per part product (Kpad / TK)
+  int M, N, nkb;        // nkb: k-blocks per part product (Kpad / TK); M: rows of the real product
+  int Mc;               // complex: rows of the caller's C (rows >= Mc are imaginary parts), else 0
   int Mpad, Npad;       // rows of one A part / one B part in the part buffers
   int nterms;
   int pa[9], pb[9];     // part index of A and of B for every term
@@ -61,6 +68,13 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, ui
 }
 __device__ __forceinline__ void umma_commit(uint64_t *bar) { mma_commit(bar); }
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) { return smem_desc_sw128(addr); }
+
+// Element (m, n) of the real product in the caller's C, as a float index.
+__device__ __forceinline__ std::size_t c_index(const TcParams &p, int m, int n) {
+  if (p.Mc == 0) return (std::size_t)n * p.ldc + m;
+  const bool im = m >= p.Mc;
+  return 2 * ((std::size_t)n * p.ldc + (im ? m - p.Mc : m)) + (im ? 1 : 0);
+}
 
 __global__ void __launch_bounds__(kThreads, 1)
     tc_split_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
@@ -172,14 +186,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int n = n0 + c0 + j;
-            old[j] = (prm.beta != 0.f && n < prm.N) ? prm.C[(std::size_t)n * prm.ldc + m] : 0.f;
+            old[j] = (prm.beta != 0.f && n < prm.N) ? prm.C[c_index(prm, m, n)] : 0.f;
           }
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const int n = n0 + c0 + j;
             if (n < prm.N) {
               const float x = prm.alpha * __uint_as_float(v[j]);
-              prm.C[(std::size_t)n * prm.ldc + m] = (prm.beta == 0.f) ? x : fmaf(prm.beta, old[j], x);
+              prm.C[c_index(prm, m, n)] = (prm.beta == 0.f) ? x : fmaf(prm.beta, old[j], x);
             }
           }
         }
@@ -202,16 +216,30 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16 &h, __nv_bfloat16 
   l = __float2bfloat16_rn(r - __bfloat162float(m));
 }
 
-// A (M x K, column-major, lda) -> parts[p][row][k], rows of Kpad, Mpad rows per
-// part; the transpose goes through a 32 x 33 shared tile.
-__global__ void split_a_kernel(int M, int K, const float *__restrict__ A, int lda, int Mpad,
+// Element (m, k) of the real A operand: A itself, or for complex (Mc > 0,
+// Kc = the complex depth) the block [[Ar, -Ai]; [Ai, Ar]].
+template <typename T>
+__device__ __forceinline__ float a_at(const T *A, int lda, int Mc, int Kc, int m, int k) {
+  if constexpr (std::is_same<T, float2>::value) {
+    const bool lo = m < Mc, left = k < Kc;
+    const float2 z = A[(std::size_t)(left ? k : k - Kc) * lda + (lo ? m : m - Mc)];
+    return lo ? (left ? z.x : -z.y) : (left ? z.y : z.x);
+  } else {
+    return A[(std::size_t)k * lda + m];
+  }
+}
+
+// A (M x K real rows; column-major, lda) -> parts[p][row][k], rows of Kpad,
+// Mpad rows per part; the transpose goes through a 32 x 33 shared tile.
+template <typename T>
+__global__ void split_a_kernel(int M, int K, const T *__restrict__ A, int lda, int Mc, int Kc, int Mpad,
                                int Kpad, int nparts, __nv_bfloat16 *__restrict__ parts) {
   __shared__ float tile[32][33];
   const int mb = blockIdx.x * 32, kb = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
   for (int r = ty; r < 32; r += 8) {  // read: consecutive m along tx
     const int m = mb + tx, k = kb + r;
-    tile[r][tx] = (m < M && k < K) ? A[(std::size_t)k * lda + m] : 0.f;
+    tile[r][tx] = (m < M && k < K) ? a_at<T>(A, lda, Mc, Kc, m, k) : 0.f;
   }
   __syncthreads();
   const std::size_t part_stride = (std::size_t)Mpad * Kpad;
@@ -228,14 +256,24 @@ __global__ void split_a_kernel(int M, int K, const float *__restrict__ A, int ld
   }
 }
 
-// B (K x N, column-major, ldb) -> parts[p][col][k]: already K-contiguous.
-__global__ void split_b_kernel(int K, int N, const float *__restrict__ B, int ldb, int Npad,
+// B (K x N real; column-major, ldb; for complex [Br; Bi] with Kc the complex
+// depth) -> parts[p][col][k]: already K-contiguous.
+template <typename T>
+__global__ void split_b_kernel(int K, int N, const T *__restrict__ B, int ldb, int Kc, int Npad,
                                int Kpad, int nparts, __nv_bfloat16 *__restrict__ parts) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= Kpad) return;
   const std::size_t part_stride = (std::size_t)Npad * Kpad;
   for (int n = blockIdx.y; n < Npad; n += gridDim.y) {
-    const float x = (k < K && n < N) ? B[(std::size_t)n * ldb + k] : 0.f;
+    float x = 0.f;
+    if (k < K && n < N) {
+      if constexpr (std::is_same<T, float2>::value) {
+        const float2 z = B[(std::size_t)n * ldb + (k < Kc ? k : k - Kc)];
+        x = k < Kc ? z.x : z.y;
+      } else {
+        x = B[(std::size_t)n * ldb + k];
+      }
+    }
     __nv_bfloat16 h, m, l;
     split3(x, h, m, l);
     const std::size_t at = (std::size_t)n * Kpad + k;
@@ -293,14 +331,17 @@ bool make_rowmajor_map_sw128(CUtensorMap *map, CUtensorMapDataType type, int ele
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms) {
-  return split_layout(M, N, K, terms == 3 ? 2 : 3).total;
+std::size_t tc_gemm_workspace_bytes(int M, int N, int K, int terms, bool cplx) {
+  return split_layout(cplx ? 2 * M : M, N, cplx ? 2 * K : K, terms == 3 ? 2 : 3).total;
 }
 
-cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const float *A, int lda,
-                        const float *B, int ldb, double beta, float *C, int ldc, void *ws,
-                        std::size_t ws_bytes, int terms) {
-  if (M <= 0 || N <= 0) return cudaSuccess;
+namespace {
+template <typename T>
+cudaError_t tc_gemm_run(cudaStream_t s, int Mc, int N, int Kc, double alpha, const T *A, int lda, const T *B,
+                        int ldb, double beta, float *C, int ldc, void *ws, std::size_t ws_bytes, int terms) {
+  constexpr bool cplx = std::is_same<T, float2>::value;
+  if (Mc <= 0 || N <= 0) return cudaSuccess;
+  const int M = cplx ? 2 * Mc : Mc, K = cplx ? 2 * Kc : Kc;  // the real product
   const int nparts = terms == 3 ? 2 : 3;
   const SplitLayout L = split_layout(M, N, K > 0 ? K : 1, nparts);
   if (ws == nullptr || ws_bytes < L.total) return cudaErrorInvalidValue;
@@ -310,11 +351,13 @@ cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const
   auto *pb = reinterpret_cast<__nv_bfloat16 *>(w + 256 + L.a_bytes);
 
   cudaError_t e;
-  split_a_kernel<<<dim3(L.Mpad / 32, L.Kpad / 32), 256, 0, s>>>(M, K, A, lda, L.Mpad, L.Kpad, nparts, pa);
+  split_a_kernel<T><<<dim3(L.Mpad / 32, L.Kpad / 32), 256, 0, s>>>(M, K, A, lda, Mc, Kc, L.Mpad, L.Kpad, nparts,
+                                                                   pa);
   if ((e = launched()) != cudaSuccess) return e;
   {
     const int gy = L.Npad < 65535 ? L.Npad : 65535;
-    split_b_kernel<<<dim3((L.Kpad + 255) / 256, gy), 256, 0, s>>>(K, N, B, ldb, L.Npad, L.Kpad, nparts, pb);
+    split_b_kernel<T><<<dim3((L.Kpad + 255) / 256, gy), 256, 0, s>>>(K, N, B, ldb, Kc, L.Npad, L.Kpad, nparts,
+                                                                     pb);
     if ((e = launched()) != cudaSuccess) return e;
   }
 
@@ -324,6 +367,7 @@ cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const
 
   TcParams p = {};
   p.M = M;
+  p.Mc = cplx ? Mc : 0;
   p.N = N;
   p.nkb = L.Kpad / TK;
   p.Mpad = L.Mpad;
@@ -353,6 +397,20 @@ cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const
   }
   tc_split_gemm_kernel<<<dim3(L.Mpad / TM, L.Npad / TN), kThreads, smem, s>>>(ma, mb, p);
   return launched();
+}
+}  // namespace
+
+cudaError_t tc_gemm_f32(cudaStream_t s, int M, int N, int K, double alpha, const float *A, int lda,
+                        const float *B, int ldb, double beta, float *C, int ldc, void *ws,
+                        std::size_t ws_bytes, int terms) {
+  return tc_gemm_run<float>(s, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, ws, ws_bytes, terms);
+}
+
+cudaError_t tc_gemm_c64(cudaStream_t s, int M, int N, int K, double alpha, const float2 *A, int lda,
+                        const float2 *B, int ldb, double beta, float2 *C, int ldc, void *ws,
+                        std::size_t ws_bytes, int terms) {
+  return tc_gemm_run<float2>(s, M, N, K, alpha, A, lda, B, ldb, beta, reinterpret_cast<float *>(C), ldc, ws,
+                             ws_bytes, terms);
 }
 
 }  // namespace clm

@@ -486,6 +486,23 @@ calamanStatus_t calaman_gemm_bf16x_s(calamanStream_t stream, int m, int n, int k
  * after setting this. Batched calls always use the FP64 tensor cores. */
 calamanStatus_t calamanSetDoubleEmulation(calamanHandle_t handle, int digits);
 calamanStatus_t calamanGetDoubleEmulation(calamanHandle_t handle, int *digits);
+/* Complex64 C = alpha A B + beta C on the tensor cores as split-BF16 part
+ * products: one real product of twice the rows and depth,
+ * [Cr; Ci] = [[Ar, -Ai]; [Ai, Ar]] [Br; Bi]. This is how the _c tier of
+ * expm/pade runs its dense products (the reference's wwr::gemm for complex
+ * float, src/expm/pade.cppm:115-136). */
+calamanStatus_t calaman_gemm_bf16x_bufferSize_c(int m, int n, int k, int terms, size_t *bytes);
+calamanStatus_t calaman_gemm_bf16x_c(calamanStream_t stream, int m, int n, int k, double alpha, const void *A,
+                                     int lda, const void *B, int ldb, double beta, void *C, int ldc, int terms,
+                                     void *work, size_t work_bytes);
+/* A device workspace attached to the handle (cublasSetWorkspace's role;
+ * 256-byte aligned; NULL and 0 detach it). horner_s and paterson_stockmeyer_s,
+ * whose own workspaces are sized as the reference's, run their products on the
+ * tensor cores when the attached workspace holds at least
+ * calaman_poly_tensor_workspace_s(n) bytes, and on the SIMT cores otherwise.
+ * The caller keeps it alive while calls that may use it run. */
+calamanStatus_t calamanSetWorkspace(calamanHandle_t handle, void *d_work, size_t bytes);
+size_t calaman_poly_tensor_workspace_s(int n);
 /* The split level the handle's _s expm/pade calls use (default 6). */
 calamanStatus_t calamanSetFloatSplit(calamanHandle_t handle, int terms);
 calamanStatus_t calamanGetFloatSplit(calamanHandle_t handle, int *terms);

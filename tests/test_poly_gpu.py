@@ -115,3 +115,42 @@ def test_golden_rational_polynomials(run):
             st, got, _ = run.poly(kind, a, c, "d")
             assert st.ok
             assert np.abs(got - want).max() <= 1e-14 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.parametrize("kind", ["ps", "horner"])
+@pytest.mark.parametrize("n,degree,seed", [(64, 9, 40), (200, 7, 41), (256, 12, 42)])
+def test_float_products_on_the_tensor_cores_with_a_handle_workspace(run, kind, n, degree, seed):
+    """horner_s / paterson_stockmeyer_s with a workspace attached to the handle:
+    the products take the split-BF16 tensor-core path (three launches per
+    product: two operand splits and the GEMM) and stay within poly_tol."""
+    import ctypes
+
+    a, c = inputs(n, degree, seed, "s")
+    base = run.lib.calamanGetLaunchCount()
+    st0, got0, _ = run.poly(kind, a, c, "s")
+    simt_launches = run.lib.calamanGetLaunchCount() - base
+    nb = run.lib.calaman_poly_tensor_workspace_s(n)
+    w = run.workspace(nb)
+    assert run.lib.calamanSetWorkspace(run.h, ctypes.c_void_p(w.data_ptr()), nb).ok
+    try:
+        base = run.lib.calamanGetLaunchCount()
+        st1, got1, _ = run.poly(kind, a, c, "s")
+        tc_launches = run.lib.calamanGetLaunchCount() - base
+    finally:
+        assert run.lib.calamanSetWorkspace(run.h, None, 0).ok
+    assert st0.ok and st1.ok
+    ref = poly_reference(a, c)
+    tol = poly_tol(a, c, "s")
+    assert np.abs(got0 - ref).max() <= tol
+    assert np.abs(got1 - ref).max() <= tol
+    assert tc_launches > simt_launches  # the split kernels ran
+
+
+def test_handle_workspace_arguments(run):
+    import ctypes
+
+    w = run.workspace(4096)
+    assert run.lib.calamanSetWorkspace(run.h, None, 16).code == 7
+    assert run.lib.calamanSetWorkspace(run.h, ctypes.c_void_p(w.data_ptr() + 8), 1024).code == 7
+    assert run.lib.calamanSetWorkspace(None, ctypes.c_void_p(w.data_ptr()), 1024).code == 1
+    assert run.lib.calamanSetWorkspace(run.h, None, 0).ok

@@ -79,3 +79,50 @@ def test_x6_is_fp32_accurate(lib):
     got = run_tc(lib, a, b, np.zeros((m, n), np.float32), 1.0, 0.0, 6)
     sgemm = (a @ b).astype(np.float64)
     assert np.linalg.norm(got - ref) <= 4 * np.linalg.norm(sgemm - ref)
+
+
+def run_tc_c(lib, a, b, c0, alpha, beta, terms, lda=None):
+    import torch
+
+    m, k = a.shape
+    n = b.shape[1]
+    lda = lda or m
+    abuf = np.zeros((k, lda), dtype=np.complex64)
+    abuf[:, :m] = a.T
+    dA = torch.from_numpy(abuf.reshape(-1)).cuda()
+    dB = torch.from_numpy(np.asfortranarray(b, dtype=np.complex64).reshape(-1, order="F")).cuda()
+    dC = torch.from_numpy(np.asfortranarray(c0, dtype=np.complex64).reshape(-1, order="F")).cuda()
+    nb = ctypes.c_size_t()
+    assert lib.calaman_gemm_bf16x_bufferSize_c(m, n, k, terms, ctypes.byref(nb)).ok
+    w = torch.zeros(nb.value, dtype=torch.uint8, device="cuda")
+    st = lib.calaman_gemm_bf16x_c(None, m, n, k, alpha, vp(dA), lda, vp(dB), k, beta, vp(dC), m,
+                                  terms, vp(w), nb.value)
+    torch.cuda.synchronize()
+    assert st.ok, st
+    assert int(w[:4].view(torch.int32).item()) == 0
+    return dC.cpu().numpy().reshape(n, m).T
+
+
+@pytest.mark.parametrize("terms", [6, 3])
+@pytest.mark.parametrize("m,n,k", [(128, 128, 64), (100, 70, 33), (300, 260, 129), (512, 512, 512)])
+def test_complex64_split_gemm_matches_fp64(lib, terms, m, n, k):
+    """complex64 as one real product of the block form [[Ar, -Ai]; [Ai, Ar]] [Br; Bi]"""
+    rng = np.random.default_rng(m + 3 * n + 7 * k)
+    a = (rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))).astype(np.complex64)
+    b = (rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))).astype(np.complex64)
+    got = run_tc_c(lib, a, b, np.zeros((m, n), np.complex64), 1.0, 0.0, terms)
+    ref = a.astype(np.complex128) @ b.astype(np.complex128)
+    rel = np.linalg.norm(got - ref) / (np.linalg.norm(a) * np.linalg.norm(b))
+    assert rel <= BOUND[terms], rel
+
+
+def test_complex64_alpha_beta_and_padded_lda(lib):
+    rng = np.random.default_rng(6)
+    m, n, k = 150, 90, 200
+    a = (rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))).astype(np.complex64)
+    b = (rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))).astype(np.complex64)
+    c = (rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))).astype(np.complex64)
+    got = run_tc_c(lib, a, b, c, 0.5, -2.0, 6, lda=m + 5)
+    ref = 0.5 * (a.astype(np.complex128) @ b.astype(np.complex128)) - 2.0 * c.astype(np.complex128)
+    rel = np.linalg.norm(got - ref) / (np.linalg.norm(a) * np.linalg.norm(b) + np.linalg.norm(c))
+    assert rel <= 2e-6, rel
