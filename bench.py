@@ -90,6 +90,13 @@ CONFIGS = {
                                        "N(0,1) rescaled to ||A||_1 log-uniform in [0.1,100]"),
     "expm_batched_f64_8192": dict(kind="batched", count=8192, nmax=256, suf="d",
                                   desc="the same 8192 matrices in float64 (plain FP64 tier)"),
+    "lu_c128_1024": dict(kind="lu", n=1024, suf="z", norm=50.0, gen="gue",
+                         desc="LU with partial pivoting + 1024-RHS solve of the complex128 1024x1024 GUE "
+                              "matrix (the factor and solve expm runs on q), beside cuSOLVER's getrf/getrs "
+                              "(torch.linalg.lu_factor / lu_solve) on the same box"),
+    "lu_f32_4096": dict(kind="lu", n=4096, suf="s", norm=8.0, gen="gauss",
+                        desc="LU with partial pivoting + 4096-RHS solve of the float32 4096x4096 matrix, "
+                             "beside cuSOLVER's getrf/getrs (torch.linalg.lu_factor / lu_solve)"),
     "expm_vjp_f64_2048": dict(kind="vjp", n=2048, suf="d", norm=6.0,
                               desc="loss <G, expm(A)>, float64 2048x2048, A and G N(0,1), "
                                    "A rescaled to ||A||_1=6"),
@@ -694,6 +701,94 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def run_lu(args, cfg):
+    """One step = calaman_getrf + calaman_getrs with n right-hand sides on the
+    workload matrix (the factor and solve of expm's q); the same factor and
+    solve by cuSOLVER (torch.linalg.lu_factor + lu_solve) timed the same way
+    on the same box, as a yardstick. Rank 0 only; L2 flushed before each step."""
+    torch, world, rank, local, dev, dist = _init_dist()
+    from calaman_g_b200 import capi
+
+    lib = capi.load()
+    suf, n = cfg["suf"], cfg["n"]
+    tdt = {"s": torch.float32, "d": torch.float64, "c": torch.complex64, "z": torch.complex128}[suf]
+    a = make_matrix(cfg)
+    rng = np.random.default_rng(7)
+    b = rng.standard_normal((n, n)) + (1j * rng.standard_normal((n, n)) if suf in "cz" else 0)
+    dA0 = torch.from_numpy(np.ascontiguousarray(a.T).reshape(-1)).to(tdt).to(dev)  # column-major
+    dB = torch.from_numpy(np.ascontiguousarray(b.T).reshape(-1)).to(tdt).to(dev)
+    dA = torch.empty_like(dA0)
+    dX = torch.empty_like(dB)
+    nb = ctypes.c_size_t()
+    assert lib.calaman_getrf_bufferSize(n, ctypes.byref(nb)).ok
+    scratch = torch.empty(max(nb.value, 256), dtype=torch.uint8, device=dev)
+    info = torch.zeros(2, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    getrf, getrs = getattr(lib, f"calaman_getrf_{suf}"), getattr(lib, f"calaman_getrs_{suf}")
+    infp = ctypes.cast(info.data_ptr(), capi.c_int_p)
+    infp1 = ctypes.cast(info.data_ptr() + 4, capi.c_int_p)
+
+    def ours():
+        dA.copy_(dA0)
+        assert getrf(sp, n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(scratch.data_ptr()), infp).ok
+        assert getrs(sp, n, n, ctypes.c_void_p(dA.data_ptr()), n, ctypes.c_void_p(scratch.data_ptr()),
+                     ctypes.c_void_p(dB.data_ptr()), n, ctypes.c_void_p(dX.data_ptr()), n, infp1).ok
+
+    Am = dA0.view(n, n).t()  # the matrix (row-major view of the column-major buffer)
+    Bm = dB.view(n, n).t()
+
+    def library():
+        lu, piv = torch.linalg.lu_factor(Am)
+        return torch.linalg.lu_solve(lu, piv, Bm)
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        with torch.cuda.stream(stream):
+            for _ in range(args.steps):
+                flush.zero_()
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                fn()
+                s1.record(stream)
+                s1.synchronize()
+                tot += s0.elapsed_time(s1)
+        return tot
+    with ClockSampler(local) as clocks:
+        ms_ours = timed(ours)
+        ms_lib = timed(library)
+    torch.cuda.synchronize()
+    # the solution against the library's (both solve the same system)
+    x = dX.view(n, n).t()
+    with torch.cuda.stream(stream):
+        xl = library()
+    torch.cuda.synchronize()
+    rel = float((x - xl).abs().norm() / xl.abs().norm())
+    resid = float((Am @ x - Bm).abs().norm() / (Am.abs().norm() * x.abs().norm()))
+    if rank == 0:
+        flops = (8.0 / 3.0 if suf not in "cz" else 4 * 8.0 / 3.0) * n ** 3  # (2/3) n^3 + 2 n^3, x4 complex
+        line = {
+            "metric": "LU + n-RHS solve per second (factor and solve of expm's q)", "value": args.steps / (ms_ours * 1e-3),
+            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_ours / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"z": "c128", "d": "f64", "s": "f32", "c": "c64"}[suf], "data": "synthetic (seeded)",
+            "config": {"workload": args.config, "desc": cfg["desc"], "l2": "flushed before every timed step"},
+            "tflops": flops * args.steps / (ms_ours * 1e-3) / 1e12,
+            "cusolver": {"value": args.steps / (ms_lib * 1e-3), "ms_per_step": ms_lib / args.steps,
+                         "entry": "torch.linalg.lu_factor + torch.linalg.lu_solve (cuSOLVER getrf / getrs), "
+                                  "a yardstick only: nothing in the library calls it"},
+            "vs_cusolver": ms_lib / ms_ours,
+            "accuracy": {"rel_vs_cusolver_solution": rel, "backward_residual": resid},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def _init_dist():
     import torch
 
@@ -1030,7 +1125,8 @@ def run_batched(args, cfg):
             # ---- the plain FP64 GPU expm: calaman_expm_d once per matrix, the
             # reference's one-matrix-per-call API (each call reads its 1-norm
             # back, one stream synchronisation per matrix); one pass over the batch
-            plain_ms = _plain_fp64_pass(lib, capi, torch, dev, stream, ns, offs, h64in, e64)
+            if not args.no_plain:
+                plain_ms = _plain_fp64_pass(lib, capi, torch, dev, stream, ns, offs, h64in, e64)
     # ---- instrumented pass (not timed into value): CUDA events around every
     # grouped-GEMM launch give the dense products' own throughput
     assert lib.calamanSetKernelTiming(h, 1).ok
@@ -1544,6 +1640,8 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    p.add_argument("--no-plain", action="store_true",
+                   help="batched workloads: skip the per-matrix FP64 expm pass (for profiling runs)")
     p.add_argument("--cpu-threads", type=int, default=0,
                    help="host threads of the CPU baseline and the reference arm (numpy's "
                         "BLAS and the C oracle's workers); 0: every host thread")
@@ -1568,6 +1666,8 @@ def main():
         run_vjp(args, cfg)
     elif kind == "geodesic":
         run_geodesic(args, cfg)
+    elif kind == "lu":
+        run_lu(args, cfg)
     else:
         run_ours(args, cfg)
 
