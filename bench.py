@@ -90,6 +90,9 @@ CONFIGS = {
                                        "N(0,1) rescaled to ||A||_1 log-uniform in [0.1,100]"),
     "expm_batched_f64_8192": dict(kind="batched", count=8192, nmax=256, suf="d",
                                   desc="the same 8192 matrices in float64 (plain FP64 tier)"),
+    "expm_batched_f32_2048": dict(kind="batched", count=2048, nmax=256, suf="s",
+                                  desc="the first 2048 matrices of the 8192-matrix batch (a profiling case: "
+                                       "inputs above L2, a few GB on the device)"),
     "lu_c128_1024": dict(kind="lu", n=1024, suf="z", norm=50.0, gen="gue",
                          desc="LU with partial pivoting + 1024-RHS solve of the complex128 1024x1024 GUE "
                               "matrix (the factor and solve expm runs on q), beside cuSOLVER's getrf/getrs "

@@ -62,6 +62,50 @@ __device__ __forceinline__ R warp_max(R v) {
   return v;
 }
 
+// The radix-2 balancing decision of LAPACK xGEBAL for one index, from its
+// off-diagonal column and row 1-norms c, r and the largest magnitudes ca, ra
+// of its column and row (Parlett and Reinsch 1969; LAPACK's DGEBAL, scaling
+// job). Written as two searches for a power of two 2^e:
+//   up:   the most doublings of the column side (halvings of the row side)
+//         while 2^e c stays below 2^-e r / 2 and no scaled quantity reaches
+//         the overflow / underflow guards sfmax2 / sfmin2;
+//   down: from there, the most halvings while 2^-d c' / 2 stays at or above
+//         2^d r', under the same guards.
+// Every scaling is by a power of two, hence exact, so evaluating 2^k x with
+// ldexp gives the values the doubling loops of DGEBAL produce. The factor
+// f = 2^(e - d) is taken when it shrinks c + r below 0.95 of its old value and
+// the accumulated scale d_i f stays inside [sfmin1, sfmax1].
+template <typename R>
+__device__ __forceinline__ bool balance_step(R c, R r, R ca, R ra, R scale_i, const BalLimits<R> &lim,
+                                             R *factor) {
+  *factor = (R)1;
+  if (c == (R)0 || r == (R)0 || !isfinite(c + r + ca + ra)) return false;
+  const R before = c + r;
+  auto p2 = [](R x, int k) { return (R)ldexp(x, k); };
+  int e = 0;
+  for (;;) {  // up
+    const bool stop = p2(c, e) >= p2(r, -e - 1) ||
+                      fmax(fmax(p2((R)1, e), p2(c, e)), p2(ca, e)) >= lim.sfmax2 ||
+                      fmin(fmin(p2(r, -e), p2(r, -e - 1)), p2(ra, -e)) <= lim.sfmin2;
+    if (stop) break;
+    ++e;
+  }
+  const R c1 = p2(c, e), r1 = p2(r, -e), ca1 = p2(ca, e), ra1 = p2(ra, -e);
+  int d = 0;
+  for (;;) {  // down
+    const bool stop = p2(c1, -d - 1) < p2(r1, d) || fmax(p2(r1, d), p2(ra1, d)) >= lim.sfmax2 ||
+                      fmin(fmin(p2((R)1, e - d), p2(c1, -d)), fmin(p2(c1, -d - 1), p2(ca1, -d))) <= lim.sfmin2;
+    if (stop) break;
+    ++d;
+  }
+  const R f = p2((R)1, e - d);
+  if (!(p2(c1, -d) + p2(r1, d) < (R)0.95 * before)) return false;
+  if (f < (R)1 && scale_i < (R)1 && f * scale_i <= lim.sfmin1) return false;
+  if (f > (R)1 && scale_i > (R)1 && scale_i >= lim.sfmax1 / f) return false;
+  *factor = f;
+  return true;
+}
+
 // One Parlett-Reinsch sweep over every index (scaling job: the window is the
 // whole matrix). noconv[0] is set when any index was rescaled.
 template <typename T>
@@ -69,7 +113,6 @@ __global__ void __launch_bounds__(kBalThreads)
     gebal_sweep_kernel(int n, T *__restrict__ A, int lda, typename elem<T>::real *__restrict__ dsc,
                        int *__restrict__ noconv, BalLimits<typename elem<T>::real> lim) {
   using R = typename elem<T>::real;
-  constexpr R kRadix = (R)2, kFactor = (R)0.95;
   constexpr int W = kBalThreads / 32;
   __shared__ R part[4][W];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -108,34 +151,7 @@ __global__ void __launch_bounds__(kBalThreads)
     }
     // the decision, on identical inputs in every thread
     R f = 1;
-    bool accept = false;
-    if (c != (R)0 && r != (R)0 && isfinite(c + r + ca + ra)) {
-      const R s0 = c + r;
-      R g = r / kRadix;
-      while (!(c >= g || fmax(fmax(f, c), ca) >= lim.sfmax2 || fmin(fmin(r, g), ra) <= lim.sfmin2)) {
-        f *= kRadix;
-        c *= kRadix;
-        ca *= kRadix;
-        r /= kRadix;
-        g /= kRadix;
-        ra /= kRadix;
-      }
-      g = c / kRadix;
-      while (!(g < r || fmax(r, ra) >= lim.sfmax2 || fmin(fmin(fmin(f, c), g), ca) <= lim.sfmin2)) {
-        f /= kRadix;
-        c /= kRadix;
-        g /= kRadix;
-        ca /= kRadix;
-        r *= kRadix;
-        ra *= kRadix;
-      }
-      if (c + r < kFactor * s0) {
-        accept = true;
-        const R sc = dsc[i];
-        if (f < (R)1 && sc < (R)1 && f * sc <= lim.sfmin1) accept = false;
-        if (f > (R)1 && sc > (R)1 && sc >= lim.sfmax1 / f) accept = false;
-      }
-    }
+    const bool accept = balance_step(c, r, ca, ra, dsc[i], lim, &f);
     __syncthreads();  // every read of this index is done
     if (accept) {     // row i by 1/f, then column i by f (A(i,i) is touched by both)
       const R inv = (R)1 / f;
