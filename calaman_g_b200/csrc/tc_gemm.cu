@@ -17,12 +17,14 @@
 // layout (rows of Kpad bf16, zero padded to the tile grid), so the GEMM's
 // producer warp reads every operand tile with one TMA copy, 128-byte swizzled.
 //
-// Kernel structure (one CTA per 128 x 256 output tile, 6 warps):
-//   warp 0      TMA producer: a 4-stage ring of (A 128x64, B 256x64) bf16 tiles
+// Kernel structure (one CTA per 128 x 256 output tile, 10 warps):
+//   warp 0      TMA producer: a 4-stage (or, for products of few k-blocks,
+//               2-stage, two CTAs per SM) ring of (A 128x64, B 256x64) tiles
 //   warp 1      TMEM allocator and MMA issuer (one elected thread issues
 //               tcgen05.mma 128x256x16, commits each stage back to the ring)
-//   warps 2..5  epilogue: tcgen05.ld 32 lanes x 32 columns at a time,
-//               alpha/beta, coalesced column-major stores
+//   warps 2..9  epilogue, two warps per TMEM lane quarter: tcgen05.ld 32 lanes
+//               x 32 columns at a time, alpha/beta, coalesced column-major
+//               stores
 // Every mbarrier wait is bounded; a wait that runs out records an error code
 // and the CTA unwinds (draining its own TMA copies, freeing its TMEM).
 #include <cuda.h>
@@ -43,8 +45,7 @@ constexpr int TM = 128;       // UMMA M (TMEM lanes)
 constexpr int TN = 256;       // UMMA N (TMEM columns)
 constexpr int TK = 64;        // k-block: one 128-byte swizzle atom of bf16
 constexpr int UK = 16;        // UMMA K for 16-bit inputs
-constexpr int STAGES = 4;
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;   // producer, MMA issuer, 8 epilogue warps
 constexpr int kA = TM * TK * 2;  // bytes of one A stage
 constexpr int kB = TN * TK * 2;  // bytes of one B stage
 
@@ -76,7 +77,11 @@ __device__ __forceinline__ std::size_t c_index(const TcParams &p, int m, int n) 
   return 2 * ((std::size_t)n * p.ldc + (im ? m - p.Mc : m)) + (im ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
+// STAGES: depth of the TMA ring; MINB: CTAs per SM the kernel is built for
+// (the two-stage variant fits two CTAs on an SM, for products with few
+// k-blocks, where the epilogue's traffic dominates).
+template <int STAGES, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     tc_split_gemm_kernel(const __grid_constant__ CUtensorMap map_a,
                          const __grid_constant__ CUtensorMap map_b, const TcParams prm) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -161,8 +166,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     umma_commit(acc_full);
     if (!mbar_wait(acc_full, 0)) record_error(prm.err, 4);
   } else if (warp >= 2) {
-    // ---- epilogue ----
+    // ---- epilogue: two warps per TMEM lane quarter, 128 columns each ----
     const int q = warp & 3;  // TMEM lane quarter this warp may access
+    const int half = (warp - 2) >> 2;
     // bounded wait for the accumulator; gives up early once the CTA aborted
     bool ok = false;
     for (long long i = 0; i < kSpinLimit; ++i) {
@@ -176,7 +182,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (ok && !*(volatile int *)abort_flag) {
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int m = m0 + q * 32 + lane;
-      for (int c0 = 0; c0 < TN; c0 += 32) {
+      for (int c0 = half * (TN / 2); c0 < (half + 1) * (TN / 2); c0 += 32) {
         if (n0 + c0 >= prm.N) break;
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
@@ -387,15 +393,17 @@ cudaError_t tc_gemm_run(cudaStream_t s, int Mc, int N, int Kc, double alpha, con
   p.ldc = ldc;
   p.err = err;
 
-  const int smem = STAGES * (kA + kB) + 1024 + 256;
-  static bool configured = false;
-  if (!configured) {
-    if ((e = cudaFuncSetAttribute(tc_split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  smem)) != cudaSuccess)
+  // few k-blocks (the LU's K = 32 / 64 updates): two stages, two CTAs per SM
+  const bool shallow = p.nterms * p.nkb <= 12;
+  auto kern = shallow ? tc_split_gemm_kernel<2, 2> : tc_split_gemm_kernel<4, 1>;
+  const int smem = (shallow ? 2 : 4) * (kA + kB) + 1024 + 256;
+  static bool configured[2] = {false, false};
+  if (!configured[shallow]) {
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
       return e;
-    configured = true;
+    configured[shallow] = true;
   }
-  tc_split_gemm_kernel<<<dim3(L.Mpad / TM, L.Npad / TN), kThreads, smem, s>>>(ma, mb, p);
+  kern<<<dim3(L.Mpad / TM, L.Npad / TN), kThreads, smem, s>>>(ma, mb, p);
   return launched();
 }
 }  // namespace
