@@ -647,18 +647,27 @@ __global__ void __launch_bounds__(kTcThreads, 2)
       const int lda = second ? o.lda2 : o.lda, ldb = second ? o.ldb2 : o.ldb;
       const int k0 = (second ? i - nkb : i) * kTcK;
       unsigned char *sa = base + s * kTcStage, *sb = sa + 3 * kTcPart;
+      {  // A: four consecutive rows x one chunk of 8 k per thread; lanes along rows
+        const int rq = t & 31, ch = t >> 5;
+        const int gm = m0 + 4 * rq, kc = k0 + ch * 8;
+        float x[4][8];
+        const bool vec = gm + 3 < n && kc + 8 <= n && (lda & 3) == 0 &&
+                         (reinterpret_cast<uintptr_t>(Am + gm) & 15) == 0;
+        if (vec) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {  // A: 128 rows x 8 chunks of 8 k; lanes along rows
-        const int id = t + q * (kTcProd * 32);
-        const int row = id & 127, ch = id >> 7;
-        const int gm = m0 + row;
-        float x[8];
+          for (int j = 0; j < 8; ++j) {
+            const float4 u = *reinterpret_cast<const float4 *>(Am + (std::size_t)(kc + j) * lda + gm);
+            x[0][j] = u.x, x[1][j] = u.y, x[2][j] = u.z, x[3][j] = u.w;
+          }
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int k = k0 + ch * 8 + j;
-          x[j] = (gm < n && k < n) ? Am[(std::size_t)k * lda + gm] : 0.f;
+          for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+              x[r][j] = (gm + r < n && kc + j < n) ? Am[(std::size_t)(kc + j) * lda + gm + r] : 0.f;
         }
-        split_store8(x, sa, row, ch);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) split_store8(x[r], sa, 4 * rq + r, ch);
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {  // B: 128 columns x 8 chunks of 8 k; lanes along k
