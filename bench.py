@@ -137,6 +137,23 @@ def batched_spec(cfg, count, seed=20261204):
     return sizes, norms
 
 
+def batched_shard(lib, cfg, world, rank):
+    """This rank's matrices of a global batch of world x count (weak
+    scaling): the cost-balanced partition every rank computes alike from the
+    plans the library picks (calaman_expm_plan_*, host-side). Returns
+    (indices, global count)."""
+    from calaman_g_b200.shard import expm_cost, partition
+
+    total = world * cfg["count"]
+    sizes, norms = batched_spec(cfg, total)
+    plan_fn = lib.calaman_expm_plan_s if cfg["suf"] == "s" else lib.calaman_expm_plan_d
+    costs = []
+    for n_, t_ in zip(sizes, norms):
+        p_ = plan_fn(float(t_))
+        costs.append(expm_cost(int(n_), p_.m, p_.s))
+    return partition(costs, world)[rank], total
+
+
 def batched_matrix(n, norm, i, seed=20261204):
     """Matrix i of the batched workload: N(0,1) entries from its own seeded
     stream (so any rank can draw any matrix), rescaled to its 1-norm, float32
@@ -1043,16 +1060,7 @@ def run_batched(args, cfg):
     if world > 1:
         # weak scaling: a global batch of world x count matrices, partitioned
         # across the ranks by algorithmic cost (no data-path collective)
-        from calaman_g_b200.shard import expm_cost, partition
-
-        total = world * cfg["count"]
-        sizes, norms = batched_spec(cfg, total)
-        plan_fn = lib.calaman_expm_plan_s if suf == "s" else lib.calaman_expm_plan_d
-        costs = []
-        for n_, t_ in zip(sizes, norms):
-            p_ = plan_fn(float(t_))
-            costs.append(expm_cost(int(n_), p_.m, p_.s))
-        mine = partition(costs, world)[rank]
+        mine, total = batched_shard(lib, cfg, world, rank)
         mats = batched_workload(cfg, mine, total)
     else:
         mats = batched_workload(cfg)

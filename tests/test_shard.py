@@ -69,3 +69,53 @@ def test_two_rank_gloo_shards_match_single_process():
         p.join(timeout=120)
     assert all(p.exitcode == 0 for p in procs)
     assert out.get(timeout=5) is True
+
+
+def _bench_worker(rank, world, port, out):
+    """What bench.py does for a batched workload under torchrun: each rank
+    takes its share of the global batch from the plans the library picks."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        from calaman_g_b200 import capi
+
+        lib = capi.load()
+        cfg = dict(bench.CONFIGS["expm_batched_f32_8192"], count=48)
+        mine, total = bench.batched_shard(lib, cfg, world, rank)
+        sizes, norms = bench.batched_spec(cfg, total)
+        plans = [lib.calaman_expm_plan_s(float(norms[i])) for i in mine]
+        mats = bench.batched_workload(cfg, mine, total)
+        local = {"idx": mine, "n": [m.shape[0] for m in mats],
+                 "plans": [(p.m, p.s) for p in plans],
+                 "cost": sum(expm_cost(int(sizes[i]), p.m, p.s) for i, p in zip(mine, plans))}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local)
+        if rank == 0:
+            allidx = sorted(i for g in gathered for i in g["idx"])
+            ok = allidx == list(range(total))                      # the shards cover the batch
+            ok &= sum(len(g["idx"]) for g in gathered) == total    # disjointly
+            ok &= all(g["n"] == [int(sizes[i]) for i in g["idx"]] for g in gathered)
+            from oracle import oracle as O
+            want = {i: O.expm_plan(float(norms[i]), single=True) for i in range(total)}
+            ok &= all((m, s_) == (want[i].m, want[i].s)
+                      for g in gathered for i, (m, s_) in zip(g["idx"], g["plans"]))
+            costs = [g["cost"] for g in gathered]
+            ok &= max(costs) <= 1.2 * min(costs)                   # balanced
+            out.put(bool(ok))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_gloo_bench_shards_are_the_batch():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = 30500 + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_bench_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+    assert all(p.exitcode == 0 for p in procs)
+    assert out.get(timeout=5) is True
