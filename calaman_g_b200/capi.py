@@ -142,6 +142,7 @@ SIGNATURES["calaman_gemm_bf16x_bufferSize_c"] = (Status, [c_int, c_int, c_int, c
 SIGNATURES["calaman_gemm_bf16x_c"] = (Status, _GEMM + [c_int, c_void_p, c_size_t])
 SIGNATURES["calamanSetWorkspace"] = (Status, [_H, c_void_p, c_size_t])
 SIGNATURES["calaman_poly_tensor_workspace_s"] = (c_size_t, [c_int])
+SIGNATURES["calaman_grid_barrier_wait_check"] = (Status, [c_void_p, ctypes.c_uint, c_void_p, c_size_t, c_int_p])
 SIGNATURES["calamanSetDoubleEmulation"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetDoubleEmulation"] = (Status, [_H, c_int_p])
 SIGNATURES["calaman_gemm_ozaki_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_int, c_size_t_p])

@@ -117,7 +117,7 @@ __device__ __forceinline__ void red_add_release(unsigned *p, unsigned v) {
 // The arrival is a release (it publishes every write the CTA made before the
 // block barrier), the polls are acquires (later reads of the CTA see every
 // CTA's published writes).
-__device__ bool grid_sync(unsigned *count, int *err, unsigned &epoch, int *s_ok) {
+__device__ bool grid_sync(unsigned *count, int *err, unsigned &epoch, int *s_ok, unsigned limit = kSpinLimit) {
   __syncthreads();
   if (threadIdx.x == 0) {
     ++epoch;
@@ -126,7 +126,7 @@ __device__ bool grid_sync(unsigned *count, int *err, unsigned &epoch, int *s_ok)
     int ok = 1;
     unsigned spins = 0;
     while (ld_acquire(count) < target) {
-      if (++spins > kSpinLimit || *(volatile int *)err) {
+      if (++spins > limit || *(volatile int *)err) {
         ok = 0;
         break;
       }
@@ -137,6 +137,15 @@ __device__ bool grid_sync(unsigned *count, int *err, unsigned &epoch, int *s_ok)
   }
   __syncthreads();
   return *s_ok != 0;
+}
+
+// Self-test of the barrier's bound: CTA 1 never arrives, so CTA 0's wait runs
+// out after `limit` polls, records the failure in *err and returns.
+__global__ void grid_sync_check_kernel(unsigned *count, int *err, unsigned limit) {
+  __shared__ int s_ok;
+  unsigned epoch = 0;
+  if (blockIdx.x != 0) return;
+  grid_sync(count, err, epoch, &s_ok, limit);
 }
 
 // ---- stage 0: range scaling and the Hermitian working copy -----------------
@@ -1385,6 +1394,23 @@ std::size_t geodesic_bytes(int n, int num_samples) {
 using namespace clm;
 
 extern "C" {
+
+calamanStatus_t calaman_grid_barrier_wait_check(calamanStream_t stream, unsigned limit, void *work,
+                                                size_t work_bytes, int *code) {
+  if (work == nullptr || code == nullptr || limit < 1) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (work_bytes < 256) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned *count = static_cast<unsigned *>(work);
+  int *err = reinterpret_cast<int *>(static_cast<char *>(work) + 128);
+  CLM_CUDA(cudaMemsetAsync(work, 0, 256, st));
+  grid_sync_check_kernel<<<2, 64, 0, st>>>(count, err, limit);
+  CLM_CUDA(launched());
+  int h = 0;
+  CLM_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CLM_CUDA(cudaStreamSynchronize(st));
+  *code = h;
+  return ok_status();
+}
 
 #define CLM_HERM_API(SUF, T, R, PT, CPT)                                                                    \
   calamanStatus_t calaman_expm_herm_bufferSize_##SUF(calamanSolverHandle_t, int uplo, int n, size_t *bytes) { \

@@ -536,6 +536,14 @@ calamanStatus_t calaman_gemm_ozaki_z(calamanStream_t stream, int m, int n, int k
 calamanStatus_t calaman_gemm_ozaki_wait_check(calamanStream_t stream, long long spin, void *work,
                                               size_t work_bytes, int *code);
 
+/* Self-test of the grid barrier of the one-launch tridiagonal reduction
+ * (expm_herm / heevd): a two-CTA launch in which one CTA never arrives, so the
+ * other's wait runs out after `limit` polls; synchronises and returns in *code
+ * the failure flag the barrier set (1: it gave up instead of hanging). `work`:
+ * at least 256 bytes of device memory. No counterpart in the reference. */
+calamanStatus_t calaman_grid_barrier_wait_check(calamanStream_t stream, unsigned limit, void *work,
+                                                size_t work_bytes, int *code);
+
 /* LU with partial pivoting and the n-right-hand-side solve that pade() runs on
  * q_m(A) (the reference calls the solver library's getrf/getrs through
  * WarpWraps, src/expm/pade.cppm:186-188). LAPACK semantics: P A = L U, pivot

@@ -204,3 +204,24 @@ def test_nan_input_completes(run, suf):
     assert np.isnan(w).any() or np.isnan(u).any()
     st, e, _, info = run.expm_herm(a, suf)
     assert st.ok and np.isnan(e).any()
+
+
+def test_grid_barrier_wait_runs_out_and_the_context_survives(run):
+    """The tridiagonal reduction's grid barrier is bounded: with one CTA that
+    never arrives, the waiting CTA gives up after its (short) limit, sets the
+    failure flag and returns; the context then still runs expm_herm."""
+    import ctypes
+
+    w = run.workspace(256)
+    code = ctypes.c_int(-1)
+    st = run.lib.calaman_grid_barrier_wait_check(None, 1 << 12, ctypes.c_void_p(w.data_ptr()), 256,
+                                                 ctypes.byref(code))
+    assert st.ok, st
+    assert code.value == 1
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((64, 64)) + 1j * rng.standard_normal((64, 64))
+    h = (x + x.conj().T) / 2
+    st, e, _, info = run.expm_herm(h, "z")
+    wv, v = np.linalg.eigh(h)
+    want = (v * np.exp(wv)) @ v.conj().T
+    assert st.ok and np.linalg.norm(e - want) <= 1e-12 * np.linalg.norm(want)
