@@ -821,13 +821,15 @@ cudaError_t launch_group(cudaStream_t st, dim3 grid, const Item *items, const BP
 // before the first store, so the L2 latency is paid once per eight elements.
 constexpr int kBU = 8;
 
-// CTAs per SM the LU kernel is compiled for: FP32 rows fit 128 registers
-// (two 256-thread CTAs); FP64 as the solve kind says (Lu::kFp64Ctas): two
+// CTAs per SM the LU kernel is compiled for: FP32 three 256-thread CTAs (80
+// registers, a few spilled; three CTAs' shared memory fits; measured 2 %
+// faster on the mixed tier than two at 128 registers, four no better); FP64
+// as the solve kind says (Lu::kFp64Ctas): two
 // CTAs (128 registers, a few spilled, and both CTAs' shared memory fit)
 // measured faster for the expm solve, one (up to 255 registers) for the
 // adjoint's, which spills more at 128.
 template <typename T, int NT, typename Lu> struct BLuOcc {
-  static constexpr int kMinBlocks = (sizeof(T) == 4 ? 2 : Lu::kFp64Ctas) * (256 / NT);
+  static constexpr int kMinBlocks = (sizeof(T) == 4 ? 3 : Lu::kFp64Ctas) * (256 / NT);
 };
 
 // D(r0 + i, c) -= sum_{j < jb} L(i, j) blk[j][c] for i < mrows, c in [c0, c0 + ncols),
