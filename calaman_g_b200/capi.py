@@ -143,6 +143,12 @@ SIGNATURES["calaman_gemm_bf16x_c"] = (Status, _GEMM + [c_int, c_void_p, c_size_t
 SIGNATURES["calamanSetWorkspace"] = (Status, [_H, c_void_p, c_size_t])
 SIGNATURES["calaman_poly_tensor_workspace_s"] = (c_size_t, [c_int])
 SIGNATURES["calaman_grid_barrier_wait_check"] = (Status, [c_void_p, ctypes.c_uint, c_void_p, c_size_t, c_int_p])
+SIGNATURES["calamanSetBatchedGraphs"] = (Status, [_H, c_int])
+SIGNATURES["calamanGetBatchedGraphs"] = (Status, [_H, c_int_p, c_int_p])
+SIGNATURES["calamanSetBatchedTuning"] = (Status, [_H, c_int_p, c_int])
+SIGNATURES["calamanGetBatchedTuning"] = (Status, [_H, c_int_p, c_int_p])
+SIGNATURES["calamanTuneBatched_bufferSize"] = (c_size_t, [c_int])
+SIGNATURES["calamanTuneBatched"] = (Status, [_H, c_int, c_void_p, c_size_t, c_int_p, c_int_p])
 SIGNATURES["calamanSetDoubleEmulation"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetDoubleEmulation"] = (Status, [_H, c_int_p])
 SIGNATURES["calaman_gemm_ozaki_bufferSize"] = (Status, [c_int, c_int, c_int, c_int, c_int, c_size_t_p])

@@ -1214,32 +1214,48 @@ template <typename T, int NT> constexpr std::size_t lu_smem_bytes() {
   return sizeof(T) * (kBPanel * (blk_ld<NT>() + 64) + kBPanel * (kBPanel + 1));
 }
 
-// The LU kernel over a batch sorted by n (ascending), one launch per size
-// class: 64-thread CTAs for n <= 64, 128 for n <= 128, 256 above, so small
-// matrices pack more CTAs per SM.
+// The LU kernel over a batch sorted by n (ascending), one launch per run of
+// matrices that share a CTA size: by default 64-thread CTAs for n <= 64, 128
+// for n <= 128, 256 above (small matrices pack more CTAs per SM); a schedule
+// (lu_threads[ceil(n / 16)], each >= n) may choose per size bucket.
 template <typename Item, typename T, typename Lu, bool kFactor>
 cudaError_t launch_lu(cudaStream_t st, const Item *items, const BPlan *plans, int *info, int mode,
-                      const std::vector<int> &ns) {
+                      const std::vector<int> &ns, const int *lu_threads = nullptr) {
   const int count = (int)ns.size();
-  const int b64 = (int)(std::upper_bound(ns.begin(), ns.end(), 64) - ns.begin());
-  const int b128 = (int)(std::upper_bound(ns.begin(), ns.end(), 128) - ns.begin());
+  auto threads_of = [&](int n) {
+    const int d = n <= 64 ? 64 : n <= 128 ? 128 : 256;
+    if (lu_threads == nullptr) return d;
+    const int t = lu_threads[(n + 15) / 16];
+    return (t == 64 || t == 128 || t == 256) && t >= n ? t : d;
+  };
   auto one = [&](auto nt_tag, int from, int to) -> cudaError_t {
     constexpr int NT = decltype(nt_tag)::value;
     if (to <= from) return cudaSuccess;
     auto kern = g_lu_kernel<Item, T, Lu, kFactor, NT>;
     constexpr std::size_t smem = lu_smem_bytes<T, NT>();
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    // the largest shared-memory carveout, so the CTAs the registers allow fit
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    if (e != cudaSuccess) return e;
+    static bool configured = false;  // once, before any graph capture of a call
+    if (!configured) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      // the largest shared-memory carveout, so the CTAs the registers allow fit
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+      if (e != cudaSuccess) return e;
+      configured = true;
+    }
     kern<<<to - from, NT, smem, st>>>(items + from, plans + from, info, mode);
     return launched();
   };
-  cudaError_t e;
-  if ((e = one(std::integral_constant<int, 64>{}, 0, b64)) != cudaSuccess) return e;
-  if ((e = one(std::integral_constant<int, 128>{}, b64, b128)) != cudaSuccess) return e;
-  return one(std::integral_constant<int, 256>{}, b128, count);
+  for (int from = 0; from < count;) {
+    const int nt = threads_of(ns[from]);
+    int to = from + 1;
+    while (to < count && threads_of(ns[to]) == nt) ++to;
+    cudaError_t e = nt == 64    ? one(std::integral_constant<int, 64>{}, from, to)
+                    : nt == 128 ? one(std::integral_constant<int, 128>{}, from, to)
+                                : one(std::integral_constant<int, 256>{}, from, to);
+    if (e != cudaSuccess) return e;
+    from = to;
+  }
+  return cudaSuccess;
 }
 
 // ---- precision conversion between the caller's buffers and FP64 copies ----
@@ -1380,23 +1396,34 @@ double phase_flops(const std::vector<int> &ns, const std::vector<BPlan> &pls, in
   return f;
 }
 
-// d_prefix128 / tiles128: the 128-tile numbering of the FP32 tensor-core
-// products (FP32 items only; the FP64 items' products stay on DMMA tiles).
+// FP32 items [tc_first, count) run their products on the tensor cores, with
+// the 128-tile numbering d_prefix128 of that range (tiles128 tiles); items
+// [0, tc_first) on the SIMT kernel with the 64-tile numbering d_prefix. The
+// FP64 items' products stay on DMMA tiles. lu_threads: the LU's schedule.
 template <typename C>
 cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *d_items,
                        const BPlan *d_plans, const int *d_prefix, int count, int tiles, int max_n,
                        int max_s, int *d_info, const std::vector<int> &ns,
                        const std::vector<BPlan> &pls, const int *d_prefix128 = nullptr, int tiles128 = 0,
-                       int *d_err = nullptr) {
+                       int *d_err = nullptr, int tc_first = 0, int tiles_simt = 0,
+                       const int *lu_threads = nullptr) {
   using W = typename Wide<C>::type;
   cudaError_t e;
   const dim3 ew((unsigned)count, (unsigned)((max_n * max_n + kEwChunk - 1) / kEwChunk));
   auto gemm = [&](int phase, int ysub) -> cudaError_t {
     return timed_group(st, phase_flops(ns, pls, phase, 0), [&] {
       if constexpr (std::is_same<C, float>::value) {
-        if (d_prefix128)
-          return launch_group_tc<BItem<C, W>, ExpmOps>(st, dim3(tiles128, ysub), d_items, d_plans, d_prefix128,
-                                                       count, phase, d_err);
+        if (d_prefix128) {
+          cudaError_t e2 = cudaSuccess;
+          if (tc_first > 0 && tiles_simt > 0)
+            e2 = launch_group<BItem<C, W>, C, ExpmOps, false>(st, dim3(tiles_simt, ysub), d_items, d_plans,
+                                                              d_prefix, tc_first, phase, 0);
+          if (e2 == cudaSuccess && tc_first < count && tiles128 > 0)
+            e2 = launch_group_tc<BItem<C, W>, ExpmOps>(st, dim3(tiles128, ysub), d_items + tc_first,
+                                                       d_plans + tc_first, d_prefix128, count - tc_first, phase,
+                                                       d_err);
+          return e2;
+        }
       }
       return launch_group<BItem<C, W>, C, ExpmOps, false>(st, dim3(tiles, ysub), d_items, d_plans, d_prefix,
                                                            count, phase, 0);
@@ -1412,7 +1439,8 @@ cudaError_t run_phases(cudaStream_t st, const BItem<C, typename Wide<C>::type> *
   if ((e = gemm(kPhU, 1)) != cudaSuccess) return e;
   b_split_kernel<C, W><<<ew, 256, 0, st>>>(d_items);
   if ((e = launched()) != cudaSuccess) return e;
-  if ((e = launch_lu<BItem<C, W>, C, ExpmLu, true>(st, d_items, d_plans, d_info, 0, ns)) != cudaSuccess)
+  if ((e = launch_lu<BItem<C, W>, C, ExpmLu, true>(st, d_items, d_plans, d_info, 0, ns, lu_threads)) !=
+      cudaSuccess)
     return e;
   if (max_s > 0) {
     b_widen_kernel<C, W><<<ew, 256, 0, st>>>(d_items, d_plans);
@@ -1547,17 +1575,23 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
     }
   }
   const int nlo = (int)lo_items.size(), nhi = (int)hi_items.size();
+  const BatchedTuning tune = blas ? blas->tune : default_batched_tuning();
+  const bool tc = std::is_same<T, float>::value;
+  // the FP32 items from tc_first on take the tensor cores (items are in ascending n)
+  int tc_first = 0;
+  while (tc && tc_first < nlo && lo_n[tc_first] < tune.fp32_tc_min_n) ++tc_first;
+  std::vector<int> tc_prefix(1, 0);
+  for (int i = tc_first; i < nlo; ++i) tc_prefix.push_back(tc_prefix.back() + tiles128_of(lo_n[i]));
+  // the call's tables (every call; the kernels read them from the workspace)
   if (nlo > 0) {
     CLM_CUDA(cudaMemcpyAsync(d_lo, lo_items.data(), sizeof(BItem<T, Hi>) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_plo, lo_plans.data(), sizeof(BPlan) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_xlo, lo_prefix.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
-    const bool tc = std::is_same<T, float>::value;
     if (tc) {
-      CLM_CUDA(cudaMemcpyAsync(d_x128, lo_prefix128.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
+      CLM_CUDA(cudaMemcpyAsync(d_x128, tc_prefix.data(), sizeof(int) * tc_prefix.size(), cudaMemcpyHostToDevice,
+                               st));
       CLM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     }
-    CLM_CUDA(run_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info, lo_n,
-                               lo_plans, tc ? d_x128 : nullptr, lo_prefix128.back(), d_err));
   }
   if (nhi > 0) {
     CLM_CUDA(cudaMemcpyAsync(d_hi, hi_items.data(), sizeof(BItem<Hi, Hi>) * nhi, cudaMemcpyHostToDevice, st));
@@ -1565,14 +1599,86 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
     CLM_CUDA(cudaMemcpyAsync(d_xhi, hi_prefix.data(), sizeof(int) * (nhi + 1), cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_cin, cin.data(), sizeof(BConv) * nhi, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_cout, cout.data(), sizeof(BConv) * nhi, cudaMemcpyHostToDevice, st));
-    const dim3 ew((unsigned)nhi, (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk));
-    b_conv_kernel<T, Hi><<<ew, 256, 0, st>>>(d_cin);
-    CLM_CUDA(launched());
-    CLM_CUDA(run_phases<Hi>(st, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info, hi_n,
-                                hi_plans));
-    b_conv_kernel<Hi, T><<<ew, 256, 0, st>>>(d_cout);
-    CLM_CUDA(launched());
   }
+  // every kernel of the call
+  auto launch_all = [&]() -> cudaError_t {
+    cudaError_t e;
+    if (nlo > 0 &&
+        (e = run_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info, lo_n,
+                           lo_plans, tc ? d_x128 : nullptr, tc_prefix.back(), d_err, tc_first,
+                           lo_prefix[tc_first], tune.lu_threads)) != cudaSuccess)
+      return e;
+    if (nhi > 0) {
+      const dim3 ew((unsigned)nhi, (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk));
+      b_conv_kernel<T, Hi><<<ew, 256, 0, st>>>(d_cin);
+      if ((e = launched()) != cudaSuccess) return e;
+      if ((e = run_phases<Hi>(st, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info, hi_n,
+                              hi_plans, nullptr, 0, nullptr, 0, 0, tune.lu_threads)) != cudaSuccess)
+        return e;
+      b_conv_kernel<Hi, T><<<ew, 256, 0, st>>>(d_cout);
+      if ((e = launched()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  // Graph replay: the launches depend only on the call's configuration, so a
+  // configuration seen twice in a row is captured once and replayed after.
+  // Kernel timing (CUDA events per launch) runs the launches directly.
+  // (the legacy default streams cannot be captured: those calls run directly)
+  if (blas == nullptr || !blas->graphs || tl_timer != nullptr || st == nullptr || st == cudaStreamLegacy ||
+      st == cudaStreamPerThread) {
+    CLM_CUDA(launch_all());
+    return ok_status();
+  }
+  unsigned long long key = 1469598103934665603ull;
+  auto mix = [&key](unsigned long long v) { key = (key ^ v) * 1099511628211ull; };
+  mix((unsigned long long)batch);
+  mix(sizeof(T));
+  mix(reinterpret_cast<std::uintptr_t>(work));
+  mix((unsigned long long)lwork);
+  mix(reinterpret_cast<std::uintptr_t>(d_info));
+  mix(reinterpret_cast<std::uintptr_t>(st));
+  mix((unsigned long long)tune.fp32_tc_min_n);
+  for (int b = 0; b <= 16; ++b) mix((unsigned long long)tune.lu_threads[b]);
+  for (int i = 0; i < batch; ++i) {
+    mix((unsigned long long)h_n[i] | ((unsigned long long)plans[i].m << 32) |
+        ((unsigned long long)plans[i].s << 48));
+    mix(reinterpret_cast<std::uintptr_t>(h_A[i]));
+    mix(reinterpret_cast<std::uintptr_t>(h_E[i]));
+    mix((unsigned long long)h_lda[i] | ((unsigned long long)h_lde[i] << 32));
+  }
+  BatchedGraph &g = blas->graph[std::is_same<T, double>::value ? 1 : 0];
+  if (g.exec != nullptr && g.key == key) {
+    CLM_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(g.exec), st));
+    note_launch(g.launches);
+    return ok_status();
+  }
+  if (g.seen != key) {  // first sighting: run directly
+    g.seen = key;
+    CLM_CUDA(launch_all());
+    return ok_status();
+  }
+  const unsigned long long before = g_launch_count();
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const cudaError_t el = launch_all();
+    e = cudaStreamEndCapture(st, &graph);
+    if (el != cudaSuccess) e = el;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {  // no graph for this handle: the launches run directly from now on
+    cudaGetLastError();
+    blas->graphs = 0;
+    CLM_CUDA(launch_all());
+    return ok_status();
+  }
+  if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
+  g.exec = exec;
+  g.key = key;
+  g.launches = (unsigned)(g_launch_count() - before);
+  CLM_CUDA(cudaGraphLaunch(exec, st));
   return ok_status();
 }
 
@@ -2082,6 +2188,106 @@ calamanStatus_t vjp_batched_bytes(int batch, const int *h_n, std::size_t *bytes)
   return ok_status();
 }
 
+// Deterministic test matrices for the tuner: count n x n matrices, entries
+// uniform in (-1, 1) from a hash of (matrix, index), scaled to a 1-norm of
+// about 4 (single-precision plan m = 9, s = 0).
+__global__ void tune_fill_kernel(float *A, int count, int n) {
+  const std::size_t total = (std::size_t)count * n * n;
+  for (std::size_t i = blockIdx.x * (std::size_t)blockDim.x + threadIdx.x; i < total;
+       i += (std::size_t)gridDim.x * blockDim.x) {
+    unsigned h = (unsigned)(i * 2654435761u) ^ (unsigned)(i >> 32) ^ 0x9e3779b9u;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    const float u = (float)(h >> 8) * (2.0f / 16777216.0f) - 1.0f;
+    A[i] = u * (8.0f / (float)n);
+  }
+}
+
+// The batched schedule, measured: for every size bucket n = 16, 32, ..., 256
+// a batch of `count` n x n float32 matrices runs through the mixed tier with
+// every admissible per-matrix LU CTA size (64 / 128 / 256 threads, >= n) and
+// both FP32 product engines (tensor cores, SIMT); the fastest configuration of
+// each bucket is kept, and the FP32 engine threshold is the smallest n from
+// which the tensor cores won every larger bucket.
+calamanStatus_t tune_batched(calamanHandle_t h, int count, void *d_work, std::size_t work_bytes, int *lu_out,
+                             int *tc_min_out) {
+  cudaStream_t st = h->stream;
+  const std::size_t mat = align_up((std::size_t)count * kBatchedMaxN * kBatchedMaxN * sizeof(float), 256);
+  char *w = static_cast<char *>(d_work);
+  float *A = reinterpret_cast<float *>(w);
+  float *E = reinterpret_cast<float *>(w + mat);
+  int *info = reinterpret_cast<int *>(w + 2 * mat);
+  char *ws = w + 2 * mat + align_up((std::size_t)2 * count * sizeof(int), 256);
+  const std::size_t ws_bytes = work_bytes - (std::size_t)(ws - w);
+  const BatchedTuning saved = h->tune;
+  const int saved_graphs = h->graphs;
+  h->graphs = 0;
+  BatchedTuning best = default_batched_tuning();
+  bool tc_best[17] = {};
+  cudaEvent_t a = nullptr, b = nullptr;
+  CLM_CUDA(cudaEventCreate(&a));
+  CLM_CUDA(cudaEventCreate(&b));
+  calamanStatus_t status = ok_status();
+  for (int bucket = 1; bucket <= 16 && is_ok(status); ++bucket) {
+    const int n = 16 * bucket;
+    std::vector<int> ns(count, n), lds(count, n);
+    std::vector<const float *> pa(count);
+    std::vector<float *> pe(count);
+    for (int i = 0; i < count; ++i) {
+      pa[i] = A + (std::size_t)i * n * n;
+      pe[i] = E + (std::size_t)i * n * n;
+    }
+    tune_fill_kernel<<<4 * 148, 256, 0, st>>>(A, count, n);
+    if (launched() != cudaSuccess) {
+      status = runtime_status(cudaGetLastError());
+      break;
+    }
+    float best_ms = 1e30f;
+    for (int nt : {64, 128, 256}) {
+      if (nt < n) continue;
+      for (int eng = 0; eng < 2 && is_ok(status); ++eng) {
+        BatchedTuning t = saved;
+        t.lu_threads[bucket] = nt;
+        t.fp32_tc_min_n = eng ? 1 : kBatchedMaxN + 1;
+        h->tune = t;
+        float ms = 0.f;
+        for (int rep = 0; rep < 3 && is_ok(status); ++rep) {  // one warm-up, two timed
+          if (rep == 1) cudaEventRecord(a, st);
+          status = batched_api<float>(h, st, count, ns.data(), pa.data(), lds.data(), pe.data(), lds.data(), ws,
+                                      ws_bytes, info, nullptr);
+        }
+        if (!is_ok(status)) break;
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best.lu_threads[bucket] = nt;
+          tc_best[bucket] = eng == 1;
+        }
+      }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  h->graphs = saved_graphs;
+  if (!is_ok(status)) {
+    h->tune = saved;
+    return status;
+  }
+  int min_n = kBatchedMaxN + 1;
+  for (int bucket = 16; bucket >= 1 && tc_best[bucket]; --bucket) min_n = 16 * bucket - 15;
+  best.fp32_tc_min_n = min_n;
+  h->tune = best;
+  if (lu_out)
+    for (int bb = 0; bb <= 16; ++bb) lu_out[bb] = best.lu_threads[bb];
+  if (tc_min_out) *tc_min_out = best.fp32_tc_min_n;
+  return ok_status();
+}
+
 }  // namespace
 }  // namespace clm
 
@@ -2105,6 +2311,60 @@ calamanStatus_t calaman_expm_batched_s(calamanBlasHandle_t blas, calamanSolverHa
   return batched_api<float>(blas, stream, batch, h_n, h_A, h_lda, h_E, h_lde, d_work, lwork, d_info,
                             h_plans);
 }
+calamanStatus_t calamanSetBatchedGraphs(calamanHandle_t handle, int enable) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  handle->graphs = enable != 0;
+  return ok_status();
+}
+
+calamanStatus_t calamanGetBatchedGraphs(calamanHandle_t handle, int *enabled, int *cached) {
+  if (handle == nullptr || enabled == nullptr || cached == nullptr)
+    return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  *enabled = handle->graphs;
+  *cached = (handle->graph[0].exec != nullptr) + (handle->graph[1].exec != nullptr);
+  return ok_status();
+}
+
+calamanStatus_t calamanSetBatchedTuning(calamanHandle_t handle, const int *lu_threads, int fp32_tc_min_n) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  BatchedTuning t = default_batched_tuning();
+  if (lu_threads != nullptr)
+    for (int b = 1; b <= 16; ++b) {
+      const int v = lu_threads[b];
+      if (!((v == 64 || v == 128 || v == 256) && v >= 16 * b)) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+      t.lu_threads[b] = v;
+    }
+  if (fp32_tc_min_n < 1) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  t.fp32_tc_min_n = fp32_tc_min_n;
+  handle->tune = t;
+  return ok_status();
+}
+
+calamanStatus_t calamanGetBatchedTuning(calamanHandle_t handle, int *lu_threads, int *fp32_tc_min_n) {
+  if (handle == nullptr || lu_threads == nullptr || fp32_tc_min_n == nullptr)
+    return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  for (int b = 0; b <= 16; ++b) lu_threads[b] = handle->tune.lu_threads[b];
+  *fp32_tc_min_n = handle->tune.fp32_tc_min_n;
+  return ok_status();
+}
+
+size_t calamanTuneBatched_bufferSize(int count) {
+  if (count < 1) return 0;
+  std::vector<int> ns(count, kBatchedMaxN);
+  std::size_t wb = 0;
+  batched_bytes<float>(count, ns.data(), &wb);
+  const std::size_t mat = align_up((std::size_t)count * kBatchedMaxN * kBatchedMaxN * sizeof(float), 256);
+  return 2 * mat + align_up((std::size_t)2 * count * sizeof(int), 256) + wb;
+}
+
+calamanStatus_t calamanTuneBatched(calamanHandle_t handle, int count, void *d_work, size_t work_bytes,
+                                   int *lu_threads, int *fp32_tc_min_n) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  if (count < 1 || d_work == nullptr) return blas_status(CALAMAN_STATUS_INVALID_VALUE);
+  if (work_bytes < calamanTuneBatched_bufferSize(count)) return blas_status(CALAMAN_STATUS_ALLOC_FAILED);
+  return tune_batched(handle, count, d_work, work_bytes, lu_threads, fp32_tc_min_n);
+}
+
 calamanStatus_t calaman_expm_batched_d(calamanBlasHandle_t blas, calamanSolverHandle_t,
                                        calamanStream_t stream, int batch, const int *h_n,
                                        const double *const *h_A, const int *h_lda, double *const *h_E,

@@ -193,6 +193,7 @@ int sm_count();
 
 // Every launcher bumps this process-wide counter (calamanGetLaunchCount).
 void note_launch(unsigned n = 1);
+unsigned long long g_launch_count();
 // After a <<<>>> launch: count it and return the launch error.
 inline cudaError_t launched() {
   note_launch(1);
@@ -308,6 +309,31 @@ __device__ __forceinline__ ArgMax cta_argmax(ArgMax a, unsigned long long *red_k
   return warp_argmax(b);
 }
 
+// Per-size schedule of the batched tier (size buckets b = ceil(n / 16), n <= 256):
+// the CTA size of the per-matrix LU (>= n) and the smallest n whose FP32
+// products run on the tensor cores (smaller ones on the SIMT kernel). The
+// defaults are the table calamanTuneBatched measured on a B200;
+// calamanTuneBatched re-measures it on the caller's device.
+struct BatchedTuning {
+  int lu_threads[17];
+  int fp32_tc_min_n;
+};
+inline BatchedTuning default_batched_tuning() {
+  BatchedTuning t{};
+  for (int b = 0; b <= 16; ++b) t.lu_threads[b] = 16 * b <= 64 ? 64 : 16 * b <= 128 ? 128 : 256;
+  t.fp32_tc_min_n = 1;
+  return t;
+}
+
+// A batched call's launches captured as a CUDA graph, replayed while the
+// call's configuration (sizes, plans, pointers, schedule) is unchanged.
+struct BatchedGraph {
+  unsigned long long key = 0;   // configuration of the cached graph
+  unsigned long long seen = 0;  // configuration of the last call (captured when it repeats)
+  void *exec = nullptr;         // cudaGraphExec_t
+  unsigned launches = 0;        // kernels in the graph (counted again at every replay)
+};
+
 }  // namespace clm
 
 // The opaque handle behind calamanHandle_t.
@@ -321,5 +347,8 @@ struct calamanContext {
   int fp64_digits = -1;        // FP64 products: -1 by size, 0 FP64 tensor cores, else Ozaki digits
   void *work = nullptr;        // caller-attached device workspace (calamanSetWorkspace)
   std::size_t work_bytes = 0;
+  clm::BatchedTuning tune = clm::default_batched_tuning();
+  int graphs = 1;              // batched calls replay a captured CUDA graph of their launches
+  clm::BatchedGraph graph[2];  // per batched tier: [0] float, [1] double
   clm::KernelTimer timer;
 };

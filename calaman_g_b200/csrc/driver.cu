@@ -441,6 +441,8 @@ calamanStatus_t calamanCreate(calamanHandle_t *handle) {
 calamanStatus_t calamanDestroy(calamanHandle_t handle) {
   if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
   if (handle->h_pinned) cudaFreeHost(handle->h_pinned);
+  for (auto &g : handle->graph)
+    if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
   delete handle;
   return ok_status();
 }

@@ -536,6 +536,25 @@ calamanStatus_t calaman_gemm_ozaki_z(calamanStream_t stream, int m, int n, int k
 calamanStatus_t calaman_gemm_ozaki_wait_check(calamanStream_t stream, long long spin, void *work,
                                               size_t work_bytes, int *code);
 
+/* The batched tier's schedule and launch mode (no counterpart: the reference
+ * evaluates one matrix per call). A batched call whose configuration (sizes,
+ * plans, pointers, schedule) repeats the previous call's is captured once as a
+ * CUDA graph of its kernels and replayed from then on (on by default; off
+ * while kernel timing is on). The schedule gives, per size bucket
+ * b = ceil(n / 16) (index 1..16 of a 17-int array), the CTA size of the
+ * per-matrix LU (64, 128 or 256 threads, >= 16 b), and the smallest n whose
+ * FP32 products run on the tensor cores. calamanTuneBatched measures it on the
+ * current device with `count` float32 matrices per size (scratch:
+ * calamanTuneBatched_bufferSize(count) bytes), keeps it in the handle and
+ * returns it; the built-in default is the table it measured on a B200. */
+calamanStatus_t calamanSetBatchedGraphs(calamanHandle_t handle, int enable);
+calamanStatus_t calamanGetBatchedGraphs(calamanHandle_t handle, int *enabled, int *cached);
+calamanStatus_t calamanSetBatchedTuning(calamanHandle_t handle, const int *lu_threads, int fp32_tc_min_n);
+calamanStatus_t calamanGetBatchedTuning(calamanHandle_t handle, int *lu_threads, int *fp32_tc_min_n);
+size_t calamanTuneBatched_bufferSize(int count);
+calamanStatus_t calamanTuneBatched(calamanHandle_t handle, int count, void *d_work, size_t work_bytes,
+                                   int *lu_threads, int *fp32_tc_min_n);
+
 /* Self-test of the grid barrier of the one-launch tridiagonal reduction
  * (expm_herm / heevd): a two-CTA launch in which one CTA never arrives, so the
  * other's wait runs out after `limit` polls; synchronises and returns in *code
