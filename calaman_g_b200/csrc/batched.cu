@@ -1938,7 +1938,8 @@ template <typename C>
 cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::type> *d_items,
                            const BPlan *d_plans, const int *d_prefix, int count, int tiles, int max_n,
                            int max_s, int *d_info, const std::vector<int> &ns,
-                           const std::vector<BPlan> &pls) {
+                           const std::vector<BPlan> &pls, const int *d_prefix128 = nullptr, int tiles128 = 0,
+                           int *d_err = nullptr, int tc_first = 0, int tiles_simt = 0) {
   using W = typename Wide<C>::type;
   using Item = BVItem<C, W>;
   cudaError_t e;
@@ -1964,6 +1965,18 @@ cudaError_t run_vjp_phases(cudaStream_t st, const BVItem<C, typename Wide<C>::ty
   };
   auto gemm = [&](int phase, int ysub) -> cudaError_t {
     return timed_group(st, vflops(phase, 0), [&] {
+      if constexpr (std::is_same<C, float>::value) {
+        if (d_prefix128) {  // FP32 products of items [tc_first, count) on the tensor cores
+          cudaError_t e2 = cudaSuccess;
+          if (tc_first > 0 && tiles_simt > 0)
+            e2 = launch_group<Item, C, VjpOps, false>(st, dim3(tiles_simt, ysub), d_items, d_plans, d_prefix,
+                                                      tc_first, phase, 0);
+          if (e2 == cudaSuccess && tc_first < count && tiles128 > 0)
+            e2 = launch_group_tc<Item, VjpOps>(st, dim3(tiles128, ysub), d_items + tc_first, d_plans + tc_first,
+                                               d_prefix128, count - tc_first, phase, d_err);
+          return e2;
+        }
+      }
       return launch_group<Item, C, VjpOps, false>(st, dim3(tiles, ysub), d_items, d_plans, d_prefix, count,
                                                   phase, 0);
     });
@@ -2005,7 +2018,7 @@ struct BVLayout {
   using Hi = typename Wide<T>::type;
   static constexpr bool kSplit = !std::is_same<T, Hi>::value;
   std::size_t items_lo = 0, items_hi = 0, plans_lo = 0, plans_hi = 0, prefix_lo = 0, prefix_hi = 0,
-              norms = 0, conv = 0, total = 0;
+              prefix128 = 0, err = 0, norms = 0, conv = 0, total = 0;
   std::vector<std::size_t> slab;
   static std::size_t slab_bytes(int n) {
     if (!kSplit) return vslab_of<T>(n);
@@ -2020,6 +2033,8 @@ struct BVLayout {
     plans_hi = L.used;  L.take<BPlan>(kSplit ? batch : 0);
     prefix_lo = L.used; L.take<int>(batch + 1);
     prefix_hi = L.used; L.take<int>(kSplit ? batch + 1 : 0);
+    prefix128 = L.used; L.take<int>(batch + 1);
+    err = L.used;       L.take<int>(1);
     norms = L.used;     L.take<double>(batch);
     conv = L.used;      L.take<BConv>(kSplit ? 4 * (std::size_t)batch : 0);
     slab.resize(batch);
@@ -2153,8 +2168,23 @@ calamanStatus_t vjp_batched_api(calamanHandle_t blas, calamanStream_t stream, in
     CLM_CUDA(cudaMemcpyAsync(d_lo, lo_items.data(), sizeof(BVItem<T, Hi>) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_plo, lo_plans.data(), sizeof(BPlan) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_xlo, lo_prefix.data(), sizeof(int) * (nlo + 1), cudaMemcpyHostToDevice, st));
+    // FP32 pairs from the schedule's threshold on take the tensor cores
+    const bool tc = std::is_same<T, float>::value;
+    const BatchedTuning tune = blas ? blas->tune : default_batched_tuning();
+    int tc_first = 0;
+    while (tc && tc_first < nlo && lo_n[tc_first] < tune.fp32_tc_min_n) ++tc_first;
+    std::vector<int> tc_prefix(1, 0);
+    for (int i = tc_first; i < nlo; ++i) tc_prefix.push_back(tc_prefix.back() + tiles128_of(lo_n[i]));
+    auto *d_x128 = reinterpret_cast<int *>(base + lay.prefix128);
+    auto *d_err = reinterpret_cast<int *>(base + lay.err);
+    if (tc) {
+      CLM_CUDA(cudaMemcpyAsync(d_x128, tc_prefix.data(), sizeof(int) * tc_prefix.size(), cudaMemcpyHostToDevice,
+                               st));
+      CLM_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    }
     CLM_CUDA(run_vjp_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info,
-                               lo_n, lo_plans));
+                               lo_n, lo_plans, tc ? d_x128 : nullptr, tc_prefix.back(), d_err, tc_first,
+                               lo_prefix[tc_first]));
   }
   if (nhi > 0) {
     const int nin = (int)cin.size(), nout = (int)cout.size();
