@@ -65,41 +65,40 @@ __device__ __forceinline__ R warp_max(R v) {
 // The radix-2 balancing decision of LAPACK xGEBAL for one index, from its
 // off-diagonal column and row 1-norms c, r and the largest magnitudes ca, ra
 // of its column and row (Parlett and Reinsch 1969; LAPACK's DGEBAL, scaling
-// job). Written as two searches for a power of two 2^e:
-//   up:   the most doublings of the column side (halvings of the row side)
-//         while 2^e c stays below 2^-e r / 2 and no scaled quantity reaches
-//         the overflow / underflow guards sfmax2 / sfmin2;
-//   down: from there, the most halvings while 2^-d c' / 2 stays at or above
-//         2^d r', under the same guards.
-// Every scaling is by a power of two, hence exact, so evaluating 2^k x with
-// ldexp gives the values the doubling loops of DGEBAL produce. The factor
-// f = 2^(e - d) is taken when it shrinks c + r below 0.95 of its old value and
-// the accumulated scale d_i f stays inside [sfmin1, sfmax1].
+// job). Two passes over powers of two, each step exact:
+//   grow:   while the column side is below half the row side (c < r / 2) and
+//           no scaled quantity reaches the guards, double the column side and
+//           halve the row side (f *= 2);
+//   shrink: while half the column side is still at least the row side, halve
+//           the column side and double the row side (f /= 2), under the same
+//           guards.
+// f is taken when it shrinks c + r below 0.95 of its old value and the
+// accumulated scale d_i f stays inside [sfmin1, sfmax1].
 template <typename R>
 __device__ __forceinline__ bool balance_step(R c, R r, R ca, R ra, R scale_i, const BalLimits<R> &lim,
                                              R *factor) {
   *factor = (R)1;
   if (c == (R)0 || r == (R)0 || !isfinite(c + r + ca + ra)) return false;
   const R before = c + r;
-  auto p2 = [](R x, int k) { return (R)ldexp(x, k); };
-  int e = 0;
-  for (;;) {  // up
-    const bool stop = p2(c, e) >= p2(r, -e - 1) ||
-                      fmax(fmax(p2((R)1, e), p2(c, e)), p2(ca, e)) >= lim.sfmax2 ||
-                      fmin(fmin(p2(r, -e), p2(r, -e - 1)), p2(ra, -e)) <= lim.sfmin2;
-    if (stop) break;
-    ++e;
+  R f = 1, half_r = r / 2;
+  while (c < half_r && fmax(fmax(f, c), ca) < lim.sfmax2 && fmin(fmin(r, half_r), ra) > lim.sfmin2) {
+    f *= 2;
+    c *= 2;
+    ca *= 2;
+    r /= 2;
+    half_r /= 2;
+    ra /= 2;
   }
-  const R c1 = p2(c, e), r1 = p2(r, -e), ca1 = p2(ca, e), ra1 = p2(ra, -e);
-  int d = 0;
-  for (;;) {  // down
-    const bool stop = p2(c1, -d - 1) < p2(r1, d) || fmax(p2(r1, d), p2(ra1, d)) >= lim.sfmax2 ||
-                      fmin(fmin(p2((R)1, e - d), p2(c1, -d)), fmin(p2(c1, -d - 1), p2(ca1, -d))) <= lim.sfmin2;
-    if (stop) break;
-    ++d;
+  R half_c = c / 2;
+  while (half_c >= r && fmax(r, ra) < lim.sfmax2 && fmin(fmin(f, c), fmin(half_c, ca)) > lim.sfmin2) {
+    f /= 2;
+    c /= 2;
+    half_c /= 2;
+    ca /= 2;
+    r *= 2;
+    ra *= 2;
   }
-  const R f = p2((R)1, e - d);
-  if (!(p2(c1, -d) + p2(r1, d) < (R)0.95 * before)) return false;
+  if (!(c + r < (R)0.95 * before)) return false;
   if (f < (R)1 && scale_i < (R)1 && f * scale_i <= lim.sfmin1) return false;
   if (f > (R)1 && scale_i > (R)1 && scale_i >= lim.sfmax1 / f) return false;
   *factor = f;
