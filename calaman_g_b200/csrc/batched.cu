@@ -837,8 +837,41 @@ template <typename T, int NT, typename Lu> struct BLuOcc {
 // part: 64 x (NT / 4) output blocks, thread (tr, tc) = (t % 16, t / 16) owns
 // rows tr + 16 a and columns 4 tc + b (a, b < 4) of a block; L's 64 rows of a
 // block are staged in shared memory. c0 is a multiple of 4 and blk rows are
-// padded by 64 columns, so the 4-wide shared loads never leave their row.
-template <int NT> constexpr int blk_ld() { return NT + 64; }
+// padded by at least 64 columns, so the 4-wide shared loads never leave their
+// row; the padding also makes the row pitch 4 (mod 32) 4-byte words for float
+// and 2 (mod 16) 8-byte words for double, so the row-block copies below hit
+// 32 distinct banks.
+template <typename T, int NT> constexpr int blk_ld() { return NT + (sizeof(T) == 4 ? 68 : 66); }
+
+// Rows [k, k + jb) of the ncols columns of M (column-major, ld) outside
+// [skip, skip + skipw) to blk[j][c] (kToShared) or back, c the column. Each
+// warp instruction moves 8 consecutive rows of 4 columns: four contiguous
+// 32-byte (float) or 64-byte (double) pieces, where a column per thread
+// would touch 32 lines.
+template <bool kToShared, typename T, int NT>
+__device__ __forceinline__ void blk_rows(T *M, int ld, int k, int jb, int ncols, int skip, int skipw,
+                                         T (*blk)[blk_ld<T, NT>()]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int groups = 4 * ((ncols + 3) >> 2);
+  for (int g = warp; g < groups; g += NT / 32) {
+    const int j = (g & 3) * 8 + (lane & 7), ci = (g >> 2) * 4 + (lane >> 3);
+    if (j < jb && ci < ncols) {
+      const int c = ci < skip ? ci : ci + skipw;
+      if (kToShared) blk[j][c] = M[(std::size_t)c * ld + k + j];
+      else M[(std::size_t)c * ld + k + j] = blk[j][c];
+    }
+  }
+}
+
+// The jb x jb diagonal block of Q (ld n) at (k, k) to diag[row][column],
+// consecutive threads reading down a column.
+template <typename T, int NT>
+__device__ __forceinline__ void stage_diag(const T *Q, int n, int k, int jb, T (*diag)[kBPanel + 1]) {
+  for (int e = threadIdx.x; e < jb * jb; e += NT) {
+    const int q = e / jb, j = e - q * jb;
+    diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
+  }
+}
 
 // Triangular solves of one right-hand-side column against the diagonal block
 // in shared memory: unit lower (forward) and non-unit upper with the diagonal's
@@ -869,7 +902,7 @@ __device__ __forceinline__ void trsv_upper(T (&x)[kBPanel], const T (*diag)[kBPa
 template <typename T, int NT>
 __device__ void cta_update(T *__restrict__ D, int ldd, int r0, int mrows, int c0, int ncols,
                            const T *__restrict__ L, int ldl, int jb,
-                           const T (*__restrict__ blk)[blk_ld<NT>()], T (*__restrict__ Ls)[64]) {
+                           const T (*__restrict__ blk)[blk_ld<T, NT>()], T (*__restrict__ Ls)[64]) {
   constexpr int CB = NT / 4;  // columns per block
   const int t = threadIdx.x, tr = t & 15, tc = t >> 4;
   for (int rb = 0; rb < mrows; rb += 64) {
@@ -964,7 +997,7 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT, Lu>::kMinBlocks)
   // right-hand-side block rows), Ls[kBPanel][64] (staged L rows of the block
   // updates), then diag[kBPanel][kBPanel + 1]
   extern __shared__ __align__(16) unsigned char b_smem[];
-  constexpr int LD = blk_ld<NT>();
+  constexpr int LD = blk_ld<T, NT>();
   auto blk = reinterpret_cast<T(*)[LD]>(b_smem);
   auto Ls = reinterpret_cast<T(*)[64]>(b_smem + sizeof(T) * kBPanel * LD);
   auto diag = reinterpret_cast<T(*)[kBPanel + 1]>(b_smem + sizeof(T) * kBPanel * (LD + 64));
@@ -1092,16 +1125,15 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT, Lu>::kMinBlocks)
       for (int j = 0; j < kBPanel; ++j)
         if (j < jb) diag[t - k][j] = r[j];
     }
+    // columns outside the panel: the old top block to shared memory
+    blk_rows<true, T, NT>(Q, n, k, jb, n - jb, k, jb, blk);
     __syncthreads();
-    // columns outside the panel: apply the panel's swaps (rows >= k + jb only
-    // ever receive rows of the top block [k, k + jb)), then, right of the
-    // panel, solve the top block with the unit-lower L11
+    // apply the panel's swaps (rows >= k + jb only ever receive rows of the
+    // top block [k, k + jb)), then, right of the panel, solve the top block
+    // with the unit-lower L11; the new top block goes back through blk
     if (t < n - jb) {
       const int c = t < k ? t : t + jb;
       T *col = Q + (std::size_t)c * n;
-#pragma unroll
-      for (int j = 0; j < kBPanel; ++j)
-        if (j < jb) blk[j][c] = col[k + j];  // the old top block, staged
       T x[kBPanel];
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j) {
@@ -1124,13 +1156,12 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT, Lu>::kMinBlocks)
       }
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
-        if (j < jb) {
-          blk[j][c] = x[j];
-          col[k + j] = x[j];
-        }
+        if (j < jb) blk[j][c] = x[j];
     }
     __syncthreads();
-    // trailing update A22 -= L21 U12 by the whole CTA
+    blk_rows<false, T, NT>(Q, n, k, jb, n - jb, k, jb, blk);
+    // trailing update A22 -= L21 U12 by the whole CTA (its first barrier
+    // orders the copy above before blk is rewritten)
     cta_update<T, NT>(Q, n, k + jb, n - k - jb, k + jb, n - k - jb, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
   if (kFactor) {
@@ -1159,59 +1190,49 @@ __global__ void __launch_bounds__(NT, BLuOcc<T, NT, Lu>::kMinBlocks)
   // forward, unit lower
   for (int k = 0; k < n; k += kBPanel) {
     const int jb = min(kBPanel, n - k);
-    for (int e = t; e < jb * jb; e += NT) {
-      const int j = e / jb, q = e - j * jb;  // row j, column q of the block
-      diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
-    }
+    stage_diag<T, NT>(Q, n, k, jb, diag);
+    blk_rows<true, T, NT>(D, ldd, k, jb, n, n, 0, blk);
     __syncthreads();
     if (t < n) {
-      T *col = D + (std::size_t)t * ldd;
       T x[kBPanel];
 #pragma unroll
-      for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? col[k + j] : elem<T>::zero();
+      for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? blk[j][t] : elem<T>::zero();
       if (jb == kBPanel) trsv_lower_unit<T, true>(x, diag, jb);
       else trsv_lower_unit<T, false>(x, diag, jb);
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
-        if (j < jb) {
-          blk[j][t] = x[j];
-          col[k + j] = x[j];
-        }
+        if (j < jb) blk[j][t] = x[j];
     }
     __syncthreads();
+    blk_rows<false, T, NT>(D, ldd, k, jb, n, n, 0, blk);
     cta_update<T, NT>(D, ldd, k + jb, n - k - jb, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
   // backward, non-unit upper
   for (int k = ((n - 1) / kBPanel) * kBPanel; k >= 0; k -= kBPanel) {
     const int jb = min(kBPanel, n - k);
-    for (int e = t; e < jb * jb; e += NT) {
-      const int j = e / jb, q = e - j * jb;
-      diag[j][q] = Q[(std::size_t)(k + q) * n + k + j];
-    }
+    stage_diag<T, NT>(Q, n, k, jb, diag);
+    blk_rows<true, T, NT>(D, ldd, k, jb, n, n, 0, blk);
     __syncthreads();
     if (t < jb) rdiag[t] = divide(elem<T>::one(), diag[t][t]);
     __syncthreads();
     if (t < n) {
-      T *col = D + (std::size_t)t * ldd;
       T x[kBPanel];
 #pragma unroll
-      for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? col[k + j] : elem<T>::zero();
+      for (int j = 0; j < kBPanel; ++j) x[j] = j < jb ? blk[j][t] : elem<T>::zero();
       if (jb == kBPanel) trsv_upper<T, true>(x, diag, rdiag, jb);
       else trsv_upper<T, false>(x, diag, rdiag, jb);
 #pragma unroll
       for (int j = 0; j < kBPanel; ++j)
-        if (j < jb) {
-          blk[j][t] = x[j];
-          col[k + j] = x[j];
-        }
+        if (j < jb) blk[j][t] = x[j];
     }
     __syncthreads();
+    blk_rows<false, T, NT>(D, ldd, k, jb, n, n, 0, blk);
     cta_update<T, NT>(D, ldd, 0, k, 0, n, Q + (std::size_t)k * n, n, jb, blk, Ls);
   }
 }
 
 template <typename T, int NT> constexpr std::size_t lu_smem_bytes() {
-  return sizeof(T) * (kBPanel * (blk_ld<NT>() + 64) + kBPanel * (kBPanel + 1));
+  return sizeof(T) * (kBPanel * (blk_ld<T, NT>() + 64) + kBPanel * (kBPanel + 1));
 }
 
 // The LU kernel over a batch sorted by n (ascending), one launch per run of
