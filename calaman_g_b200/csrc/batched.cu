@@ -1484,6 +1484,36 @@ inline int tiles_of(int n) {
   return t * t;
 }
 
+// The handle's second stream for the FP64 matrices of a mixed batch (they
+// share no buffer with the FP32 ones: one stream per precision pipeline keeps
+// the tensor cores busy with FP32 products while the FP64 products and LUs
+// run), created on first use with its fork and join events. side = nullptr:
+// one stream (no handle, or kernel timing, or a batch of one precision).
+cudaError_t side_stream(calamanHandle_t blas, bool want, cudaStream_t &side) {
+  side = nullptr;
+  if (!want || blas == nullptr || tl_timer != nullptr) return cudaSuccess;
+  if (blas->side == nullptr) {
+    cudaError_t e = cudaEventCreateWithFlags(&blas->side_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&blas->side_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&blas->side, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+  }
+  side = blas->side;
+  return cudaSuccess;
+}
+
+// Fork (before) or join (after) the side stream around a call's launches.
+cudaError_t side_fork(calamanHandle_t blas, cudaStream_t st, cudaStream_t side) {
+  if (side == nullptr) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(blas->side_fork, st);
+  return e == cudaSuccess ? cudaStreamWaitEvent(side, blas->side_fork, 0) : e;
+}
+cudaError_t side_join(calamanHandle_t blas, cudaStream_t st, cudaStream_t side) {
+  if (side == nullptr) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(blas->side_join, side);
+  return e == cudaSuccess ? cudaStreamWaitEvent(st, blas->side_join, 0) : e;
+}
+
 template <typename T>
 calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int batch, const int *h_n,
                             const T *const *h_A, const int *h_lda, T *const *h_E, const int *h_lde,
@@ -1621,25 +1651,30 @@ calamanStatus_t batched_api(calamanHandle_t blas, calamanStream_t stream, int ba
     CLM_CUDA(cudaMemcpyAsync(d_cin, cin.data(), sizeof(BConv) * nhi, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_cout, cout.data(), sizeof(BConv) * nhi, cudaMemcpyHostToDevice, st));
   }
-  // every kernel of the call
+  // every kernel of the call; a mixed batch runs its FP64 matrices on the
+  // handle's side stream, beside the FP32 ones
+  cudaStream_t side = nullptr;
+  CLM_CUDA(side_stream(blas, nlo > 0 && nhi > 0, side));
   auto launch_all = [&]() -> cudaError_t {
     cudaError_t e;
+    if ((e = side_fork(blas, st, side)) != cudaSuccess) return e;
+    if (nhi > 0) {
+      cudaStream_t sh = side ? side : st;
+      const dim3 ew((unsigned)nhi, (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk));
+      b_conv_kernel<T, Hi><<<ew, 256, 0, sh>>>(d_cin);
+      if ((e = launched()) != cudaSuccess) return e;
+      if ((e = run_phases<Hi>(sh, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info, hi_n,
+                              hi_plans, nullptr, 0, nullptr, 0, 0, tune.lu_threads)) != cudaSuccess)
+        return e;
+      b_conv_kernel<Hi, T><<<ew, 256, 0, sh>>>(d_cout);
+      if ((e = launched()) != cudaSuccess) return e;
+    }
     if (nlo > 0 &&
         (e = run_phases<T>(st, d_lo, d_plo, d_xlo, nlo, lo_prefix.back(), lo_max_n, lo_max_s, d_info, lo_n,
                            lo_plans, tc ? d_x128 : nullptr, tc_prefix.back(), d_err, tc_first,
                            lo_prefix[tc_first], tune.lu_threads)) != cudaSuccess)
       return e;
-    if (nhi > 0) {
-      const dim3 ew((unsigned)nhi, (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk));
-      b_conv_kernel<T, Hi><<<ew, 256, 0, st>>>(d_cin);
-      if ((e = launched()) != cudaSuccess) return e;
-      if ((e = run_phases<Hi>(st, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info, hi_n,
-                              hi_plans, nullptr, 0, nullptr, 0, 0, tune.lu_threads)) != cudaSuccess)
-        return e;
-      b_conv_kernel<Hi, T><<<ew, 256, 0, st>>>(d_cout);
-      if ((e = launched()) != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    return side_join(blas, st, side);
   };
   // Graph replay: the launches depend only on the call's configuration, so a
   // configuration seen twice in a row is captured once and replayed after.
@@ -2185,6 +2220,27 @@ calamanStatus_t vjp_batched_api(calamanHandle_t blas, calamanStream_t stream, in
     }
   }
   const int nlo = (int)lo_items.size(), nhi = (int)hi_items.size();
+  // a mixed batch runs its FP64 pairs on the handle's side stream, beside the
+  // FP32 ones (every table is uploaded on st before the fork)
+  cudaStream_t side = nullptr;
+  CLM_CUDA(side_stream(blas, nlo > 0 && nhi > 0, side));
+  cudaStream_t sh = side ? side : st;
+  if (nhi > 0) {
+    const int nin = (int)cin.size(), nout = (int)cout.size();
+    CLM_CUDA(cudaMemcpyAsync(d_hi, hi_items.data(), sizeof(BVItem<Hi, Hi>) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_phi, hi_plans.data(), sizeof(BPlan) * nhi, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_xhi, hi_prefix.data(), sizeof(int) * (nhi + 1), cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_conv, cin.data(), sizeof(BConv) * nin, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(cudaMemcpyAsync(d_conv + nin, cout.data(), sizeof(BConv) * nout, cudaMemcpyHostToDevice, st));
+    CLM_CUDA(side_fork(blas, st, side));
+    const unsigned chunks = (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk);
+    b_conv_kernel<T, Hi><<<dim3((unsigned)nin, chunks), 256, 0, sh>>>(d_conv);
+    CLM_CUDA(launched());
+    CLM_CUDA(run_vjp_phases<Hi>(sh, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info,
+                                hi_n, hi_plans));
+    b_conv_kernel<Hi, T><<<dim3((unsigned)nout, chunks), 256, 0, sh>>>(d_conv + nin);
+    CLM_CUDA(launched());
+  }
   if (nlo > 0) {
     CLM_CUDA(cudaMemcpyAsync(d_lo, lo_items.data(), sizeof(BVItem<T, Hi>) * nlo, cudaMemcpyHostToDevice, st));
     CLM_CUDA(cudaMemcpyAsync(d_plo, lo_plans.data(), sizeof(BPlan) * nlo, cudaMemcpyHostToDevice, st));
@@ -2207,21 +2263,7 @@ calamanStatus_t vjp_batched_api(calamanHandle_t blas, calamanStream_t stream, in
                                lo_n, lo_plans, tc ? d_x128 : nullptr, tc_prefix.back(), d_err, tc_first,
                                lo_prefix[tc_first]));
   }
-  if (nhi > 0) {
-    const int nin = (int)cin.size(), nout = (int)cout.size();
-    CLM_CUDA(cudaMemcpyAsync(d_hi, hi_items.data(), sizeof(BVItem<Hi, Hi>) * nhi, cudaMemcpyHostToDevice, st));
-    CLM_CUDA(cudaMemcpyAsync(d_phi, hi_plans.data(), sizeof(BPlan) * nhi, cudaMemcpyHostToDevice, st));
-    CLM_CUDA(cudaMemcpyAsync(d_xhi, hi_prefix.data(), sizeof(int) * (nhi + 1), cudaMemcpyHostToDevice, st));
-    CLM_CUDA(cudaMemcpyAsync(d_conv, cin.data(), sizeof(BConv) * nin, cudaMemcpyHostToDevice, st));
-    CLM_CUDA(cudaMemcpyAsync(d_conv + nin, cout.data(), sizeof(BConv) * nout, cudaMemcpyHostToDevice, st));
-    const unsigned chunks = (unsigned)((hi_max_n * hi_max_n + kEwChunk - 1) / kEwChunk);
-    b_conv_kernel<T, Hi><<<dim3((unsigned)nin, chunks), 256, 0, st>>>(d_conv);
-    CLM_CUDA(launched());
-    CLM_CUDA(run_vjp_phases<Hi>(st, d_hi, d_phi, d_xhi, nhi, hi_prefix.back(), hi_max_n, hi_max_s, d_info,
-                                hi_n, hi_plans));
-    b_conv_kernel<Hi, T><<<dim3((unsigned)nout, chunks), 256, 0, st>>>(d_conv + nin);
-    CLM_CUDA(launched());
-  }
+  CLM_CUDA(side_join(blas, st, side));
   return ok_status();
 }
 

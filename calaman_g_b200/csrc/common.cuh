@@ -352,5 +352,9 @@ struct calamanContext {
   clm::BatchedTuning tune = clm::default_batched_tuning();
   int graphs = 1;              // batched calls replay a captured CUDA graph of their launches
   clm::BatchedGraph graph[2];  // per batched tier: [0] float, [1] double
+  // second stream of the batched mixed tiers (the FP64 matrices run on it
+  // beside the FP32 ones) and the fork / join events, created on first use
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_fork = nullptr, side_join = nullptr;
   clm::KernelTimer timer;
 };

@@ -443,6 +443,9 @@ calamanStatus_t calamanDestroy(calamanHandle_t handle) {
   if (handle->h_pinned) cudaFreeHost(handle->h_pinned);
   for (auto &g : handle->graph)
     if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
+  if (handle->side) cudaStreamDestroy(handle->side);
+  if (handle->side_fork) cudaEventDestroy(handle->side_fork);
+  if (handle->side_join) cudaEventDestroy(handle->side_join);
   delete handle;
   return ok_status();
 }
