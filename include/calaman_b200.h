@@ -186,8 +186,11 @@ calamanStatus_t calaman_expm_vjp_z(calamanBlasHandle_t blas, calamanSolverHandle
  * ints ([2i] LU info of matrix i, [2i + 1] solve info). h_plans (host, may be
  * NULL) receives every plan. Synchronises `stream` once (one readback of all
  * norms); a non-finite norm anywhere fails the whole call with
- * INVALID_VALUE before any output is written. The _s tier multiplies in FP32
- * and squares in FP64, like calaman_expm_s. */
+ * INVALID_VALUE before any output is written. The _s tier evaluates matrices
+ * with s_i = 0 in FP32 and those with s_i > 0 wholly in FP64. When a batch
+ * holds both, the FP64 ones run on a second stream that the blas handle
+ * creates on first use (non-blocking, forked from and joined back to `stream`
+ * within the call, released by calamanDestroy). */
 calamanStatus_t calaman_expm_batched_bufferSize_s(calamanSolverHandle_t h, int batch,
                                                   const int *h_n, size_t *bytes);
 calamanStatus_t calaman_expm_batched_bufferSize_d(calamanSolverHandle_t h, int batch,
