@@ -781,7 +781,7 @@ template <typename T> constexpr bool panel_rotates() {
 
 // One pivot step's search and row exchange. The pivot is the largest
 // |Re| + |Im| of column col among rows >= a, first index on ties; the owner of
-// row a publishes that row into slot 16. kOneBarrier: every warp's winner
+// row a publishes that row into slot kRowA (after the warps' slots). kOneBarrier: every warp's winner
 // publishes its whole row into the warp's slot before the single barrier, and
 // after it every thread agrees on the pivot p and reads the pivot row from its
 // slot (the caller alternates buffers by step: a slot is rewritten two steps
@@ -790,7 +790,7 @@ template <typename T> constexpr bool panel_rotates() {
 // its row into slot 0 before a second barrier; measured faster with one row
 // per thread (float64, 256 rows: 2.5 %), slower with two or more. Returns the
 // slot of the pivot row. forced: no comparable candidate (NaN column), p = a.
-template <typename T, int KBS, int RPT, bool kOneBarrier>
+template <typename T, int KBS, int RPT, bool kOneBarrier, int kRowA>
 __device__ __forceinline__ int panel_pivot(const T (&r)[RPT][KBS], int col, int a, int h, T (*wrow)[KBS],
                                            unsigned long long *red_key, int *red_idx, int &p, bool &forced,
                                            double &pv) {
@@ -810,7 +810,7 @@ __device__ __forceinline__ int panel_pivot(const T (&r)[RPT][KBS], int col, int 
       const int gi = tid + q * NT;
       if (gi == a) {
 #pragma unroll
-        for (int c = 0; c < KBS; ++c) wrow[16][c] = r[q][c];
+        for (int c = 0; c < KBS; ++c) wrow[kRowA][c] = r[q][c];
       }
       if (gi == wa.idx) {
 #pragma unroll
@@ -832,7 +832,7 @@ __device__ __forceinline__ int panel_pivot(const T (&r)[RPT][KBS], int col, int 
       pv = 0.0;
       forced = true;
     }
-    return forced ? 16 : wp;
+    return forced ? kRowA : wp;
   } else {
     const ArgMax am = cta_argmax(argmax_key(bv, bi, bi != INT_MAX), red_key, red_idx);
     pv = __longlong_as_double((long long)am.key);
@@ -848,7 +848,7 @@ __device__ __forceinline__ int panel_pivot(const T (&r)[RPT][KBS], int col, int 
       const int gi = tid + q * NT;
       if (gi == a) {
 #pragma unroll
-        for (int c = 0; c < KBS; ++c) wrow[16][c] = r[q][c];
+        for (int c = 0; c < KBS; ++c) wrow[kRowA][c] = r[q][c];
       }
       if (gi == p) {
 #pragma unroll
@@ -860,8 +860,8 @@ __device__ __forceinline__ int panel_pivot(const T (&r)[RPT][KBS], int col, int 
   }
 }
 
-template <typename T, int KBS, int RPT, bool kRotate = panel_rotates<T>()>
-__global__ void __launch_bounds__(512, 1)
+template <typename T, int KBS, int RPT, int MAXT = 512, bool kRotate = panel_rotates<T>()>
+__global__ void __launch_bounds__(MAXT, 1)
     lu_panel_cta_kernel(int n, T *__restrict__ A, int lda, int k, int kb, int *__restrict__ ipiv,
                         int *__restrict__ perm, int *__restrict__ g_map_pos, int *__restrict__ g_map_src,
                         int *__restrict__ g_map_count, int *__restrict__ info) {
@@ -870,13 +870,14 @@ __global__ void __launch_bounds__(512, 1)
   const int NT = blockDim.x, nwarps = NT >> 5;
   const int h = n - k;
   T *P = A + (std::size_t)k * lda + k;  // the panel: P[c * lda + i], i < h, c < kb
-  // per pivot step, alternating: slots 0..15 each warp winner's row, slot 16
-  // row a before the exchange
-  __shared__ __align__(16) T wrow[2][17][KBS];
+  // per pivot step, alternating: slots 0..kW-1 each warp winner's row, slot
+  // kW row a before the exchange
+  constexpr int kW = MAXT / 32;  // warps at most (MAXT threads)
+  __shared__ __align__(16) T wrow[2][kW + 1][KBS];
   __shared__ T l11[KBS][KBS + 1];
   __shared__ __align__(16) T u12[KBS][kMaxKb];
-  __shared__ unsigned long long red_key[2][16];
-  __shared__ int red_idx[2][16];
+  __shared__ unsigned long long red_key[2][kW];
+  __shared__ int red_idx[2][kW];
   __shared__ int plist[kMaxKb];
   __shared__ int flags[1];
   __shared__ int mpos[2 * kMaxKb], morg[2 * kMaxKb];
@@ -908,7 +909,7 @@ __global__ void __launch_bounds__(512, 1)
         int p;
         bool forced;
         double pv;
-        const int ps = panel_pivot<T, KBS, RPT, (RPT > 1)>(r, 0, a, h, wrow[buf], red_key[buf], red_idx[buf], p, forced, pv);
+        const int ps = panel_pivot<T, KBS, RPT, (RPT > 1), kW>(r, 0, a, h, wrow[buf], red_key[buf], red_idx[buf], p, forced, pv);
         const T *prow = wrow[buf][ps];
         if (tid == 0) {
           plist[a] = p;
@@ -932,7 +933,7 @@ __global__ void __launch_bounds__(512, 1)
           }
           if (gi == p) {
 #pragma unroll
-            for (int c = 0; c < KBS; ++c) r[q][c] = wrow[buf][16][c];
+            for (int c = 0; c < KBS; ++c) r[q][c] = wrow[buf][kW][c];
           }
           const T l = singular ? r[q][0] : (use_recip ? mul(r[q][0], rpiv) : divide(r[q][0], piv));
           r[q][0] = l;
@@ -958,7 +959,7 @@ __global__ void __launch_bounds__(512, 1)
       int p;
       bool forced;
       double pv;
-      const int ps = panel_pivot<T, KBS, RPT, (RPT > 1)>(r, j, a, h, wrow[buf], red_key[buf], red_idx[buf], p, forced, pv);
+      const int ps = panel_pivot<T, KBS, RPT, (RPT > 1), kW>(r, j, a, h, wrow[buf], red_key[buf], red_idx[buf], p, forced, pv);
       const T *prow = wrow[buf][ps];
       if (tid == 0) {
         plist[a] = p;
@@ -981,7 +982,7 @@ __global__ void __launch_bounds__(512, 1)
         }
         if (gi == p) {
 #pragma unroll
-          for (int c = 0; c < KBS; ++c) r[q][c] = wrow[buf][16][c];
+          for (int c = 0; c < KBS; ++c) r[q][c] = wrow[buf][kW][c];
         }
         const T l = singular ? r[q][j] : (use_recip ? mul(r[q][j], rpiv) : divide(r[q][j], piv));
         r[q][j] = l;
@@ -1114,20 +1115,24 @@ __global__ void __launch_bounds__(512, 1)
 }
 
 // One-CTA panel configurations by height: RPT rows per thread for heights up
-// to 512 RPT, sub-panel width KBS (64 registers of sub-panel per thread at
-// most), outer panel width KB.
+// to 512 RPT (512 threads), sub-panel width KBS (64 registers of sub-panel per
+// thread at most), outer panel width KB. Heights 2049..4096 take RPT8 rows per
+// thread on NT8 threads: float32 runs 1024 threads of 4 rows there (64
+// registers, a few spilled), measured 5 % faster on the float32 4096 expm than
+// 512 threads of 8 rows; float64 1024 x 2 rows at heights up to 2048, and
+// complex128 1024 x 1 row (sub-panels of 4) at 1024, measured slower.
 template <typename T> struct CtaPanel;
 template <> struct CtaPanel<double2> {
-  static constexpr int KBS1 = 8, KBS2 = 8, KBS4 = 4, KBS8 = 0, KB = 32;
+  static constexpr int KBS1 = 8, KBS2 = 8, KBS4 = 4, KBS8 = 0, RPT8 = 8, NT8 = 512, KB = 32;
 };
 template <> struct CtaPanel<double> {
-  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, KB = 32;
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, RPT8 = 8, NT8 = 512, KB = 32;
 };
 template <> struct CtaPanel<float2> {
-  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, KB = 32;
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, RPT8 = 8, NT8 = 512, KB = 32;
 };
 template <> struct CtaPanel<float> {  // 32 wide: the in-panel SIMT update costs h kb^2 / 2 per panel
-  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, KB = 32;
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, RPT8 = 4, NT8 = 1024, KB = 32;
 };
 
 // Panel width of the one-CTA path for an n x n factorisation, 0 if n is too
@@ -1202,7 +1207,7 @@ cudaError_t launch_reg_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb
                             sc.map_src, sc.map_count, info);
 }
 
-template <typename T, int KBS, int RPT>
+template <typename T, int KBS, int RPT, int MAXT = 512>
 cudaError_t launch_cta_panel_cfg(cudaStream_t s, int n, T *A, int lda, int k, int kb, const LuScratch &sc,
                                  int *info) {
   const int h = n - k;
@@ -1218,7 +1223,7 @@ cudaError_t launch_cta_panel_cfg(cudaStream_t s, int n, T *A, int lda, int k, in
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   note_launch();
-  return cudaLaunchKernelEx(&cfg, lu_panel_cta_kernel<T, KBS, RPT>, n, A, lda, k, kb, sc.ipiv, sc.perm,
+  return cudaLaunchKernelEx(&cfg, lu_panel_cta_kernel<T, KBS, RPT, MAXT>, n, A, lda, k, kb, sc.ipiv, sc.perm,
                             sc.map_pos, sc.map_src, sc.map_count, info);
 }
 
@@ -1234,7 +1239,8 @@ cudaError_t launch_cta_panel(cudaStream_t s, int n, T *A, int lda, int k, int kb
   } else if (n <= 2048) {
     if constexpr (C::KBS4 > 0) return launch_cta_panel_cfg<T, C::KBS4, 4>(s, n, A, lda, k, kb, sc, info);
   } else {
-    if constexpr (C::KBS8 > 0) return launch_cta_panel_cfg<T, C::KBS8, 8>(s, n, A, lda, k, kb, sc, info);
+    if constexpr (C::KBS8 > 0)
+      return launch_cta_panel_cfg<T, C::KBS8, C::RPT8, C::NT8>(s, n, A, lda, k, kb, sc, info);
   }
   return cudaErrorInvalidValue;
 }

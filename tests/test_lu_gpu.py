@@ -64,7 +64,7 @@ def test_getrf_matches_oracle_exactly_in_pivots(lib, oracle, suf, n):
 
 
 @pytest.mark.parametrize("suf", ["s", "c"])
-@pytest.mark.parametrize("n", [5, 64, 200, 700])
+@pytest.mark.parametrize("n", [5, 64, 200, 700, 3001])  # 3001: the tallest one-CTA panel class
 def test_getrf_single_backward_error(lib, suf, n):
     a = gaussian(n, suf, 600 + n)
     _, _, lu, ipiv, info = run_getrf(lib, a, suf)
