@@ -703,10 +703,11 @@ __global__ void gather_rows_kernel(int n, int nrhs, const int *__restrict__ perm
     X[(std::size_t)c * ldx + row] = B[(std::size_t)c * ldb + src];
 }
 
-// Diagonal-block triangular solve on rows [k, k+kb) of X, one warp per RHS
-// column. LOWER: unit lower (forward); else non-unit upper (backward), whose
-// diagonal reciprocals are formed once per block, off the dependent chain.
-template <typename T, bool LOWER>
+// Diagonal-block triangular solve on rows [k, k+kb) of X (kb <= 32 VPL), one
+// warp per RHS column, lane l keeping rows l, l + 32, ... LOWER: unit lower
+// (forward); else non-unit upper (backward), whose diagonal reciprocals are
+// formed once per block, off the dependent chain.
+template <typename T, bool LOWER, int VPL>
 __global__ void __launch_bounds__(256)
     trsm_diag_kernel(int nrhs, const T *__restrict__ LU, int lda, int k, int kb, T *__restrict__ X,
                      int ldx) {
@@ -725,25 +726,37 @@ __global__ void __launch_bounds__(256)
   const int c = blockIdx.x * warps + (threadIdx.x >> 5);
   if (c >= nrhs) return;
   T *col = X + (std::size_t)c * ldx + k;
-  T x0 = lane < kb ? col[lane] : elem<T>::zero();
-  T x1 = lane + 32 < kb ? col[lane + 32] : elem<T>::zero();
+  T x[VPL];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v) x[v] = lane + 32 * v < kb ? col[lane + 32 * v] : elem<T>::zero();
   if (LOWER) {
     for (int l = 0; l < kb; ++l) {
-      const T xl = shfl(l < 32 ? x0 : x1, l & 31);
-      if (lane > l && lane < kb) x0 = sub(x0, mul(D[l * kb + lane], xl));
-      if (lane + 32 > l && lane + 32 < kb) x1 = sub(x1, mul(D[l * kb + lane + 32], xl));
+      T src = x[0];
+#pragma unroll
+      for (int v = 1; v < VPL; ++v)
+        if ((l >> 5) == v) src = x[v];
+      const T xl = shfl(src, l & 31);
+#pragma unroll
+      for (int v = 0; v < VPL; ++v)
+        if (lane + 32 * v > l && lane + 32 * v < kb) x[v] = sub(x[v], mul(D[l * kb + lane + 32 * v], xl));
     }
   } else {
     for (int l = kb - 1; l >= 0; --l) {
-      const T xl = mul(shfl(l < 32 ? x0 : x1, l & 31), rdiag[l]);
-      if (lane == l) x0 = xl;
-      if (lane + 32 == l) x1 = xl;
-      if (lane < l) x0 = sub(x0, mul(D[l * kb + lane], xl));
-      if (lane + 32 < l) x1 = sub(x1, mul(D[l * kb + lane + 32], xl));
+      T src = x[0];
+#pragma unroll
+      for (int v = 1; v < VPL; ++v)
+        if ((l >> 5) == v) src = x[v];
+      const T xl = mul(shfl(src, l & 31), rdiag[l]);
+#pragma unroll
+      for (int v = 0; v < VPL; ++v) {
+        if (lane + 32 * v == l) x[v] = xl;
+        if (lane + 32 * v < l) x[v] = sub(x[v], mul(D[l * kb + lane + 32 * v], xl));
+      }
     }
   }
-  if (lane < kb) col[lane] = x0;
-  if (lane + 32 < kb) col[lane + 32] = x1;
+#pragma unroll
+  for (int v = 0; v < VPL; ++v)
+    if (lane + 32 * v < kb) col[lane + 32 * v] = x[v];
 }
 
 // ---------------------------------------------------------------------------
@@ -1417,11 +1430,15 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
     gather_rows_kernel<T><<<dim3((n + 255) / 256, gy), 256, 0, s>>>(n, nrhs, sc.perm, B, ldb, X, ldx);
     if ((e = launched()) != cudaSuccess) return e;
   }
-  constexpr int NB = 64;
+  // Diagonal blocks of 64 rows; float32 systems above 1024 take 128 (half as
+  // many passes of the off-diagonal updates over the right-hand side: float32
+  // 4096 expm +3 %; float64 2048 measured 8 % slower with 128)
+  const bool wide = std::is_same<T, float>::value && n > 1024;
+  const int NB = wide ? 128 : 64;
   const int warps = 8;
   const std::size_t smem = sizeof(T) * (NB * NB + NB);
-  auto kl = trsm_diag_kernel<T, true>;
-  auto ku = trsm_diag_kernel<T, false>;
+  auto kl = wide ? trsm_diag_kernel<T, true, 4> : trsm_diag_kernel<T, true, 2>;
+  auto ku = wide ? trsm_diag_kernel<T, false, 4> : trsm_diag_kernel<T, false, 2>;
   if ((e = cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
   if ((e = cudaFuncSetAttribute(ku, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
   const int blocks = (nrhs + warps - 1) / warps;

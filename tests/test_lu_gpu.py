@@ -82,7 +82,7 @@ def test_getrf_single_backward_error(lib, suf, n):
 
 
 @pytest.mark.parametrize("suf", ["s", "d", "c", "z"])
-@pytest.mark.parametrize("n,nrhs", [(1, 1), (9, 3), (64, 64), (130, 7), (400, 400)])
+@pytest.mark.parametrize("n,nrhs", [(1, 1), (9, 3), (64, 64), (130, 7), (400, 400), (1500, 77)])
 def test_getrs_solves(lib, suf, n, nrhs):
     import torch
 
