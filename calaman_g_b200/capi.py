@@ -145,6 +145,8 @@ SIGNATURES["calaman_poly_tensor_workspace_s"] = (c_size_t, [c_int])
 SIGNATURES["calaman_grid_barrier_wait_check"] = (Status, [c_void_p, ctypes.c_uint, c_void_p, c_size_t, c_int_p])
 SIGNATURES["calamanSetBatchedGraphs"] = (Status, [_H, c_int])
 SIGNATURES["calamanGetBatchedGraphs"] = (Status, [_H, c_int_p, c_int_p])
+SIGNATURES["calamanSetExpmGraphs"] = (Status, [_H, c_int])
+SIGNATURES["calamanGetExpmGraphs"] = (Status, [_H, c_int_p, c_int_p])
 SIGNATURES["calamanSetBatchedTuning"] = (Status, [_H, c_int_p, c_int])
 SIGNATURES["calamanGetBatchedTuning"] = (Status, [_H, c_int_p, c_int_p])
 SIGNATURES["calamanTuneBatched_bufferSize"] = (c_size_t, [c_int])

@@ -143,6 +143,11 @@ calamanStatus_t pade_api(calamanHandle_t blas, calamanStream_t stream, int m, in
 }
 
 // ---- expm<T>, src/expm/expm.cppm:87-174 -------------------------------------
+// The handle's graph slot of each expm type.
+template <typename T> constexpr int type_slot() {
+  return std::is_same<T, float>::value ? 0 : std::is_same<T, double>::value ? 1 : std::is_same<T, float2>::value ? 2 : 3;
+}
+
 template <typename T>
 calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, const T *A, int lda,
                          T *E, int lde, void *work, std::size_t lwork, int *d_info,
@@ -170,43 +175,100 @@ calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, co
   const calamanExpmPlan_t chosen = plan_for<R>((R)norm);
   if (plan_out) *plan_out = chosen;
 
-  const T *src = A;
-  int ld_src = lda;
-  if (chosen.s > 0) {
-    CLM_CUDA(launch_scale_copy<T>(st, n, std::ldexp(1.0, -chosen.s), A, lda, ws.As, n));
-    src = ws.As;
-    ld_src = n;
-  }
-  CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info, blas));
-
-  // the squarings borrow the (now free) Pade region's digit planes
-  PadeWs<T> pw;
-  pw.carve(ws.pade, n, chosen.m, oz_scratch_bytes<T>(blas, n));
-  GemmScratch gs = lend_scratch<T>(blas, n, nullptr, 0, pw.oz, pw.oz_bytes);
-  GemmScratchScope gss(pw.oz ? &gs : nullptr);
-
-  if (elem<T>::single && chosen.s > 0) {
-    // single tiers: the squarings, where errors grow, run in FP64 tensor cores
-    using W = typename Wide<T>::type;
-    W *cw = ws.wide, *ow = ws.wide + (std::size_t)n * n;
-    CLM_CUDA((launch_convert<T, W>(st, n, E, lde, cw, n)));
-    for (int k = 0; k < chosen.s; ++k) {
-      CLM_CUDA(gemm_nn<W>(st, n, n, n, 1.0, cw, n, cw, n, 0.0, ow, n));
-      std::swap(cw, ow);
+  // everything after the plan: launches only, no host synchronisation
+  auto post = [&]() -> calamanStatus_t {
+    const T *src = A;
+    int ld_src = lda;
+    if (chosen.s > 0) {
+      CLM_CUDA(launch_scale_copy<T>(st, n, std::ldexp(1.0, -chosen.s), A, lda, ws.As, n));
+      src = ws.As;
+      ld_src = n;
     }
-    CLM_CUDA((launch_convert<W, T>(st, n, cw, n, E, lde)));
+    CLM_TRY(pade_run<T>(st, chosen.m, n, src, ld_src, E, lde, ws.pade, d_info, blas));
+
+    // the squarings borrow the (now free) Pade region's digit planes
+    PadeWs<T> pw;
+    pw.carve(ws.pade, n, chosen.m, oz_scratch_bytes<T>(blas, n));
+    GemmScratch gs = lend_scratch<T>(blas, n, nullptr, 0, pw.oz, pw.oz_bytes);
+    GemmScratchScope gss(pw.oz ? &gs : nullptr);
+
+    if (elem<T>::single && chosen.s > 0) {
+      // single tiers: the squarings, where errors grow, run in FP64 tensor cores
+      using W = typename Wide<T>::type;
+      W *cw = ws.wide, *ow = ws.wide + (std::size_t)n * n;
+      CLM_CUDA((launch_convert<T, W>(st, n, E, lde, cw, n)));
+      for (int k = 0; k < chosen.s; ++k) {
+        CLM_CUDA(gemm_nn<W>(st, n, n, n, 1.0, cw, n, cw, n, 0.0, ow, n));
+        std::swap(cw, ow);
+      }
+      CLM_CUDA((launch_convert<W, T>(st, n, cw, n, E, lde)));
+      return ok_status();
+    }
+
+    // square s times, ping-ponging between the output and the scratch
+    T *cur = E, *other = ws.As;
+    int ld_cur = lde, ld_other = n;
+    for (int k = 0; k < chosen.s; ++k) {
+      CLM_CUDA(gemm_nn<T>(st, n, n, n, 1.0, cur, ld_cur, cur, ld_cur, 0.0, other, ld_other));
+      std::swap(cur, other);
+      std::swap(ld_cur, ld_other);
+    }
+    if (cur != E) CLM_CUDA(launch_scale_copy<T>(st, n, 1.0, cur, ld_cur, E, lde));
+    return ok_status();
+  };
+  // A call whose configuration (size, plan, pointers, stream, handle settings)
+  // repeats the previous call's of the same type is captured once as a CUDA
+  // graph and replayed from then on: one launch instead of one per kernel and
+  // per look-ahead event. Not while kernel timing is on, on the legacy default
+  // streams (not capturable), or on a thread that must create no CUDA
+  // resources (the no-look-ahead scope).
+  if (blas == nullptr || !blas->expm_graphs || tl_timer != nullptr || tl_no_lookahead || st == nullptr ||
+      st == cudaStreamLegacy || st == cudaStreamPerThread)
+    return post();
+  unsigned long long key = 1469598103934665603ull;
+  auto mix = [&key](unsigned long long v) { key = (key ^ v) * 1099511628211ull; };
+  mix((unsigned long long)n | ((unsigned long long)chosen.m << 32) | ((unsigned long long)chosen.s << 48));
+  mix(reinterpret_cast<std::uintptr_t>(A));
+  mix((unsigned long long)lda | ((unsigned long long)lde << 32));
+  mix(reinterpret_cast<std::uintptr_t>(E));
+  mix(reinterpret_cast<std::uintptr_t>(work));
+  mix((unsigned long long)lwork);
+  mix(reinterpret_cast<std::uintptr_t>(d_info));
+  mix(reinterpret_cast<std::uintptr_t>(st));
+  mix((unsigned long long)blas->split_terms | ((unsigned long long)(blas->fp64_digits + 16) << 32));
+  mix(reinterpret_cast<std::uintptr_t>(blas->work));
+  mix((unsigned long long)blas->work_bytes);
+  BatchedGraph &g = blas->single[type_slot<T>()];
+  if (g.exec != nullptr && g.key == key) {
+    CLM_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(g.exec), st));
+    note_launch(g.launches);
     return ok_status();
   }
-
-  // square s times, ping-ponging between the output and the scratch
-  T *cur = E, *other = ws.As;
-  int ld_cur = lde, ld_other = n;
-  for (int k = 0; k < chosen.s; ++k) {
-    CLM_CUDA(gemm_nn<T>(st, n, n, n, 1.0, cur, ld_cur, cur, ld_cur, 0.0, other, ld_other));
-    std::swap(cur, other);
-    std::swap(ld_cur, ld_other);
+  if (g.seen != key) {  // first sighting: run directly
+    g.seen = key;
+    return post();
   }
-  if (cur != E) CLM_CUDA(launch_scale_copy<T>(st, n, 1.0, cur, ld_cur, E, lde));
+  const unsigned long long before = g_launch_count();
+  cudaGraph_t graph = nullptr;
+  calamanStatus_t ps = ok_status();
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    ps = post();
+    e = cudaStreamEndCapture(st, &graph);
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess && is_ok(ps)) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess || !is_ok(ps) || exec == nullptr) {  // run directly from now on
+    cudaGetLastError();
+    blas->expm_graphs = 0;
+    return post();
+  }
+  if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
+  g.exec = exec;
+  g.key = key;
+  g.launches = (unsigned)(g_launch_count() - before);
+  CLM_CUDA(cudaGraphLaunch(exec, st));
   return ok_status();
 }
 
@@ -443,10 +505,27 @@ calamanStatus_t calamanDestroy(calamanHandle_t handle) {
   if (handle->h_pinned) cudaFreeHost(handle->h_pinned);
   for (auto &g : handle->graph)
     if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
+  for (auto &g : handle->single)
+    if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
   if (handle->side) cudaStreamDestroy(handle->side);
   if (handle->side_fork) cudaEventDestroy(handle->side_fork);
   if (handle->side_join) cudaEventDestroy(handle->side_join);
   delete handle;
+  return ok_status();
+}
+
+calamanStatus_t calamanSetExpmGraphs(calamanHandle_t handle, int enable) {
+  if (handle == nullptr) return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  handle->expm_graphs = enable != 0;
+  return ok_status();
+}
+
+calamanStatus_t calamanGetExpmGraphs(calamanHandle_t handle, int *enabled, int *cached) {
+  if (handle == nullptr || enabled == nullptr || cached == nullptr)
+    return blas_status(CALAMAN_STATUS_NOT_INITIALIZED);
+  *enabled = handle->expm_graphs;
+  *cached = 0;
+  for (const auto &g : handle->single) *cached += g.exec != nullptr;
   return ok_status();
 }
 
