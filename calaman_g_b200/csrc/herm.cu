@@ -980,7 +980,7 @@ __global__ void wy_t_kernel(int n, const C *__restrict__ tau, const C *__restric
     if (r < i) {
       C sacc = from_re<C>(0.0);
       for (int l = r; l < i; ++l) sacc = fmac(Ts[l * kb + r], Gs[i * kb + l], sacc);
-      Ts[i * kb + r] = neg(mul(tau[j0 + i], sacc));  // column i: no thread reads it this round
+      Ts[i * kb + r] = neg(mul(tau[j0 + i], sacc));  // column i: no thread reads it in this pass
     } else if (r == i) {
       Ts[i * kb + i] = tau[j0 + i];
     }
