@@ -861,7 +861,11 @@ def hbm_min(ns, esz, ms_per_step):
             "what": "each matrix read once and its exponential written once, per GPU"}
 
 
-E2E_SUB_BATCHES = 4
+# sub-batches of the batched end-to-end pipelines (--e2e-parts): measured on a
+# B200, the 8192-matrix expm gave 231k / 253k / 264k expm/s end to end with
+# 4 / 8 / 16, the 512-pair adjoint 168k / 151k vjp/s with 4 / 8
+E2E_PARTS_EXPM = 16
+E2E_PARTS_VJP = 4
 
 
 def _sub_batches(lib, capi, torch, dev, suf, ns, offs, dA, dE, host_in, host_out, info, parts):
@@ -1101,9 +1105,9 @@ def run_batched(args, cfg):
         # streams (one handle each), so one sub-batch's copies overlap another's
         # compute; every step still copies all inputs in and all results out
         subs = _sub_batches(lib, capi, torch, dev, suf, ns, offs, dA, dE, host_in, host_out, info,
-                            E2E_SUB_BATCHES)
+                            args.e2e_parts or E2E_PARTS_EXPM)
         e2e_ms = 0.0
-        for i in range(args.steps):
+        for i in range(args.warmup + args.steps):  # warm-up steps first, untimed
             a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a_ev.record(stream)
             for sb in subs:
@@ -1117,7 +1121,8 @@ def run_batched(args, cfg):
                 stream.wait_event(sb["done"])
             b_ev.record(stream)
             b_ev.synchronize()
-            e2e_ms += a_ev.elapsed_time(b_ev)
+            if i >= args.warmup:
+                e2e_ms += a_ev.elapsed_time(b_ev)
         for sb in subs:
             lib.calamanDestroy(sb["h"])
         # ---- the plain FP64 tier on the same matrices, timed the same way
@@ -1231,7 +1236,7 @@ def run_batched(args, cfg):
             "e2e": {"value": e2e_value, "unit": "expm/s",
                     "h2d_bytes_per_step": sum(n * n for n in ns) * esz,
                     "d2h_bytes_per_step": sum(n * n for n in ns) * esz,
-                    "pipeline": f"{E2E_SUB_BATCHES} sub-batches of equal sum n^3, one handle and stream "
+                    "pipeline": f"{args.e2e_parts or E2E_PARTS_EXPM} sub-batches of equal sum n^3, one handle and stream "
                                 "each, copies overlapping compute"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
@@ -1421,8 +1426,8 @@ def run_vjp(args, cfg):
             # as for the batched expm: sub-batches on their own streams, copies
             # overlapping compute, every input in and every gradient out each step
             subs = _vjp_sub_batches(lib, capi, torch, dev, suf, n, count, dA, dG, dD, host_a, host_g,
-                                    host_d, E2E_SUB_BATCHES)
-            for i in range(args.steps):
+                                    host_d, args.e2e_parts or E2E_PARTS_VJP)
+            for i in range(args.warmup + args.steps):  # warm-up steps first, untimed
                 a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a_ev.record(stream)
                 for sb in subs:
@@ -1437,7 +1442,8 @@ def run_vjp(args, cfg):
                     stream.wait_event(sb["done"])
                 b_ev.record(stream)
                 b_ev.synchronize()
-                e2e_ms += a_ev.elapsed_time(b_ev)
+                if i >= args.warmup:
+                    e2e_ms += a_ev.elapsed_time(b_ev)
             for sb in subs:
                 lib.calamanDestroy(sb["h"])
     torch.cuda.synchronize()
@@ -1486,7 +1492,7 @@ def run_vjp(args, cfg):
             "e2e": {"value": e2e_value, "unit": "vjp/s",
                     "h2d_bytes_per_step": 2 * count * n * n * esz,
                     "d2h_bytes_per_step": count * n * n * esz,
-                    "pipeline": (f"{E2E_SUB_BATCHES} sub-batches, one handle and stream each, copies "
+                    "pipeline": (f"{args.e2e_parts or E2E_PARTS_VJP} sub-batches, one handle and stream each, copies "
                                  "overlapping compute") if count > 1 else "one call"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
@@ -1651,6 +1657,8 @@ def main():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    p.add_argument("--e2e-parts", type=int, default=0,
+                   help="sub-batches of the batched end-to-end pipelines (copies of one overlap another's compute; 0: 16 for the batched expm, 4 for the batched adjoint)")
     p.add_argument("--no-plain", action="store_true",
                    help="batched workloads: skip the per-matrix FP64 expm pass (for profiling runs)")
     p.add_argument("--cpu-threads", type=int, default=0,
