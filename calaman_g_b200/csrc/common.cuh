@@ -354,6 +354,7 @@ struct calamanContext {
   clm::BatchedGraph graph[2];  // per batched tier: [0] float, [1] double
   int expm_graphs = 1;         // calaman_expm_* replays its launches after the norm readback
   clm::BatchedGraph single[4]; // per expm type: [0] float, [1] double, [2] complex64, [3] complex128
+  clm::BatchedGraph vjp[4];    // per expm_vjp type, the same order
   // second stream of the batched mixed tiers (the FP64 matrices run on it
   // beside the FP32 ones) and the fork / join events, created on first use
   cudaStream_t side = nullptr;

@@ -10,6 +10,7 @@
 #include <utility>
 
 #include "expm_common.cuh"
+#include "graph_replay.cuh"
 
 namespace clm {
 
@@ -143,11 +144,6 @@ calamanStatus_t pade_api(calamanHandle_t blas, calamanStream_t stream, int m, in
 }
 
 // ---- expm<T>, src/expm/expm.cppm:87-174 -------------------------------------
-// The handle's graph slot of each expm type.
-template <typename T> constexpr int type_slot() {
-  return std::is_same<T, float>::value ? 0 : std::is_same<T, double>::value ? 1 : std::is_same<T, float2>::value ? 2 : 3;
-}
-
 template <typename T>
 calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, const T *A, int lda,
                          T *E, int lde, void *work, std::size_t lwork, int *d_info,
@@ -216,60 +212,21 @@ calamanStatus_t expm_api(calamanHandle_t blas, calamanStream_t stream, int n, co
     if (cur != E) CLM_CUDA(launch_scale_copy<T>(st, n, 1.0, cur, ld_cur, E, lde));
     return ok_status();
   };
-  // A call whose configuration (size, plan, pointers, stream, handle settings)
-  // repeats the previous call's of the same type is captured once as a CUDA
-  // graph and replayed from then on: one launch instead of one per kernel and
-  // per look-ahead event. Not while kernel timing is on, on the legacy default
-  // streams (not capturable), or on a thread that must create no CUDA
-  // resources (the no-look-ahead scope).
-  if (blas == nullptr || !blas->expm_graphs || tl_timer != nullptr || tl_no_lookahead || st == nullptr ||
-      st == cudaStreamLegacy || st == cudaStreamPerThread)
-    return post();
-  unsigned long long key = 1469598103934665603ull;
-  auto mix = [&key](unsigned long long v) { key = (key ^ v) * 1099511628211ull; };
-  mix((unsigned long long)n | ((unsigned long long)chosen.m << 32) | ((unsigned long long)chosen.s << 48));
-  mix(reinterpret_cast<std::uintptr_t>(A));
-  mix((unsigned long long)lda | ((unsigned long long)lde << 32));
-  mix(reinterpret_cast<std::uintptr_t>(E));
-  mix(reinterpret_cast<std::uintptr_t>(work));
-  mix((unsigned long long)lwork);
-  mix(reinterpret_cast<std::uintptr_t>(d_info));
-  mix(reinterpret_cast<std::uintptr_t>(st));
-  mix((unsigned long long)blas->split_terms | ((unsigned long long)(blas->fp64_digits + 16) << 32));
-  mix(reinterpret_cast<std::uintptr_t>(blas->work));
-  mix((unsigned long long)blas->work_bytes);
-  BatchedGraph &g = blas->single[type_slot<T>()];
-  if (g.exec != nullptr && g.key == key) {
-    CLM_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(g.exec), st));
-    note_launch(g.launches);
-    return ok_status();
-  }
-  if (g.seen != key) {  // first sighting: run directly
-    g.seen = key;
-    return post();
-  }
-  const unsigned long long before = g_launch_count();
-  cudaGraph_t graph = nullptr;
-  calamanStatus_t ps = ok_status();
-  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    ps = post();
-    e = cudaStreamEndCapture(st, &graph);
-  }
-  cudaGraphExec_t exec = nullptr;
-  if (e == cudaSuccess && is_ok(ps)) e = cudaGraphInstantiate(&exec, graph, 0);
-  if (graph) cudaGraphDestroy(graph);
-  if (e != cudaSuccess || !is_ok(ps) || exec == nullptr) {  // run directly from now on
-    cudaGetLastError();
-    blas->expm_graphs = 0;
-    return post();
-  }
-  if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
-  g.exec = exec;
-  g.key = key;
-  g.launches = (unsigned)(g_launch_count() - before);
-  CLM_CUDA(cudaGraphLaunch(exec, st));
-  return ok_status();
+  // replayed as a CUDA graph while the configuration repeats
+  CallKey key;
+  key.mix((unsigned long long)n | ((unsigned long long)chosen.m << 32) | ((unsigned long long)chosen.s << 48));
+  key.mix(A);
+  key.mix((unsigned long long)lda | ((unsigned long long)lde << 32));
+  key.mix(E);
+  key.mix(work);
+  key.mix((unsigned long long)lwork);
+  key.mix(d_info);
+  key.mix(st);
+  if (blas == nullptr) return post();
+  key.mix((unsigned long long)blas->split_terms | ((unsigned long long)(blas->fp64_digits + 16) << 32));
+  key.mix(blas->work);
+  key.mix((unsigned long long)blas->work_bytes);
+  return run_or_replay(&blas->expm_graphs, blas->single[type_slot<T>()], st, key.h, post);
 }
 
 template <typename T, typename R>
@@ -507,6 +464,8 @@ calamanStatus_t calamanDestroy(calamanHandle_t handle) {
     if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
   for (auto &g : handle->single)
     if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
+  for (auto &g : handle->vjp)
+    if (g.exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g.exec));
   if (handle->side) cudaStreamDestroy(handle->side);
   if (handle->side_fork) cudaEventDestroy(handle->side_fork);
   if (handle->side_join) cudaEventDestroy(handle->side_join);
@@ -526,6 +485,7 @@ calamanStatus_t calamanGetExpmGraphs(calamanHandle_t handle, int *enabled, int *
   *enabled = handle->expm_graphs;
   *cached = 0;
   for (const auto &g : handle->single) *cached += g.exec != nullptr;
+  for (const auto &g : handle->vjp) *cached += g.exec != nullptr;
   return ok_status();
 }
 

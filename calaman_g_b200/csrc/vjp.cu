@@ -22,6 +22,7 @@
 #include <utility>
 
 #include "expm_common.cuh"
+#include "graph_replay.cuh"
 
 namespace clm {
 namespace {
@@ -121,106 +122,127 @@ calamanStatus_t vjp_api(calamanHandle_t blas, calamanStream_t stream, int n, con
   const int m = plan.m, np = pade_num_powers(m);
   const double *b = pade_coeffs(m);
 
-  VjpWs<T> ws;
-  ws.carve(work, n, m, oz_scratch_bytes<T>(blas, n));
-  GemmScratch gs = lend_scratch<T>(blas, n, ws.tc, ws.tc_bytes, ws.oz, ws.oz_bytes);
-  GemmScratchScope gss((ws.tc || ws.oz) ? &gs : nullptr);
-  auto mm = [&](const T *X, const T *Y, double beta, T *Z) {
-    return gemm_nn<T>(st, n, n, n, 1.0, X, n, Y, n, beta, Z, n);
-  };
+  // everything after the plan: launches only, replayed as a CUDA graph while
+  // the configuration repeats
+  auto post = [&]() -> calamanStatus_t {
+    VjpWs<T> ws;
+    ws.carve(work, n, m, oz_scratch_bytes<T>(blas, n));
+    GemmScratch gs = lend_scratch<T>(blas, n, ws.tc, ws.tc_bytes, ws.oz, ws.oz_bytes);
+    GemmScratchScope gss((ws.tc || ws.oz) ? &gs : nullptr);
+    auto mm = [&](const T *X, const T *Y, double beta, T *Z) {
+      return gemm_nn<T>(st, n, n, n, 1.0, X, n, Y, n, beta, Z, n);
+    };
 
-  // X = 2^-s A^H, D = 2^-s G
-  const double f = std::ldexp(1.0, -plan.s);
-  CLM_CUDA(launch_transpose<T>(st, n, n, f, A, lda, ws.Xs, n, true));
-  CLM_CUDA(launch_scale_copy<T>(st, n, f, G, ldg, ws.Ds, n));
+    // X = 2^-s A^H, D = 2^-s G
+    const double f = std::ldexp(1.0, -plan.s);
+    CLM_CUDA(launch_transpose<T>(st, n, n, f, A, lda, ws.Xs, n, true));
+    CLM_CUDA(launch_scale_copy<T>(st, n, f, G, ldg, ws.Ds, n));
 
-  // even powers and their derivatives (the forward pass's order: A4 = A2 A2,
-  // A6 = A4 A2, A8 = A4 A4)
-  T **P = ws.P, **M = ws.M;
-  CLM_CUDA(mm(ws.Xs, ws.Xs, 0.0, P[0]));
-  CLM_CUDA(mm(ws.Xs, ws.Ds, 0.0, M[0]));
-  CLM_CUDA(mm(ws.Ds, ws.Xs, 1.0, M[0]));
-  if (np >= 2) {
-    CLM_CUDA(mm(P[0], P[0], 0.0, P[1]));
-    CLM_CUDA(mm(P[0], M[0], 0.0, M[1]));
-    CLM_CUDA(mm(M[0], P[0], 1.0, M[1]));
-  }
-  if (np >= 3) {
-    CLM_CUDA(mm(P[1], P[0], 0.0, P[2]));
-    CLM_CUDA(mm(M[1], P[0], 0.0, M[2]));
-    CLM_CUDA(mm(P[1], M[0], 1.0, M[2]));
-  }
-  if (np >= 4) {
-    CLM_CUDA(mm(P[1], P[1], 0.0, P[3]));
-    CLM_CUDA(mm(P[1], M[1], 0.0, M[3]));
-    CLM_CUDA(mm(M[1], P[1], 1.0, M[3]));
-  }
-
-  if (m != 13) {
-    double cv[5] = {0, 0, 0, 0, 0}, cw[5] = {0, 0, 0, 0, 0};
-    for (int i = 0; i <= np; ++i) {
-      cv[i] = b[2 * i];
-      cw[i] = b[2 * i + 1];
+    // even powers and their derivatives (the forward pass's order: A4 = A2 A2,
+    // A6 = A4 A2, A8 = A4 A4)
+    T **P = ws.P, **M = ws.M;
+    CLM_CUDA(mm(ws.Xs, ws.Xs, 0.0, P[0]));
+    CLM_CUDA(mm(ws.Xs, ws.Ds, 0.0, M[0]));
+    CLM_CUDA(mm(ws.Ds, ws.Xs, 1.0, M[0]));
+    if (np >= 2) {
+      CLM_CUDA(mm(P[0], P[0], 0.0, P[1]));
+      CLM_CUDA(mm(P[0], M[0], 0.0, M[1]));
+      CLM_CUDA(mm(M[0], P[0], 1.0, M[1]));
     }
-    CLM_CUDA(launch_pade_even_odd<T>(st, n, np, P[0], P[1], P[2], P[3], cv, cw, ws.V, ws.W));
-    cv[0] = 0.0;
-    cw[0] = 0.0;  // the derivative of the identity term is zero
-    CLM_CUDA(launch_pade_even_odd<T>(st, n, np, M[0], M[1], M[2], M[3], cv, cw, ws.LV, ws.LW));
-  } else {
-    // odd: W1 = b9 A2 + b11 A4 + b13 A6, W = b1 I + b3 A2 + b5 A4 + b7 A6 + A6 W1
-    const double co[5] = {0.0, b[9], b[11], b[13], 0.0};
-    const double cwo[5] = {b[1], b[3], b[5], b[7], 0.0};
-    const double cwo0[5] = {0.0, b[3], b[5], b[7], 0.0};
-    CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, P[0], P[1], P[2], nullptr, co, cwo, ws.T1, ws.W));
-    CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, M[0], M[1], M[2], nullptr, co, cwo0, ws.T2, ws.LW));
-    CLM_CUDA(mm(P[2], ws.T2, 1.0, ws.LW));  // dW += A6 dW1 + dA6 W1
-    CLM_CUDA(mm(M[2], ws.T1, 1.0, ws.LW));
-    CLM_CUDA(mm(P[2], ws.T1, 1.0, ws.W));
-    // even: Z1 = b8 A2 + b10 A4 + b12 A6, V = b0 I + b2 A2 + b4 A4 + b6 A6 + A6 Z1
-    const double ce[5] = {0.0, b[8], b[10], b[12], 0.0};
-    const double cve[5] = {b[0], b[2], b[4], b[6], 0.0};
-    const double cve0[5] = {0.0, b[2], b[4], b[6], 0.0};
-    CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, P[0], P[1], P[2], nullptr, ce, cve, ws.T1, ws.V));
-    CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, M[0], M[1], M[2], nullptr, ce, cve0, ws.T2, ws.LV));
-    CLM_CUDA(mm(P[2], ws.T2, 1.0, ws.LV));
-    CLM_CUDA(mm(M[2], ws.T1, 1.0, ws.LV));
-    CLM_CUDA(mm(P[2], ws.T1, 1.0, ws.V));
-  }
-  // U = X W, dU = X dW + D W
-  CLM_CUDA(mm(ws.Xs, ws.W, 0.0, ws.T1));
-  CLM_CUDA(mm(ws.Xs, ws.LW, 0.0, ws.T2));
-  CLM_CUDA(mm(ws.Ds, ws.W, 1.0, ws.T2));
-  // p = V + U over T1, q = V - U over V; dp over T2, dq over LV
-  CLM_CUDA(launch_pade_split<T>(st, n, ws.T1, ws.V, ws.T1, n, ws.V));
-  CLM_CUDA(launch_pade_split<T>(st, n, ws.T2, ws.LV, ws.T2, n, ws.LV));
-  // R = q^-1 p; dR = q^-1 (dp - dq R)
-  T *Rm = P[0], *Lm = M[0];
-  CLM_CUDA(getrf<T>(st, n, ws.V, n, ws.lu, d_info));
-  CLM_CUDA(getrs<T>(st, n, n, ws.V, n, ws.lu, ws.T1, n, Rm, n, d_info + 1));
-  CLM_CUDA(gemm_nn<T>(st, n, n, n, -1.0, ws.LV, n, Rm, n, 1.0, ws.T2, n));
-  CLM_CUDA(getrs<T>(st, n, n, ws.V, n, ws.lu, ws.T2, n, Lm, n, d_info + 1));
-
-  if (elem<T>::single && plan.s > 0) {
-    // single tiers square in FP64, like expm
-    using Wd = typename Wide<T>::type;
-    const std::size_t nn = (std::size_t)n * n;
-    Wd *r = ws.wide, *l = ws.wide + nn, *r2 = ws.wide + 2 * nn, *l2 = ws.wide + 3 * nn;
-    CLM_CUDA((launch_convert<T, Wd>(st, n, Rm, n, r, n)));
-    CLM_CUDA((launch_convert<T, Wd>(st, n, Lm, n, l, n)));
-    CLM_CUDA(frechet_squarings<Wd>(st, n, plan.s, &r, &l, &r2, &l2));
-    CLM_CUDA((launch_convert<Wd, T>(st, n, l, n, gradA, ldga)));
-    if (E) {
-      CLM_CUDA((launch_convert<Wd, T>(st, n, r, n, ws.T1, n)));
-      CLM_CUDA(launch_transpose<T>(st, n, n, 1.0, ws.T1, n, E, lde, true));
+    if (np >= 3) {
+      CLM_CUDA(mm(P[1], P[0], 0.0, P[2]));
+      CLM_CUDA(mm(M[1], P[0], 0.0, M[2]));
+      CLM_CUDA(mm(P[1], M[0], 1.0, M[2]));
     }
+    if (np >= 4) {
+      CLM_CUDA(mm(P[1], P[1], 0.0, P[3]));
+      CLM_CUDA(mm(P[1], M[1], 0.0, M[3]));
+      CLM_CUDA(mm(M[1], P[1], 1.0, M[3]));
+    }
+
+    if (m != 13) {
+      double cv[5] = {0, 0, 0, 0, 0}, cw[5] = {0, 0, 0, 0, 0};
+      for (int i = 0; i <= np; ++i) {
+        cv[i] = b[2 * i];
+        cw[i] = b[2 * i + 1];
+      }
+      CLM_CUDA(launch_pade_even_odd<T>(st, n, np, P[0], P[1], P[2], P[3], cv, cw, ws.V, ws.W));
+      cv[0] = 0.0;
+      cw[0] = 0.0;  // the derivative of the identity term is zero
+      CLM_CUDA(launch_pade_even_odd<T>(st, n, np, M[0], M[1], M[2], M[3], cv, cw, ws.LV, ws.LW));
+    } else {
+      // odd: W1 = b9 A2 + b11 A4 + b13 A6, W = b1 I + b3 A2 + b5 A4 + b7 A6 + A6 W1
+      const double co[5] = {0.0, b[9], b[11], b[13], 0.0};
+      const double cwo[5] = {b[1], b[3], b[5], b[7], 0.0};
+      const double cwo0[5] = {0.0, b[3], b[5], b[7], 0.0};
+      CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, P[0], P[1], P[2], nullptr, co, cwo, ws.T1, ws.W));
+      CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, M[0], M[1], M[2], nullptr, co, cwo0, ws.T2, ws.LW));
+      CLM_CUDA(mm(P[2], ws.T2, 1.0, ws.LW));  // dW += A6 dW1 + dA6 W1
+      CLM_CUDA(mm(M[2], ws.T1, 1.0, ws.LW));
+      CLM_CUDA(mm(P[2], ws.T1, 1.0, ws.W));
+      // even: Z1 = b8 A2 + b10 A4 + b12 A6, V = b0 I + b2 A2 + b4 A4 + b6 A6 + A6 Z1
+      const double ce[5] = {0.0, b[8], b[10], b[12], 0.0};
+      const double cve[5] = {b[0], b[2], b[4], b[6], 0.0};
+      const double cve0[5] = {0.0, b[2], b[4], b[6], 0.0};
+      CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, P[0], P[1], P[2], nullptr, ce, cve, ws.T1, ws.V));
+      CLM_CUDA(launch_pade_even_odd<T>(st, n, 3, M[0], M[1], M[2], nullptr, ce, cve0, ws.T2, ws.LV));
+      CLM_CUDA(mm(P[2], ws.T2, 1.0, ws.LV));
+      CLM_CUDA(mm(M[2], ws.T1, 1.0, ws.LV));
+      CLM_CUDA(mm(P[2], ws.T1, 1.0, ws.V));
+    }
+    // U = X W, dU = X dW + D W
+    CLM_CUDA(mm(ws.Xs, ws.W, 0.0, ws.T1));
+    CLM_CUDA(mm(ws.Xs, ws.LW, 0.0, ws.T2));
+    CLM_CUDA(mm(ws.Ds, ws.W, 1.0, ws.T2));
+    // p = V + U over T1, q = V - U over V; dp over T2, dq over LV
+    CLM_CUDA(launch_pade_split<T>(st, n, ws.T1, ws.V, ws.T1, n, ws.V));
+    CLM_CUDA(launch_pade_split<T>(st, n, ws.T2, ws.LV, ws.T2, n, ws.LV));
+    // R = q^-1 p; dR = q^-1 (dp - dq R)
+    T *Rm = P[0], *Lm = M[0];
+    CLM_CUDA(getrf<T>(st, n, ws.V, n, ws.lu, d_info));
+    CLM_CUDA(getrs<T>(st, n, n, ws.V, n, ws.lu, ws.T1, n, Rm, n, d_info + 1));
+    CLM_CUDA(gemm_nn<T>(st, n, n, n, -1.0, ws.LV, n, Rm, n, 1.0, ws.T2, n));
+    CLM_CUDA(getrs<T>(st, n, n, ws.V, n, ws.lu, ws.T2, n, Lm, n, d_info + 1));
+
+    if (elem<T>::single && plan.s > 0) {
+      // single tiers square in FP64, like expm
+      using Wd = typename Wide<T>::type;
+      const std::size_t nn = (std::size_t)n * n;
+      Wd *r = ws.wide, *l = ws.wide + nn, *r2 = ws.wide + 2 * nn, *l2 = ws.wide + 3 * nn;
+      CLM_CUDA((launch_convert<T, Wd>(st, n, Rm, n, r, n)));
+      CLM_CUDA((launch_convert<T, Wd>(st, n, Lm, n, l, n)));
+      CLM_CUDA(frechet_squarings<Wd>(st, n, plan.s, &r, &l, &r2, &l2));
+      CLM_CUDA((launch_convert<Wd, T>(st, n, l, n, gradA, ldga)));
+      if (E) {
+        CLM_CUDA((launch_convert<Wd, T>(st, n, r, n, ws.T1, n)));
+        CLM_CUDA(launch_transpose<T>(st, n, n, 1.0, ws.T1, n, E, lde, true));
+      }
+      return ok_status();
+    }
+    T *r2 = ws.T1, *l2 = ws.LW;
+    CLM_CUDA(frechet_squarings<T>(st, n, plan.s, &Rm, &Lm, &r2, &l2));
+    CLM_CUDA(launch_scale_copy<T>(st, n, 1.0, Lm, n, gradA, ldga));
+    // g(A^H) = g(A)^H
+    if (E) CLM_CUDA(launch_transpose<T>(st, n, n, 1.0, Rm, n, E, lde, true));
     return ok_status();
-  }
-  T *r2 = ws.T1, *l2 = ws.LW;
-  CLM_CUDA(frechet_squarings<T>(st, n, plan.s, &Rm, &Lm, &r2, &l2));
-  CLM_CUDA(launch_scale_copy<T>(st, n, 1.0, Lm, n, gradA, ldga));
-  // g(A^H) = g(A)^H
-  if (E) CLM_CUDA(launch_transpose<T>(st, n, n, 1.0, Rm, n, E, lde, true));
-  return ok_status();
+  };
+  if (blas == nullptr) return post();
+  CallKey key;
+  key.mix((unsigned long long)n | ((unsigned long long)plan.m << 32) | ((unsigned long long)plan.s << 48));
+  key.mix(A);
+  key.mix(G);
+  key.mix(gradA);
+  key.mix(E);
+  key.mix((unsigned long long)lda | ((unsigned long long)ldg << 32));
+  key.mix((unsigned long long)ldga | ((unsigned long long)lde << 32));
+  key.mix(work);
+  key.mix((unsigned long long)lwork);
+  key.mix(d_info);
+  key.mix(st);
+  key.mix((unsigned long long)blas->split_terms | ((unsigned long long)(blas->fp64_digits + 16) << 32));
+  key.mix(blas->work);
+  key.mix((unsigned long long)blas->work_bytes);
+  return run_or_replay(&blas->expm_graphs, blas->vjp[type_slot<T>()], st, key.h, post);
 }
 
 }  // namespace

@@ -551,13 +551,14 @@ calamanStatus_t calaman_gemm_ozaki_wait_check(calamanStream_t stream, long long 
  * calamanTuneBatched_bufferSize(count) bytes), keeps it in the handle and
  * returns it; the built-in default is the table it measured on a B200. */
 calamanStatus_t calamanSetBatchedGraphs(calamanHandle_t handle, int enable);
-/* calaman_expm_{s,d,c,z} likewise (no counterpart in the reference, whose
- * expm launches its kernels one by one): everything after the 1-norm readback
- * depends only on the size, the plan, the pointers, the stream and the
- * handle's settings, so a call that repeats the previous call of its type in
- * all of them replays a captured CUDA graph of those launches (on by default;
- * off while kernel timing is on, on the legacy default streams, and in
- * calaman_expm_noalloc_d). `cached`: the types with a graph held. */
+/* calaman_expm_{s,d,c,z} and calaman_expm_vjp_{s,d,c,z} likewise (no
+ * counterpart in the reference, whose expm launches its kernels one by one):
+ * everything after the 1-norm readback depends only on the size, the plan, the
+ * pointers, the stream and the handle's settings, so a call that repeats the
+ * previous call of its entry and type in all of them replays a captured CUDA
+ * graph of those launches (on by default; off while kernel timing is on, on
+ * the legacy default streams, and in calaman_expm_noalloc_d). `cached`: the
+ * entry and type pairs with a graph held. */
 calamanStatus_t calamanSetExpmGraphs(calamanHandle_t handle, int enable);
 calamanStatus_t calamanGetExpmGraphs(calamanHandle_t handle, int *enabled, int *cached);
 calamanStatus_t calamanGetBatchedGraphs(calamanHandle_t handle, int *enabled, int *cached);
