@@ -231,6 +231,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the first sample before the timed region starts, so a region
+            # shorter than the sampling period still has one
+            t0 = time.time()
+            while not self.rows and self.proc.poll() is None and time.time() - t0 < 3.0:
+                time.sleep(0.01)
         except (OSError, ValueError):
             self.proc = None
         return self

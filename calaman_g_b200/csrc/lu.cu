@@ -1133,19 +1133,23 @@ __global__ void __launch_bounds__(MAXT, 1)
 // thread on NT8 threads: float32 runs 1024 threads of 4 rows there (64
 // registers, a few spilled), measured 5 % faster on the float32 4096 expm than
 // 512 threads of 8 rows; float64 1024 x 2 rows at heights up to 2048, and
-// complex128 1024 x 1 row (sub-panels of 4) at 1024, measured slower.
+// complex128 1024 x 1 row (sub-panels of 4) at 1024, measured slower. Panels
+// of 16 columns for float32, float64 and complex128: with the expm's launches
+// replayed as a graph, more and narrower panels cost less than a second
+// sub-panel's rest-of-panel update on the one SM (float64 256 expm +15 %,
+// complex128 1024 +4 %, float32 4096 +3 %; 8 columns: float32 4096 -20 %).
 template <typename T> struct CtaPanel;
 template <> struct CtaPanel<double2> {
-  static constexpr int KBS1 = 8, KBS2 = 8, KBS4 = 4, KBS8 = 0, RPT8 = 8, NT8 = 512, KB = 32;
+  static constexpr int KBS1 = 8, KBS2 = 8, KBS4 = 4, KBS8 = 0, RPT8 = 8, NT8 = 512, KB = 16;
 };
 template <> struct CtaPanel<double> {
-  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, RPT8 = 8, NT8 = 512, KB = 32;
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, RPT8 = 8, NT8 = 512, KB = 16;
 };
 template <> struct CtaPanel<float2> {
   static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 8, KBS8 = 4, RPT8 = 8, NT8 = 512, KB = 32;
 };
 template <> struct CtaPanel<float> {  // 32 wide: the in-panel SIMT update costs h kb^2 / 2 per panel
-  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, RPT8 = 4, NT8 = 1024, KB = 32;
+  static constexpr int KBS1 = 16, KBS2 = 16, KBS4 = 16, KBS8 = 8, RPT8 = 4, NT8 = 1024, KB = 16;
 };
 
 // Panel width of the one-CTA path for an n x n factorisation, 0 if n is too
