@@ -631,11 +631,26 @@ __global__ void __launch_bounds__(NT)
                g_map_count, info);
 }
 
-// Load the kb x kb diagonal block A[k:k+kb, k:k+kb] into shared memory.
+// Load the kb x kb diagonal block A[k:k+kb, k:k+kb] into shared memory (D[l kb + i]
+// = A(k + i, k + l)): a warp per column, 16-byte copies when every column of
+// the block starts 16-byte aligned, else one element per copy. (The per-element
+// form with an index division per element set the time of the 128-row float32
+// solve blocks: 16k copies per CTA.)
 template <typename T>
 __device__ __forceinline__ void load_diag_block(T *D, const T *A, int lda, int k, int kb) {
-  for (int idx = threadIdx.x; idx < kb * kb; idx += blockDim.x)
-    cp_async_elem(&D[idx], &A[(std::size_t)(k + idx / kb) * lda + (k + idx % kb)]);
+  constexpr int V = 16 / sizeof(T);  // elements per 16-byte copy
+  const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+  const T *base = A + (std::size_t)k * lda + k;
+  if (V > 1 && kb % V == 0 && lda % V == 0 && (reinterpret_cast<std::uintptr_t>(base) & 15) == 0) {
+    for (int l = threadIdx.x >> 5; l < kb; l += warps)
+      for (int i = lane * V; i < kb; i += 32 * V) {
+        const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(&D[l * kb + i]));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(&base[(std::size_t)l * lda + i]));
+      }
+  } else {
+    for (int l = threadIdx.x >> 5; l < kb; l += warps)
+      for (int i = lane; i < kb; i += 32) cp_async_elem(&D[l * kb + i], &base[(std::size_t)l * lda + i]);
+  }
   cp_async_wait_all();
 }
 
