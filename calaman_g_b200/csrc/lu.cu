@@ -718,6 +718,62 @@ __global__ void gather_rows_kernel(int n, int nrhs, const int *__restrict__ perm
     X[(std::size_t)c * ldx + row] = B[(std::size_t)c * ldb + src];
 }
 
+// The same solve for a full block (kb = 32 VPL): the steps run in runs of 32
+// whose pivot rows sit in one register of every lane (x[vo]), so the lane
+// selection and most bound checks are static; each row still takes the
+// updates in the same order, so the results are those of the general kernel.
+template <typename T, bool LOWER, int VPL>
+__global__ void __launch_bounds__(256)
+    trsm_diag_full_kernel(int nrhs, const T *__restrict__ LU, int lda, int k, T *__restrict__ X, int ldx) {
+  constexpr int kb = 32 * VPL;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *D = reinterpret_cast<T *>(smem_raw);
+  T *rdiag = D + kb * kb;
+  load_diag_block(D, LU, lda, k, kb);
+  __syncthreads();
+  if (!LOWER && threadIdx.x < kb) {
+    const T d = D[threadIdx.x * kb + threadIdx.x];
+    rdiag[threadIdx.x] = divide(elem<T>::one(), d);
+  }
+  __syncthreads();
+  const int warps = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * warps + (threadIdx.x >> 5);
+  if (c >= nrhs) return;
+  T *col = X + (std::size_t)c * ldx + k;
+  T x[VPL];
+#pragma unroll
+  for (int v = 0; v < VPL; ++v) x[v] = col[lane + 32 * v];
+  if (LOWER) {
+#pragma unroll
+    for (int vo = 0; vo < VPL; ++vo) {
+#pragma unroll 4
+      for (int ll = 0; ll < 32; ++ll) {
+        const int l = 32 * vo + ll;
+        const T xl = shfl(x[vo], ll);
+        if (lane > ll) x[vo] = sub(x[vo], mul(D[l * kb + lane + 32 * vo], xl));
+#pragma unroll
+        for (int v = vo + 1; v < VPL; ++v) x[v] = sub(x[v], mul(D[l * kb + lane + 32 * v], xl));
+      }
+    }
+  } else {
+#pragma unroll
+    for (int vo = VPL - 1; vo >= 0; --vo) {
+#pragma unroll 4
+      for (int ll = 31; ll >= 0; --ll) {
+        const int l = 32 * vo + ll;
+        const T xl = mul(shfl(x[vo], ll), rdiag[l]);
+        if (lane == ll) x[vo] = xl;
+        if (lane < ll) x[vo] = sub(x[vo], mul(D[l * kb + lane + 32 * vo], xl));
+#pragma unroll
+        for (int v = 0; v < vo; ++v) x[v] = sub(x[v], mul(D[l * kb + lane + 32 * v], xl));
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < VPL; ++v) col[lane + 32 * v] = x[v];
+}
+
 // Diagonal-block triangular solve on rows [k, k+kb) of X (kb <= 32 VPL), one
 // warp per RHS column, lane l keeping rows l, l + 32, ... LOWER: unit lower
 // (forward); else non-unit upper (backward), whose diagonal reciprocals are
@@ -1458,12 +1514,20 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   const std::size_t smem = sizeof(T) * (NB * NB + NB);
   auto kl = wide ? trsm_diag_kernel<T, true, 4> : trsm_diag_kernel<T, true, 2>;
   auto ku = wide ? trsm_diag_kernel<T, false, 4> : trsm_diag_kernel<T, false, 2>;
-  if ((e = cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(ku, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
+  // full blocks (every one but a ragged last) take the static-lane kernel
+  auto fl = wide ? trsm_diag_full_kernel<T, true, 4> : trsm_diag_full_kernel<T, true, 2>;
+  auto fu = wide ? trsm_diag_full_kernel<T, false, 4> : trsm_diag_full_kernel<T, false, 2>;
+  for (auto kern : {kl, ku})
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+      return e;
+  for (auto kern : {fl, fu})
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+      return e;
   const int blocks = (nrhs + warps - 1) / warps;
   for (int k = 0; k < n; k += NB) {
     const int kb = (k + NB < n) ? NB : n - k;
-    kl<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, kb, X, ldx);
+    if (kb == NB) fl<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, X, ldx);
+    else kl<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, kb, X, ldx);
     if ((e = launched()) != cudaSuccess) return e;
     if (k + kb < n) {
       e = gemm_nn<T>(s, n - (k + kb), nrhs, kb, -1.0, LU + (std::size_t)k * lda + (k + kb), lda,
@@ -1474,7 +1538,8 @@ cudaError_t getrs(cudaStream_t s, int n, int nrhs, const T *LU, int lda, const v
   const int last = ((n - 1) / NB) * NB;
   for (int k = last; k >= 0; k -= NB) {
     const int kb = (k + NB < n) ? NB : n - k;
-    ku<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, kb, X, ldx);
+    if (kb == NB) fu<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, X, ldx);
+    else ku<<<blocks, warps * 32, sizeof(T) * (kb * kb + kb), s>>>(nrhs, LU, lda, k, kb, X, ldx);
     if ((e = launched()) != cudaSuccess) return e;
     if (k > 0) {
       e = gemm_nn<T>(s, k, nrhs, kb, -1.0, LU + (std::size_t)k * lda, lda, X + k, ldx, 1.0, X, ldx);
